@@ -1,0 +1,173 @@
+/* hn_sm100 -- B200 (sm_100a) FP64 sparse linear algebra for the HyperNova LP
+ * solvers, exported as a plain C ABI.
+ *
+ * This library replaces the GPU half of HyperNova's compute backend: the
+ * dlopen'ed CUDA driver loader (core/execution/cuda_driver.cpp:24-56,112-147),
+ * the embedded sm_50 PTX kernels (core/execution/cuda_kernels_ptx.cpp:21-378)
+ * and the device work of CudaDriverBackend (core/execution/gpu_backend.cpp:141-617),
+ * and moves on to the device the host loops of the IPM hot path
+ * (core/lp/interior_point.cpp:52-69,134-200,507-696).
+ *
+ * Conventions
+ *  - Every entry point returns an int status (HN_OK == 0). On failure the
+ *    thread-local message from hn_last_error() says why. No C++ exception
+ *    crosses this boundary. There is no CPU fallback: a call that cannot run
+ *    on the GPU fails.
+ *  - Matrix arguments are CSR arrays in the reference's layout: row_ptr and
+ *    col_idx as 64-bit unsigned (std::size_t), values as double.
+ *    Device storage is int32 indices; nnz, m and n must each be < 2^31.
+ *  - Pointers named *_dev are device pointers; *_host are host pointers.
+ *    `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *  - Products and reductions on one handle must not overlap on the GPU
+ *    (each handle owns its merge-path carry buffers); reductions issued on
+ *    one stream are serialised by that stream's workspace.
+ *  - Reductions (dot, norms, maxima) are deterministic: the same inputs on the
+ *    same device give the same bits on every run.
+ */
+#ifndef HN_SM100_H
+#define HN_SM100_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define HN_OK 0
+#define HN_ERR_INVALID_ARG 1
+#define HN_ERR_CUDA 2
+#define HN_ERR_OUT_OF_MEMORY 3
+#define HN_ERR_NOT_INITIALIZED 4
+#define HN_ERR_UNSUPPORTED 5
+#define HN_ERR_NUMERICAL 6
+#define HN_ERR_INJECTED 7
+
+/* ---- hn_csr_create flags ---- */
+#define HN_CSR_NO_TRANSPOSE 1u /* do not build the device A^T */
+
+typedef struct hn_csr hn_csr;         /* device-resident CSR matrix (+ its A^T) */
+typedef struct hn_pattern hn_pattern; /* fixed pattern of A diag(d) A^T + reg I */
+
+typedef struct hn_device_info_t {
+    char name[256];
+    int device;
+    int sm_count;
+    int cc_major;
+    int cc_minor;
+    size_t total_mem;
+    size_t free_mem;
+} hn_device_info_t;
+
+/* ---- lifecycle ----
+ * hn_init replaces CudaDriverBackend::initialize (gpu_backend.cpp:159-192) and
+ * DriverApi::load/init_context (cuda_driver.cpp:112-147,204-236): binds the
+ * calling thread to `device` (primary context). Fails with
+ * HN_ERR_UNSUPPORTED unless the device is compute capability 10.0. */
+int hn_init(int device);
+/* Releases per-stream workspaces. Handles must be destroyed first.
+ * (CudaDriverBackend::finalize, gpu_backend.cpp:194-198) */
+int hn_shutdown(void);
+/* Thread-local text of the last failure (CudaDriverBackend::last_error_). */
+const char* hn_last_error(void);
+/* Device name and memory (CudaDriverBackend::name/device_memory/free_memory,
+ * gpu_backend.cpp:150-153,249-259). */
+int hn_device_info(hn_device_info_t* out);
+/* Kernel launch counter (IComputeBackend::gpu_kernel_executions,
+ * gpu_backend.hpp:47-50). */
+int hn_stats(uint64_t* kernel_launches, uint64_t* api_calls);
+int hn_reset_stats(void);
+/* Host-side fault injection for failure tests: after `after_calls` further
+ * API calls, the next call returns `status` without touching the GPU.
+ * after_calls < 0 disarms. No reference counterpart (the reference has no
+ * fault injection); it lets tests reach every error path without a GPU fault. */
+int hn_fault_inject(int64_t after_calls, int status);
+
+/* ---- device memory for callers without a CUDA runtime ----
+ * (DriverApi::allocate/free/copy_h2d/copy_d2h/memset_d8, cuda_driver.hpp:44-93) */
+int hn_malloc(void** ptr_dev, size_t bytes);
+int hn_free(void* ptr_dev);
+int hn_memcpy_h2d(void* dst_dev, const void* src_host, size_t bytes, void* stream);
+int hn_memcpy_d2h(void* dst_host, const void* src_dev, size_t bytes, void* stream);
+int hn_memcpy_d2d(void* dst_dev, const void* src_dev, size_t bytes, void* stream);
+int hn_memset(void* ptr_dev, int byte, size_t bytes, void* stream);
+int hn_stream_sync(void* stream);
+
+/* ---- CSR matrices ----
+ * Uploads A (host arrays, reference layout) once and builds on the device:
+ * int32 indices, the merge-path tile table (row binning) and, unless
+ * HN_CSR_NO_TRANSPOSE, A^T as its own CSR. A^T equals the reference's
+ * SparseMatrix::transposed() bit for bit (sparse_matrix.cpp:84-96): entries
+ * ordered by (column,row), equal keys summed in input order, exact zero sums
+ * dropped. Replaces CudaDriverBackend::upload_matrix/resident_matrix
+ * (gpu_backend.cpp:289-306,360-393) with an explicit handle. */
+int hn_csr_create(int64_t m, int64_t n, const uint64_t* row_ptr_host,
+                  const uint64_t* col_idx_host, const double* val_host, unsigned flags,
+                  hn_csr** out);
+/* New values for the same pattern (host array, nnz entries); A^T follows. */
+int hn_csr_set_values(hn_csr* A, const double* val_host);
+int hn_csr_destroy(hn_csr* A);
+int hn_csr_shape(const hn_csr* A, int64_t* m, int64_t* n, int64_t* nnz, int64_t* nnz_t);
+/* Host copy of A (trans=0) or A^T (trans=1) in the reference layout.
+ * rp: rows+1 entries; ci/val: nnz entries. */
+int hn_csr_export(const hn_csr* A, int trans, uint64_t* rp_host, uint64_t* ci_host,
+                  double* val_host);
+/* Merge-path tile table (row binning) of A or A^T: ntiles+1 coordinates. */
+int hn_csr_tiles(const hn_csr* A, int trans, int64_t* ntiles, int64_t* items_per_tile);
+int hn_csr_export_tiles(const hn_csr* A, int trans, int32_t* tile_row_host,
+                        int32_t* tile_nz_host);
+
+/* ---- products ----
+ * y = alpha*op(A)*x + beta*y, op(A) = A (trans=0) or A^T (trans=1).
+ * beta == 0 never reads y. Replaces IComputeBackend::spmv
+ * (gpu_backend.hpp:30-34; CudaDriverBackend::launch_spmv gpu_backend.cpp:395-443)
+ * and, for trans=1, SparseMatrix::transpose_multiply / the IPM's matvec_t
+ * (sparse_matrix.cpp:161-184, interior_point.cpp:61-69). */
+int hn_spmv(const hn_csr* A, int trans, double alpha, const double* x_dev, double beta,
+            double* y_dev, void* stream);
+/* Same product with host vectors, synchronous: copies x in and y out through
+ * pinned staging (IComputeBackend::spmv's calling convention). */
+int hn_spmv_host(const hn_csr* A, int trans, const double* x_host, double* y_host);
+/* C = op(A) * B with B row-major (cols(op A) x k) and C (rows(op A) x k)
+ * overwritten (IComputeBackend::spmm, gpu_backend.hpp:36-41, gpu_backend.cpp:445-487). */
+int hn_spmm(const hn_csr* A, int trans, const double* B_dev, int64_t k, double* C_dev,
+            void* stream);
+int hn_spmm_host(const hn_csr* A, int trans, const double* B_host, int64_t k, double* C_host);
+
+/* ---- BLAS-1 on device vectors; scalar results go to a device double ----
+ * (IComputeBackend::dot/axpy/norm_inf, gpu_backend.hpp:43-45; the reference's
+ * CUDA path ran these on the host, gpu_backend.cpp:236-248) */
+int hn_dot(int64_t n, const double* a_dev, const double* b_dev, double* result_dev,
+           void* stream);
+int hn_axpy(int64_t n, double alpha, const double* x_dev, double* y_dev, void* stream);
+/* max |v_i|, NaN entries ignored (std::max semantics of the reference). */
+int hn_nrm_inf(int64_t n, const double* v_dev, double* result_dev, void* stream);
+int hn_nrm2(int64_t n, const double* v_dev, double* result_dev, void* stream);
+
+/* ---- normal equations N = A diag(d) A^T + dyn_reg I ----
+ * (build_normal_equations, interior_point.cpp:144-200)
+ * Symbolic: the pattern of A A^T plus the full diagonal, both triangles,
+ * columns sorted (the pattern the reference builds when every d_j > 0).
+ * Needs the handle's A^T. m up to 1,500,000. */
+int hn_ada_symbolic(const hn_csr* A, hn_pattern** out);
+int hn_pattern_info(const hn_pattern* P, int64_t* m, int64_t* nnz);
+/* Host copy of the pattern: rp m+1, ci nnz (reference layout). */
+int hn_pattern_export(const hn_pattern* P, uint64_t* rp_host, uint64_t* ci_host);
+/* Device arrays of the pattern: rp (int64, m+1), ci (int32, nnz), diag_pos
+ * (int64, m: position of (i,i) in ci). */
+int hn_pattern_device(const hn_pattern* P, const int64_t** rp_dev, const int32_t** ci_dev,
+                      const int64_t** diag_pos_dev);
+/* Numeric: nval_dev[p] for every pattern position; columns with d_j <= 0 add
+ * nothing (their entries stay explicit zeros); each term is
+ * (a_ij * a_kj) * d_j, summed per entry in column order; the diagonal then
+ * gains dyn_reg = max(reg, 1e-12 * max_i sum_j a_ij^2 d_j). dyn_reg_dev
+ * (device double, may be NULL) receives dyn_reg. */
+int hn_ada_numeric(const hn_pattern* P, const double* d_dev, double reg, double* nval_dev,
+                   double* dyn_reg_dev, void* stream);
+int hn_pattern_destroy(hn_pattern* P);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HN_SM100_H */

@@ -1,0 +1,87 @@
+"""Build recipe for the sm_100a library (libhn_sm100.so) and its host C++ layer.
+
+Compiles every CUDA source under csrc/ with nvcc for sm_100a only
+(-gencode arch=compute_100a,code=sm_100a), links one shared library in-tree
+next to this file, and builds the host C++ solver library (libhn_host.so)
+that sits above the C ABI. Run `python build.py` or call build().
+"""
+from __future__ import annotations
+
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+INCLUDE = os.path.join(ROOT, "include")
+CSRC = os.path.join(HERE, "csrc")
+HOST = os.path.join(HERE, "host")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libhn_sm100.so")
+HOSTLIB = os.path.join(HERE, "libhn_host.so")
+
+NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+           "-I", INCLUDE, "-I", CSRC]
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout)
+        raise RuntimeError("build step failed: " + " ".join(cmd))
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_cuda(verbose: bool = False, ptxas_info: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(INCLUDE, "hn_sm100.h")]
+    objs = []
+    for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
+        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+        objs.append(obj)
+        if _stale(obj, [src] + headers) or ptxas_info:
+            cmd = [NVCC, *ARCH, *NVFLAGS, "-c", src, "-o", obj]
+            if ptxas_info:
+                cmd.insert(1, "-Xptxas=-v")
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
+    if _stale(LIB, objs):
+        _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"])
+    return LIB
+
+
+def build_host(verbose: bool = False) -> str | None:
+    srcs = sorted(glob.glob(os.path.join(HOST, "*.cpp")))
+    if not srcs:
+        return None
+    hdrs = glob.glob(os.path.join(HOST, "*.hpp")) + [os.path.join(INCLUDE, "hn_sm100.h")]
+    if _stale(HOSTLIB, srcs + hdrs + [LIB]):
+        cxx = os.environ.get("CXX", "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++")
+        cmd = [cxx, "-O3", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-march=x86-64-v3",
+               "-ffp-contract=off", "-I", INCLUDE, "-I", HOST, *srcs, "-o", HOSTLIB,
+               "-L", HERE, "-lhn_sm100", "-Wl,-rpath,$ORIGIN", "-lpthread"]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
+    return HOSTLIB
+
+
+def build(verbose: bool = False) -> None:
+    build_cuda(verbose)
+    build_host(verbose)
+
+
+if __name__ == "__main__":
+    build(verbose="-v" in sys.argv)
+    print(LIB)

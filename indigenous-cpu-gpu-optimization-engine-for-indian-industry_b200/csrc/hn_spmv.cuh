@@ -1,0 +1,202 @@
+// Merge-path FP64 CSR SpMV with a fused per-row epilogue.
+//
+// The merge path is the interleaving of the m row ends (rp[1..m]) with the
+// nnz nonzero indices; it is cut into tiles of kSpmvTile items so every CTA
+// does the same amount of work whatever the row-length distribution (the
+// Zipf-skewed A^T rows of the large configuration and the Poisson rows of A
+// alike). Inside a tile each thread walks kSpmvIpt consecutive items.
+//
+// Per tile: coalesced loads of col_idx/values (L1 no-allocate: they stream
+// once) and gathers of x (cached) fill a shared-memory product buffer; the
+// threads walk their items, finishing rows that end in their range; partial
+// rows are combined through a shared carry array in thread order. A row that
+// began in an earlier tile leaves its in-tile part in head_val and is
+// finished by a second, tiny kernel that adds the earlier tiles' carries in
+// tile order. Every row's sum therefore has a fixed association order, so
+// results are deterministic run to run.
+//
+// Epilogues receive (row, sum) exactly once per row and write the outputs
+// (y = alpha*s + beta*y, residuals, IPM directions ...).
+#pragma once
+
+#include "hn_internal.cuh"
+
+namespace hn {
+
+constexpr int kSpmvThreads = 256;
+constexpr int kSpmvIpt = 8;
+constexpr int kSpmvTile = kSpmvThreads * kSpmvIpt;
+
+struct SpmvMat {
+    int m, nnz;
+    const int32_t* rp;
+    const int32_t* ci;
+    const double* val;
+    const int32_t* tile_row;
+    const int32_t* tile_nz;
+    int32_t* carry_row;
+    double* carry_val;
+    int32_t* head_row;
+    double* head_val;
+    int64_t ntiles;
+};
+
+inline SpmvMat spmv_mat(const hn_csr* A, int trans) {
+    SpmvMat M;
+    if (!trans) {
+        M = SpmvMat{(int)A->m, (int)A->nnz, A->rp, A->ci, A->val, A->tile_row, A->tile_nz,
+                    A->carry_row, A->carry_val, A->head_row, A->head_val, A->ntiles};
+    } else {
+        M = SpmvMat{(int)A->n, (int)A->nnz_t, A->rpT, A->ciT, A->valT, A->tile_row_t, A->tile_nz_t,
+                    A->carry_row_t, A->carry_val_t, A->head_row_t, A->head_val_t, A->ntiles_t};
+    }
+    return M;
+}
+
+template <class Epi>
+__global__ void __launch_bounds__(kSpmvThreads) spmv_tile_kernel(SpmvMat a, const double* __restrict__ x,
+                                                                 Epi epi) {
+    __shared__ double s_prod[kSpmvTile];
+    __shared__ int32_t s_rowend[kSpmvTile + 1];
+    __shared__ int32_t s_crow[kSpmvThreads];
+    __shared__ double s_cval[kSpmvThreads];
+    __shared__ int32_t s_rowstart0;
+
+    const int tid = threadIdx.x;
+    const int tile = blockIdx.x;
+    const int r0 = a.tile_row[tile], k0 = a.tile_nz[tile];
+    const int r1 = a.tile_row[tile + 1], k1 = a.tile_nz[tile + 1];
+    const int nrows_t = r1 - r0;
+    const int nnz_t = k1 - k0;
+
+    if (tid == 0) {
+        s_rowstart0 = (r0 < a.m) ? a.rp[r0] : a.nnz;
+        a.head_row[tile] = -1;
+    }
+    for (int i = tid; i <= nrows_t; i += kSpmvThreads) {
+        const int r = r0 + i;
+        s_rowend[i] = (r < a.m) ? __ldg(a.rp + r + 1) : INT_MAX;
+    }
+    {
+        int cidx[kSpmvIpt];
+        double v[kSpmvIpt];
+#pragma unroll
+        for (int u = 0; u < kSpmvIpt; ++u) {
+            const int i = tid + u * kSpmvThreads;
+            if (i < nnz_t) {
+                cidx[u] = ld_stream(a.ci + k0 + i);
+                v[u] = ld_stream(a.val + k0 + i);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kSpmvIpt; ++u) {
+            const int i = tid + u * kSpmvThreads;
+            if (i < nnz_t) s_prod[i] = v[u] * __ldg(x + cidx[u]);
+        }
+    }
+    __syncthreads();
+
+    const int total_t = nrows_t + nnz_t;
+    int diag = tid * kSpmvIpt;
+    if (diag > total_t) diag = total_t;
+    int diag_end = diag + kSpmvIpt;
+    if (diag_end > total_t) diag_end = total_t;
+    int lo = diag - nnz_t > 0 ? diag - nnz_t : 0;
+    int hi = diag < nrows_t ? diag : nrows_t;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (s_rowend[mid] <= k0 + diag - mid - 1)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    int row = lo;
+    int nz = diag - lo;
+    double sum = 0.0;
+    int first_row = -1;
+    double first_val = 0.0;
+    for (int it = diag; it < diag_end; ++it) {
+        const bool take_nz = (nz < nnz_t) && (k0 + nz < s_rowend[row]);
+        if (take_nz) {
+            sum += s_prod[nz];
+            ++nz;
+        } else {
+            if (row >= nrows_t) break;  // unreachable on a consistent tile table
+            if (first_row < 0) {
+                first_row = row;
+                first_val = sum;
+            } else {
+                epi(r0 + row, sum);
+            }
+            sum = 0.0;
+            ++row;
+        }
+    }
+    s_crow[tid] = row;
+    s_cval[tid] = sum;
+    __syncthreads();
+
+    if (first_row >= 0) {
+        int t = tid - 1;
+        while (t >= 0 && s_crow[t] == first_row) --t;
+        double acc = 0.0;
+        for (int u = t + 1; u < tid; ++u) acc += s_cval[u];
+        acc += first_val;
+        if (t < 0 && first_row == 0 && k0 > s_rowstart0) {
+            a.head_row[tile] = r0;
+            a.head_val[tile] = acc;
+        } else {
+            epi(r0 + first_row, acc);
+        }
+    }
+    if (tid == kSpmvThreads - 1) {
+        const int crow = s_crow[tid];
+        if (r0 + crow < a.m) {
+            int t = tid;
+            while (t >= 0 && s_crow[t] == crow) --t;
+            double acc = 0.0;
+            for (int u = t + 1; u <= tid; ++u) acc += s_cval[u];
+            a.carry_row[tile] = r0 + crow;
+            a.carry_val[tile] = acc;
+        } else {
+            a.carry_row[tile] = -1;
+        }
+    }
+}
+
+template <class Epi>
+__global__ void spmv_fixup_kernel(SpmvMat a, Epi epi) {
+    const int64_t tile = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (tile >= a.ntiles) return;
+    const int r = a.head_row[tile];
+    if (r < 0) return;
+    int64_t s = tile - 1;
+    while (s >= 0 && a.carry_row[s] == r) --s;
+    double acc = 0.0;
+    for (int64_t u = s + 1; u < tile; ++u) acc += a.carry_val[u];
+    acc += a.head_val[tile];
+    epi(r, acc);
+}
+
+// Launches the two kernels of one product on `s`.
+template <class Epi>
+void spmv_launch(const SpmvMat& M, const double* x, const Epi& epi, cudaStream_t s) {
+    if (M.ntiles == 0) return;
+    spmv_tile_kernel<Epi><<<(unsigned)M.ntiles, kSpmvThreads, 0, s>>>(M, x, epi);
+    launched("spmv_tile_kernel");
+    if (M.ntiles > 1) {
+        spmv_fixup_kernel<Epi><<<(unsigned)((M.ntiles + 255) / 256), 256, 0, s>>>(M, epi);
+        launched("spmv_fixup_kernel");
+    }
+}
+
+// ---- epilogues ----
+struct EpiAxpby {
+    double alpha, beta;
+    double* y;
+    __device__ __forceinline__ void operator()(int r, double s) const {
+        y[r] = (beta == 0.0) ? alpha * s : alpha * s + beta * y[r];
+    }
+};
+
+}  // namespace hn

@@ -1,0 +1,284 @@
+"""ctypes binding of libhn_sm100.so (include/hn_sm100.h) for Python callers.
+
+The binding is thin: every call goes straight to the C ABI, device buffers
+are passed as raw pointers (e.g. torch.Tensor.data_ptr()), host arrays as
+numpy arrays. A missing or unloadable library raises -- there is no CPU
+fallback anywhere on this path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhn_sm100.so")
+HOST_LIB_PATH = os.path.join(HERE, "libhn_host.so")
+
+HN_OK = 0
+HN_ERR_INVALID_ARG = 1
+HN_ERR_CUDA = 2
+HN_ERR_OUT_OF_MEMORY = 3
+HN_ERR_NOT_INITIALIZED = 4
+HN_ERR_UNSUPPORTED = 5
+HN_ERR_NUMERICAL = 6
+HN_ERR_INJECTED = 7
+HN_CSR_NO_TRANSPOSE = 1
+
+_i64, _u64p, _f64p, _vp, _i32p = C.c_int64, C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+
+
+class HnError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class DeviceInfo(C.Structure):
+    _fields_ = [("name", C.c_char * 256), ("device", C.c_int), ("sm_count", C.c_int),
+                ("cc_major", C.c_int), ("cc_minor", C.c_int), ("total_mem", C.c_size_t),
+                ("free_mem", C.c_size_t)]
+
+
+# name -> argtypes (restype is int status unless listed in _RESTYPE)
+SIGNATURES = {
+    "hn_init": [C.c_int],
+    "hn_shutdown": [],
+    "hn_last_error": [],
+    "hn_device_info": [C.POINTER(DeviceInfo)],
+    "hn_stats": [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+    "hn_reset_stats": [],
+    "hn_fault_inject": [_i64, C.c_int],
+    "hn_malloc": [C.POINTER(C.c_void_p), C.c_size_t],
+    "hn_free": [_vp],
+    "hn_memcpy_h2d": [_vp, _vp, C.c_size_t, _vp],
+    "hn_memcpy_d2h": [_vp, _vp, C.c_size_t, _vp],
+    "hn_memcpy_d2d": [_vp, _vp, C.c_size_t, _vp],
+    "hn_memset": [_vp, C.c_int, C.c_size_t, _vp],
+    "hn_stream_sync": [_vp],
+    "hn_csr_create": [_i64, _i64, _u64p, _u64p, _f64p, C.c_uint, C.POINTER(_vp)],
+    "hn_csr_set_values": [_vp, _f64p],
+    "hn_csr_destroy": [_vp],
+    "hn_csr_shape": [_vp, _i64p, _i64p, _i64p, _i64p],
+    "hn_csr_export": [_vp, C.c_int, _u64p, _u64p, _f64p],
+    "hn_csr_tiles": [_vp, C.c_int, _i64p, _i64p],
+    "hn_csr_export_tiles": [_vp, C.c_int, _i32p, _i32p],
+    "hn_spmv": [_vp, C.c_int, C.c_double, _vp, C.c_double, _vp, _vp],
+    "hn_spmv_host": [_vp, C.c_int, _f64p, _f64p],
+    "hn_spmm": [_vp, C.c_int, _vp, _i64, _vp, _vp],
+    "hn_spmm_host": [_vp, C.c_int, _f64p, _i64, _f64p],
+    "hn_dot": [_i64, _vp, _vp, _vp, _vp],
+    "hn_axpy": [_i64, C.c_double, _vp, _vp, _vp],
+    "hn_nrm_inf": [_i64, _vp, _vp, _vp],
+    "hn_nrm2": [_i64, _vp, _vp, _vp],
+    "hn_ada_symbolic": [_vp, C.POINTER(_vp)],
+    "hn_pattern_info": [_vp, _i64p, _i64p],
+    "hn_pattern_export": [_vp, _u64p, _u64p],
+    "hn_pattern_device": [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)],
+    "hn_ada_numeric": [_vp, _vp, C.c_double, _vp, _vp, _vp],
+    "hn_pattern_destroy": [_vp],
+}
+_RESTYPE = {"hn_last_error": C.c_char_p}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load the library once and declare every exported signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with build.py (no CPU fallback exists)")
+    lib = C.CDLL(path)
+    for name, args in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = _RESTYPE.get(name, C.c_int)
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    if status != HN_OK:
+        raise HnError(status, load().hn_last_error().decode(errors="replace"))
+
+
+def _p(a: np.ndarray, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def u64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def init(device: int = 0) -> None:
+    check(load().hn_init(device))
+
+
+def device_info() -> DeviceInfo:
+    d = DeviceInfo()
+    check(load().hn_device_info(C.byref(d)))
+    return d
+
+
+def stats() -> tuple[int, int]:
+    a, b = C.c_uint64(), C.c_uint64()
+    check(load().hn_stats(C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+def reset_stats() -> None:
+    check(load().hn_reset_stats())
+
+
+def fault_inject(after_calls: int, status: int) -> None:
+    check(load().hn_fault_inject(after_calls, status))
+
+
+def _ptr(t) -> int | None:
+    """Device pointer of a torch tensor / int / None."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+class Csr:
+    """Device-resident CSR matrix handle (hn_csr)."""
+
+    def __init__(self, m: int, n: int, rp, ci, val, transpose: bool = True):
+        self.m, self.n = int(m), int(n)
+        self._rp, self._ci, self._val = u64(rp), u64(ci), f64(val)
+        h = C.c_void_p()
+        flags = 0 if transpose else HN_CSR_NO_TRANSPOSE
+        check(load().hn_csr_create(self.m, self.n, _p(self._rp, C.c_uint64), _p(self._ci, C.c_uint64),
+                                   _p(self._val, C.c_double), flags, C.byref(h)))
+        self.h = h
+        m_, n_, nnz, nnzt = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        check(load().hn_csr_shape(h, C.byref(m_), C.byref(n_), C.byref(nnz), C.byref(nnzt)))
+        self.nnz, self.nnz_t = nnz.value, nnzt.value
+
+    def set_values(self, val) -> None:
+        self._val = f64(val)
+        check(load().hn_csr_set_values(self.h, _p(self._val, C.c_double)))
+        m_, n_, nnz, nnzt = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        check(load().hn_csr_shape(self.h, C.byref(m_), C.byref(n_), C.byref(nnz), C.byref(nnzt)))
+        self.nnz_t = nnzt.value
+
+    def close(self) -> None:
+        if self.h:
+            check(load().hn_csr_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and _lib is not None:
+                _lib.hn_csr_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def spmv(self, x, y, trans: int = 0, alpha: float = 1.0, beta: float = 0.0, stream=None) -> None:
+        check(load().hn_spmv(self.h, trans, alpha, _ptr(x), beta, _ptr(y), _ptr(stream)))
+
+    def spmv_host(self, x, trans: int = 0) -> np.ndarray:
+        x = f64(x)
+        y = np.empty(self.n if trans else self.m, dtype=np.float64)
+        check(load().hn_spmv_host(self.h, trans, _p(x, C.c_double), _p(y, C.c_double)))
+        return y
+
+    def spmm(self, B, k: int, Cout, trans: int = 0, stream=None) -> None:
+        check(load().hn_spmm(self.h, trans, _ptr(B), k, _ptr(Cout), _ptr(stream)))
+
+    def spmm_host(self, B, k: int, trans: int = 0) -> np.ndarray:
+        B = f64(B)
+        rows = self.n if trans else self.m
+        Cout = np.empty(rows * k, dtype=np.float64)
+        check(load().hn_spmm_host(self.h, trans, _p(B, C.c_double), k, _p(Cout, C.c_double)))
+        return Cout
+
+    def export(self, trans: int = 0):
+        rows = self.n if trans else self.m
+        nnz = self.nnz_t if trans else self.nnz
+        rp = np.empty(rows + 1, dtype=np.uint64)
+        ci = np.empty(max(nnz, 1), dtype=np.uint64)
+        val = np.empty(max(nnz, 1), dtype=np.float64)
+        check(load().hn_csr_export(self.h, trans, _p(rp, C.c_uint64), _p(ci, C.c_uint64),
+                                   _p(val, C.c_double)))
+        return rp, ci[:nnz], val[:nnz]
+
+    def tiles(self, trans: int = 0):
+        nt, items = C.c_int64(), C.c_int64()
+        check(load().hn_csr_tiles(self.h, trans, C.byref(nt), C.byref(items)))
+        row = np.empty(nt.value + 1, dtype=np.int32)
+        nz = np.empty(nt.value + 1, dtype=np.int32)
+        check(load().hn_csr_export_tiles(self.h, trans, _p(row, C.c_int32), _p(nz, C.c_int32)))
+        return items.value, row, nz
+
+
+class Pattern:
+    """Fixed pattern of A diag(d) A^T + reg I (hn_pattern)."""
+
+    def __init__(self, A: Csr):
+        h = C.c_void_p()
+        check(load().hn_ada_symbolic(A.h, C.byref(h)))
+        self.h = h
+        self.A = A
+        m, nnz = C.c_int64(), C.c_int64()
+        check(load().hn_pattern_info(h, C.byref(m), C.byref(nnz)))
+        self.m, self.nnz = m.value, nnz.value
+
+    def export(self):
+        rp = np.empty(self.m + 1, dtype=np.uint64)
+        ci = np.empty(max(self.nnz, 1), dtype=np.uint64)
+        check(load().hn_pattern_export(self.h, _p(rp, C.c_uint64), _p(ci, C.c_uint64)))
+        return rp, ci[: self.nnz]
+
+    def device_arrays(self):
+        rp, ci, dp = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(load().hn_pattern_device(self.h, C.byref(rp), C.byref(ci), C.byref(dp)))
+        return rp.value, ci.value, dp.value
+
+    def numeric(self, d, reg: float, nval, dyn=None, stream=None) -> None:
+        check(load().hn_ada_numeric(self.h, _ptr(d), reg, _ptr(nval), _ptr(dyn), _ptr(stream)))
+
+    def close(self) -> None:
+        if self.h:
+            check(load().hn_pattern_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and _lib is not None:
+                _lib.hn_pattern_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def dot(n, a, b, out, stream=None) -> None:
+    check(load().hn_dot(n, _ptr(a), _ptr(b), _ptr(out), _ptr(stream)))
+
+
+def axpy(n, alpha, x, y, stream=None) -> None:
+    check(load().hn_axpy(n, alpha, _ptr(x), _ptr(y), _ptr(stream)))
+
+
+def nrm_inf(n, v, out, stream=None) -> None:
+    check(load().hn_nrm_inf(n, _ptr(v), _ptr(out), _ptr(stream)))
+
+
+def nrm2(n, v, out, stream=None) -> None:
+    check(load().hn_nrm2(n, _ptr(v), _ptr(out), _ptr(stream)))
+
+
+def exported_symbols() -> list[str]:
+    return list(SIGNATURES)

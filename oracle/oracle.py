@@ -1,0 +1,337 @@
+"""ctypes loaders for the two CPU checkers -- TEST INFRASTRUCTURE ONLY.
+
+  * port():  libhn_oracle.so, the C restatement in hn_oracle.c
+  * ref():   _ref/libhnref.so, the reference's own LP stack compiled from its
+             sources by the Makefile here (None when it was not built)
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "libhn_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libhnref.so")
+
+_i64 = C.c_int64
+_i64p = C.POINTER(C.c_int64)
+_u64p = C.POINTER(C.c_uint64)
+_f64p = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int32)
+
+_port = None
+_ref = None
+
+
+def build(ref: bool = True) -> None:
+    """make the port (always) and the reference build (when its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if ref and os.path.isdir(os.environ.get("REF", "/root/reference")):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def port():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_LIB):
+            build(ref=False)
+        lib = C.CDLL(PORT_LIB)
+        sig = {
+            "hno_csr_multiply": (None, [_i64, _i64p, _i64p, _f64p, _f64p, _f64p]),
+            "hno_csr_tmultiply": (None, [_i64, _i64, _i64p, _i64p, _f64p, _f64p, _f64p]),
+            "hno_matvec_t": (None, [_i64, _i64, _i64p, _i64p, _f64p, _f64p, _f64p]),
+            "hno_csr_transposed": (_i64, [_i64, _i64, _i64p, _i64p, _f64p, _i64p, _i64p, _f64p]),
+            "hno_spmm": (None, [_i64, _i64p, _i64p, _f64p, _f64p, _i64, _f64p]),
+            "hno_dot": (C.c_double, [_i64, _f64p, _f64p]),
+            "hno_axpy": (None, [_i64, C.c_double, _f64p, _f64p]),
+            "hno_norm_inf": (C.c_double, [_i64, _f64p]),
+            "hno_nrm2": (C.c_double, [_i64, _f64p]),
+            "hno_max_step": (C.c_double, [_i64, _f64p, _f64p]),
+            "hno_normal_equations_triplets": (_i64, [_i64, _i64, _i64p, _i64p, _f64p]),
+            "hno_normal_equations": (_i64, [_i64, _i64, _i64p, _i64p, _f64p, _f64p, C.c_double, _i64p,
+                                            _i64p, _f64p, _f64p]),
+            "hno_ada_pattern": (_i64, [_i64, _i64, _i64p, _i64p, _i64p, _i32p]),
+            "hno_merge_tiles": (None, [_i64, _i64, _i32p, _i64, _i64, _i32p, _i32p]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _port = lib
+    return _port
+
+
+def ref():
+    """The compiled reference, or None when oracle/_ref was not built."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_LIB):
+            return None
+        lib = C.CDLL(REF_LIB)
+        sig = {
+            "hnref_backend_spmv": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p]),
+            "hnref_backend_spmm": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _i64, _f64p]),
+            "hnref_backend_dot": (C.c_double, [_i64, _f64p, _f64p]),
+            "hnref_backend_axpy": (None, [_i64, C.c_double, _f64p, _f64p]),
+            "hnref_backend_norm_inf": (C.c_double, [_i64, _f64p]),
+            "hnref_multiply": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p]),
+            "hnref_tmultiply": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p]),
+            "hnref_transposed": (_i64, [_i64, _i64, _u64p, _u64p, _f64p, _u64p, _u64p, _f64p]),
+            "hnref_from_triplets": (_i64, [_i64, _i64, _i64, _u64p, _u64p, _f64p, _u64p, _u64p, _f64p]),
+            "hnref_cholesky_solve": (C.c_int, [_i64, _u64p, _u64p, _f64p, _f64p]),
+            "hnref_ipm_solve": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, _i32p, _f64p,
+                                          _f64p, C.c_int, C.c_int, C.c_int, _f64p, _i64p, _f64p, _f64p]),
+            "hnref_bench_spmv_pair": (C.c_double, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, C.c_int,
+                                                   C.c_int]),
+            "hnref_normal_equations": (_i64, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, C.c_double, _i64, _u64p,
+                                              _u64p, _f64p]),
+            "hnref_matvec_t": (None, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p]),
+            "hnref_max_step": (C.c_double, [_i64, _f64p, _f64p]),
+            "hnref_step_sample": (C.c_double, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, _f64p, _i64,
+                                               C.c_int, C.c_int, _i64p, _i64p]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _ref = lib
+    return _ref
+
+
+# ---------------------------------------------------------------- port wrappers
+def i64(a):
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def multiply(rp, ci, val, x):
+    rp, ci, val, x = i64(rp), i64(ci), f64(val), f64(x)
+    y = np.empty(rp.shape[0] - 1)
+    port().hno_csr_multiply(rp.shape[0] - 1, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(val, C.c_double),
+                            _p(x, C.c_double), _p(y, C.c_double))
+    return y
+
+
+def tmultiply(rp, ci, val, x, n):
+    rp, ci, val, x = i64(rp), i64(ci), f64(val), f64(x)
+    y = np.empty(n)
+    port().hno_csr_tmultiply(rp.shape[0] - 1, n, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(val, C.c_double),
+                             _p(x, C.c_double), _p(y, C.c_double))
+    return y
+
+
+def matvec_t(rp, ci, val, x, n):
+    rp, ci, val, x = i64(rp), i64(ci), f64(val), f64(x)
+    y = np.empty(n)
+    port().hno_matvec_t(rp.shape[0] - 1, n, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(val, C.c_double),
+                        _p(x, C.c_double), _p(y, C.c_double))
+    return y
+
+
+def transposed(rp, ci, val, n):
+    rp, ci, val = i64(rp), i64(ci), f64(val)
+    nnz = int(rp[-1])
+    rpT = np.empty(n + 1, dtype=np.int64)
+    ciT = np.empty(max(nnz, 1), dtype=np.int64)
+    valT = np.empty(max(nnz, 1))
+    w = port().hno_csr_transposed(rp.shape[0] - 1, n, _p(rp, C.c_int64), _p(ci, C.c_int64),
+                                  _p(val, C.c_double), _p(rpT, C.c_int64), _p(ciT, C.c_int64),
+                                  _p(valT, C.c_double))
+    return rpT, ciT[:w], valT[:w]
+
+
+def spmm(rp, ci, val, B, k):
+    rp, ci, val, B = i64(rp), i64(ci), f64(val), f64(B)
+    m = rp.shape[0] - 1
+    Cm = np.empty(m * k)
+    port().hno_spmm(m, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(val, C.c_double), _p(B, C.c_double), k,
+                    _p(Cm, C.c_double))
+    return Cm
+
+
+def dot(a, b):
+    a, b = f64(a), f64(b)
+    return port().hno_dot(a.shape[0], _p(a, C.c_double), _p(b, C.c_double))
+
+
+def norm_inf(v):
+    v = f64(v)
+    return port().hno_norm_inf(v.shape[0], _p(v, C.c_double))
+
+
+def nrm2(v):
+    v = f64(v)
+    return port().hno_nrm2(v.shape[0], _p(v, C.c_double))
+
+
+def axpy(alpha, x, y):
+    x, y = f64(x), f64(y).copy()
+    port().hno_axpy(x.shape[0], alpha, _p(x, C.c_double), _p(y, C.c_double))
+    return y
+
+
+def max_step(v, d):
+    v, d = f64(v), f64(d)
+    return port().hno_max_step(v.shape[0], _p(v, C.c_double), _p(d, C.c_double))
+
+
+def normal_equations(rp, ci, val, D, reg, n):
+    rp, ci, val, D = i64(rp), i64(ci), f64(val), f64(D)
+    m = rp.shape[0] - 1
+    nt = port().hno_normal_equations_triplets(m, n, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(D, C.c_double))
+    rpN = np.empty(m + 1, dtype=np.int64)
+    ciN = np.empty(max(nt, 1), dtype=np.int64)
+    valN = np.empty(max(nt, 1))
+    dyn = C.c_double()
+    w = port().hno_normal_equations(m, n, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(val, C.c_double),
+                                    _p(D, C.c_double), reg, _p(rpN, C.c_int64), _p(ciN, C.c_int64),
+                                    _p(valN, C.c_double), C.byref(dyn))
+    return rpN, ciN[:w], valN[:w], dyn.value
+
+
+def ada_pattern(rp, ci, n):
+    rp, ci = i64(rp), i64(ci)
+    m = rp.shape[0] - 1
+    rpN = np.empty(m + 1, dtype=np.int64)
+    total = port().hno_ada_pattern(m, n, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(rpN, C.c_int64), None)
+    ciN = np.empty(max(total, 1), dtype=np.int32)
+    port().hno_ada_pattern(m, n, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(rpN, C.c_int64), _p(ciN, C.c_int32))
+    return rpN, ciN[:total]
+
+
+def merge_tiles(rp32, nnz, items, ntiles):
+    rp32 = np.ascontiguousarray(rp32, dtype=np.int32)
+    row = np.empty(ntiles + 1, dtype=np.int32)
+    nz = np.empty(ntiles + 1, dtype=np.int32)
+    port().hno_merge_tiles(rp32.shape[0] - 1, nnz, _p(rp32, C.c_int32), items, ntiles, _p(row, C.c_int32),
+                           _p(nz, C.c_int32))
+    return row, nz
+
+
+# ---------------------------------------------------------------- reference wrappers
+def u64(a):
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def ref_multiply(rp, ci, val, x):
+    rp, ci, val, x = u64(rp), u64(ci), f64(val), f64(x)
+    y = np.empty(rp.shape[0] - 1)
+    ref().hnref_multiply(rp.shape[0] - 1, x.shape[0], _p(rp, C.c_uint64), _p(ci, C.c_uint64),
+                         _p(val, C.c_double), _p(x, C.c_double), _p(y, C.c_double))
+    return y
+
+
+def ref_backend_spmv(rp, ci, val, x):
+    rp, ci, val, x = u64(rp), u64(ci), f64(val), f64(x)
+    y = np.empty(rp.shape[0] - 1)
+    ref().hnref_backend_spmv(rp.shape[0] - 1, x.shape[0], _p(rp, C.c_uint64), _p(ci, C.c_uint64),
+                             _p(val, C.c_double), _p(x, C.c_double), _p(y, C.c_double))
+    return y
+
+
+def ref_tmultiply(rp, ci, val, x, n):
+    rp, ci, val, x = u64(rp), u64(ci), f64(val), f64(x)
+    y = np.empty(n)
+    ref().hnref_tmultiply(rp.shape[0] - 1, n, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
+                          _p(x, C.c_double), _p(y, C.c_double))
+    return y
+
+
+def ref_transposed(rp, ci, val, n):
+    rp, ci, val = u64(rp), u64(ci), f64(val)
+    nnz = int(rp[-1])
+    rpT = np.empty(n + 1, dtype=np.uint64)
+    ciT = np.empty(max(nnz, 1), dtype=np.uint64)
+    valT = np.empty(max(nnz, 1))
+    w = ref().hnref_transposed(rp.shape[0] - 1, n, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
+                               _p(rpT, C.c_uint64), _p(ciT, C.c_uint64), _p(valT, C.c_double))
+    return rpT, ciT[:w], valT[:w]
+
+
+def ref_from_triplets(rows, cols, ti, tj, tv):
+    ti, tj, tv = u64(ti), u64(tj), f64(tv)
+    rp = np.empty(rows + 1, dtype=np.uint64)
+    ci = np.empty(max(ti.shape[0], 1), dtype=np.uint64)
+    val = np.empty(max(ti.shape[0], 1))
+    w = ref().hnref_from_triplets(rows, cols, ti.shape[0], _p(ti, C.c_uint64), _p(tj, C.c_uint64),
+                                  _p(tv, C.c_double), _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double))
+    return rp, ci[:w], val[:w]
+
+
+def ref_backend_spmm(rp, ci, val, B, k, n):
+    rp, ci, val, B = u64(rp), u64(ci), f64(val), f64(B)
+    m = rp.shape[0] - 1
+    Cm = np.empty(m * k)
+    ref().hnref_backend_spmm(m, n, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
+                             _p(B, C.c_double), k, _p(Cm, C.c_double))
+    return Cm
+
+
+def ref_ipm_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, max_iter=0, crossover=False):
+    """InteriorPointSolver::solve on the LP (rows EQ and x >= 0 by default)."""
+    m, n = lp["m"], lp["n"]
+    rp, ci, val = u64(lp["rp"]), u64(lp["ci"]), f64(lp["val"])
+    c, b = f64(lp["c"]), f64(lp["b"])
+    sense = np.ascontiguousarray(np.full(m, 2) if sense is None else sense, dtype=np.int32)
+    lb = f64(np.zeros(n) if lb is None else lb)
+    ub = f64(np.full(n, np.inf) if ub is None else ub)
+    obj, iters, tms = C.c_double(), C.c_int64(), C.c_double()
+    x = np.zeros(n)
+    st = ref().hnref_ipm_solve(m, n, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
+                               _p(c, C.c_double), _p(b, C.c_double), _p(sense, C.c_int32), _p(lb, C.c_double),
+                               _p(ub, C.c_double), int(maximize), int(max_iter), int(crossover), C.byref(obj),
+                               C.byref(iters), C.byref(tms), _p(x, C.c_double))
+    return {"status": st, "objective": obj.value, "iterations": iters.value, "time_ms": tms.value, "x": x}
+
+
+def ref_normal_equations(rp, ci, val, D, reg, n):
+    """build_normal_equations itself (interior_point.cpp:144-200)."""
+    rp, ci, val, D = u64(rp), u64(ci), f64(val), f64(D)
+    m = rp.shape[0] - 1
+    rpN = np.empty(m + 1, dtype=np.uint64)
+    nnz = ref().hnref_normal_equations(m, n, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
+                                       _p(D, C.c_double), reg, 0, _p(rpN, C.c_uint64), None, None)
+    ciN = np.empty(max(nnz, 1), dtype=np.uint64)
+    vN = np.empty(max(nnz, 1))
+    ref().hnref_normal_equations(m, n, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
+                                 _p(D, C.c_double), reg, nnz, _p(rpN, C.c_uint64), _p(ciN, C.c_uint64),
+                                 _p(vN, C.c_double))
+    return rpN, ciN[:nnz], vN[:nnz]
+
+
+def ref_matvec_t(rp, ci, val, x, n):
+    rp, ci, val, x = u64(rp), u64(ci), f64(val), f64(x)
+    y = np.empty(n)
+    ref().hnref_matvec_t(rp.shape[0] - 1, n, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
+                         _p(x, C.c_double), _p(y, C.c_double))
+    return y
+
+
+def ref_max_step(v, d):
+    v, d = f64(v), f64(d)
+    return ref().hnref_max_step(v.shape[0], _p(v, C.c_double), _p(d, C.c_double))
+
+
+def ref_step_sample(lp, x, lam, D, ncols_sample, threads, reps):
+    """Reference CPU pass (spmv, matvec_t, build_normal_equations on column
+    slices) on `threads` host threads; returns (seconds, triplets, nnz(N))."""
+    rp, ci, val = u64(lp["rp"]), u64(lp["ci"]), f64(lp["val"])
+    x, lam, D = f64(x), f64(lam), f64(D)
+    trip, nnzn = C.c_int64(), C.c_int64()
+    secs = ref().hnref_step_sample(lp["m"], lp["n"], _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
+                                   _p(x, C.c_double), _p(lam, C.c_double), _p(D, C.c_double), int(ncols_sample),
+                                   int(threads), int(reps), C.byref(trip), C.byref(nnzn))
+    return secs, trip.value, nnzn.value

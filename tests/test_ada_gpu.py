@@ -1,0 +1,130 @@
+"""GPU: A diag(d) A^T assembly against build_normal_equations
+(core/lp/interior_point.cpp:144-200) restated by the oracle and, for one
+case, assembled by the reference's own from_triplets (golden fixture).
+
+Pattern: bit-exact. Values: |N_ik - ref_ik| <= 1e-12 * (|A| D |A|^T)_ik + the
+regularisation term (the reference sums duplicate triplets in an order its
+std::sort leaves open). dyn_reg: exactly equal (the diagonal is summed in
+the same column order on both sides).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import lpgen
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_golden.npz"))
+
+
+def assemble(hn, torch, lp, D, reg=1e-8):
+    A = hn.Csr(lp["m"], lp["n"], lp["rp"], lp["ci"], lp["val"])
+    P = hn.Pattern(A)
+    nval = torch.empty(P.nnz, dtype=torch.float64, device="cuda")
+    dyn = torch.empty(1, dtype=torch.float64, device="cuda")
+    Dd = torch.as_tensor(D, device="cuda")
+    P.numeric(Dd, reg, nval, dyn)
+    torch.cuda.synchronize()
+    rp, ci = P.export()
+    return A, P, rp.astype(np.int64), ci.astype(np.int64), nval.cpu().numpy(), float(dyn.item())
+
+
+def check_values(lp, D, reg, rp, ci, vals, dyn):
+    rpR, ciR, vR, dynR = O.normal_equations(lp["rp"], lp["ci"], lp["val"], D, reg, lp["n"])
+    _, _, absR, _ = O.normal_equations(lp["rp"], lp["ci"], np.abs(lp["val"]), D, 0.0, lp["n"])
+    assert dyn == dynR
+    # map reference entries into the device pattern (device pattern is a superset)
+    m = lp["m"]
+    key = np.repeat(np.arange(m), np.diff(rp)) * m + ci
+    keyR = np.repeat(np.arange(m), np.diff(rpR)) * m + ciR
+    pos = np.searchsorted(key, keyR)
+    assert np.array_equal(key[pos], keyR)
+    assert np.all(np.abs(vals[pos] - vR) <= 1e-12 * (absR + dynR))
+    extra = np.ones(key.shape[0], dtype=bool)
+    extra[pos] = False
+    assert np.all(vals[extra] == 0.0)  # entries only inactive columns reach stay explicit zeros
+
+
+@pytest.mark.parametrize("m,n,k,seed", [(200, 500, 8, 11), (2000, 5000, 8, 0), (529, 1322, 6, 7)])
+def test_pattern_and_values_all_active(hn, torch_cuda, m, n, k, seed):
+    lp = lpgen.scaled_problem(lpgen.lp_uniform(m, n, k, seed))
+    D = np.random.default_rng(seed).uniform(1e-3, 1e3, n)
+    A, P, rp, ci, vals, dyn = assemble(hn, torch_cuda, lp, D)
+    rpP, ciP = O.ada_pattern(lp["rp"], lp["ci"], n)
+    assert np.array_equal(rp, rpP) and np.array_equal(ci, ciP.astype(np.int64))
+    check_values(lp, D, 1e-8, rp, ci, vals, dyn)
+
+
+def test_inactive_columns_and_reference_golden(hn, torch_cuda):
+    lp = lpgen.scaled_problem(lpgen.lp_uniform(200, 500, 8, seed=11))
+    D = GOLD["ne_D"]  # every 9th column inactive (D_j = 0)
+    A, P, rp, ci, vals, dyn = assemble(hn, torch_cuda, lp, D)
+    assert dyn == GOLD["ne_dyn"][0]
+    check_values(lp, D, 1e-8, rp, ci, vals, dyn)
+    # against the reference's own assembly (from_triplets of its triplets)
+    m = 200
+    key = np.repeat(np.arange(m), np.diff(rp)) * m + ci
+    rpG, ciG, vG = GOLD["ne_rp"].astype(np.int64), GOLD["ne_ci"].astype(np.int64), GOLD["ne_val"]
+    keyG = np.repeat(np.arange(m), np.diff(rpG)) * m + ciG
+    pos = np.searchsorted(key, keyG)
+    assert np.array_equal(key[pos], keyG)
+    _, _, absR, _ = O.normal_equations(lp["rp"], lp["ci"], np.abs(lp["val"]), D, 0.0, 500)
+    assert np.all(np.abs(vals[pos] - vG) <= 1e-12 * (absR + dyn))
+
+
+def test_dynamic_regularisation_dominates(hn, torch_cuda):
+    lp = lpgen.scaled_problem(lpgen.lp_uniform(200, 500, 8, seed=3))
+    D = np.full(500, 1e9)  # 1e-12 * max diag >> reg
+    *_, rp, ci, vals, dyn = assemble(hn, torch_cuda, lp, D, reg=1e-8)
+    assert dyn > 1e-8
+    check_values(lp, D, 1e-8, rp, ci, vals, dyn)
+
+
+def test_repeat_numeric_is_deterministic(hn, torch_cuda):
+    lp = lpgen.scaled_problem(lpgen.lp_uniform(2000, 5000, 8, 0))
+    D = np.random.default_rng(1).uniform(0.1, 10, 5000)
+    A = hn.Csr(2000, 5000, lp["rp"], lp["ci"], lp["val"])
+    P = hn.Pattern(A)
+    Dd = torch_cuda.as_tensor(D, device="cuda")
+    outs = []
+    for _ in range(3):
+        nval = torch_cuda.empty(P.nnz, dtype=torch_cuda.float64, device="cuda")
+        P.numeric(Dd, 1e-8, nval)
+        outs.append(nval.cpu().numpy())
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
+
+
+def test_large_zipf_pattern_properties(hn, torch_cuda):
+    """Full 200k x 500k size: pattern symmetric with a full diagonal, and
+    N x == A (D (A^T x)) to rounding for random x (a size-independent check)."""
+    lp = lpgen.scaled_problem(lpgen.lp_zipf(seed=1000))
+    m, n = lp["m"], lp["n"]
+    torch = torch_cuda
+    A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
+    P = hn.Pattern(A)
+    D = torch.rand(n, dtype=torch.float64, device="cuda") + 0.5
+    nval = torch.empty(P.nnz, dtype=torch.float64, device="cuda")
+    dyn = torch.empty(1, dtype=torch.float64, device="cuda")
+    P.numeric(D, 1e-8, nval, dyn)
+    rp_d, ci_d, dp_d = P.device_arrays()
+    rp, ci = P.export()
+    rp = torch.as_tensor(rp.astype(np.int64), device="cuda")
+    ci = torch.as_tensor(ci.astype(np.int64), device="cuda")
+    Nt = torch.sparse_csr_tensor(rp, ci, nval, size=(m, m))
+    x = torch.randn(m, dtype=torch.float64, device="cuda")
+    y = (Nt @ x.unsqueeze(1)).squeeze(1)
+    t = torch.empty(n, dtype=torch.float64, device="cuda")
+    A.spmv(x, t, trans=1)
+    t *= D
+    z = torch.empty(m, dtype=torch.float64, device="cuda")
+    A.spmv(t, z, trans=0)
+    z += dyn * x
+    err = (y - z).abs().max().item()
+    scale = (Nt.abs() @ x.abs().unsqueeze(1)).abs().max().item()
+    assert err <= 1e-12 * scale * 10
+    # symmetry of the pattern: nnz per row equals nnz per column
+    row_cnt = torch.diff(rp)
+    col_cnt = torch.bincount(ci, minlength=m)
+    assert torch.equal(row_cnt, col_cnt)
