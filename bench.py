@@ -144,13 +144,15 @@ def run_ours(args, rank, world, local):
     sp = stream.cuda_stream
 
     names = ["spmv_A", "spmv_At", "reductions", "ada_numeric"]
-    ev = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for k in names}
-    acc = {k: 0.0 for k in names}
+    # one event pair per (step, kernel group): read after a single final sync,
+    # so no step waits on the host and per-kernel times are pure device time
+    ev = [{k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for k in names}
+          for _ in range(args.steps)]
 
-    def step(timed_kernels: bool):
+    def step(evs=None):
         def mark(k, i):
-            if timed_kernels:
-                ev[k][i].record(stream)
+            if evs is not None:
+                evs[k][i].record(stream)
 
         mark("spmv_A", 0)
         hn.check(hn.load().hn_memcpy_d2d(y.data_ptr(), b.data_ptr(), 8 * m, sp))
@@ -169,7 +171,7 @@ def run_ours(args, rank, world, local):
         mark("ada_numeric", 1)
 
     for _ in range(args.warmup):
-        step(False)
+        step()
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -179,23 +181,14 @@ def run_ours(args, rank, world, local):
     l0, _ = hn.stats()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        step(True)
-        # per-kernel times accumulate on the host between steps without syncing the stream
+    for i in range(args.steps):
+        step(ev[i])
     e1.record(stream)
     torch.cuda.synchronize()
     l1, _ = hn.stats()
     ms_total = e0.elapsed_time(e1)
     clk = clocks.stop()
-    # per-kernel breakdown: last step's events (a second, separate pass for the average)
-    for k in names:
-        acc[k] = ev[k][0].elapsed_time(ev[k][1])
-    kt = {k: 0.0 for k in names}
-    for _ in range(args.steps):
-        step(True)
-        torch.cuda.synchronize()
-        for k in names:
-            kt[k] += ev[k][0].elapsed_time(ev[k][1]) / args.steps
+    kt = {k: sum(ev[i][k][0].elapsed_time(ev[i][k][1]) for i in range(args.steps)) / args.steps for k in names}
     ms = ms_total / args.steps
     if world > 1:
         tt = torch.tensor([ms], dtype=f64, device=dev)
@@ -218,7 +211,7 @@ def run_ours(args, rank, world, local):
     def e2e_step():
         for dst, src, nb_ in ((x, hx, 8 * n), (z, hz, 8 * n), (lam, hl, 8 * m), (D, hD, 8 * n)):
             hn.check(lib.hn_memcpy_h2d(dst.data_ptr(), src.data_ptr(), nb_, sp))
-        step(False)
+        step()
         for dst, src, nb_ in ((hy, y, 8 * m), (ht, t, 8 * n), (hs, scal, 64)):
             hn.check(lib.hn_memcpy_d2h(dst.data_ptr(), src.data_ptr(), nb_, sp))
 

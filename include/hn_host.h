@@ -1,0 +1,73 @@
+/* hn_host -- host C++ layer above hn_sm100 (libhn_host.so), as a C ABI.
+ *
+ *  - hn_lp_solve: the GPU Mehrotra IPM (hn::lp::InteriorPointSolver), a
+ *    drop-in for HyperNova's lp::InteriorPointSolver::solve
+ *    (core/lp/interior_point.cpp:402-886) with crossover off.
+ *  - hn_be_*: hn::execution::B200Backend, the IComputeBackend implementation
+ *    (core/execution/gpu_backend.hpp:18-51) over std::vector arguments.
+ * Status codes are those of hn_sm100.h; hn_host_last_error() gives the text.
+ */
+#ifndef HN_HOST_H
+#define HN_HOST_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* InteriorPointOptions (core/lp/interior_point.hpp:16-27) */
+typedef struct hn_ipm_options {
+    int max_iterations;          /* 100 */
+    double time_limit_seconds;   /* 0 = none */
+    double convergence_tol;      /* 1e-8 */
+    double complementarity_tol;  /* 1e-8 */
+    double regularization;       /* 1e-8 */
+    int device;                  /* 0 */
+    int verbose;                 /* 0 */
+    /* interrupt_callback: polled once per iteration; nonzero stops the solve
+     * with status INTERRUPTED (interior_point.cpp:490-493). May be NULL. */
+    int (*interrupt_cb)(void* user);
+    void* interrupt_user;
+} hn_ipm_options;
+
+/* InteriorPointResult (core/lp/interior_point.hpp:29-38) plus phase times;
+ * status uses model::ProblemStatus numbering (core/model/problem.hpp:35-45). */
+typedef struct hn_ipm_result {
+    int status;
+    int64_t iterations;
+    double objective;
+    double solve_time_ms;
+    double device_ms;
+    double factor_ms;
+    double solve_ms;
+    int64_t nnz_normal;
+} hn_ipm_result;
+
+void hn_ipm_default_options(hn_ipm_options* opt);
+/* min/max c^T x + obj_offset s.t. row i of A (sense 0 LE, 1 GE, 2 EQ) vs b_i,
+ * lb <= x <= ub; A as CSR in the reference layout. x_out (n) may be NULL. */
+int hn_lp_solve(int64_t m, int64_t n, const uint64_t* row_ptr, const uint64_t* col_idx, const double* val,
+                const double* c, const double* b, const int* sense, const double* lb, const double* ub,
+                int maximize, double obj_offset, const hn_ipm_options* opt, hn_ipm_result* res, double* x_out);
+const char* hn_host_last_error(void);
+
+/* B200Backend through C: the matrix arrives as the reference's three vectors
+ * each call; the backend keeps it resident between calls. */
+typedef struct hn_backend hn_backend;
+int hn_be_create(int device, hn_backend** out);
+int hn_be_destroy(hn_backend* be);
+int hn_be_spmv(hn_backend* be, int64_t m, int64_t nnz, const uint64_t* rp, const uint64_t* ci, const double* val,
+               int64_t nx, const double* x, double* y);
+int hn_be_spmv_t(hn_backend* be, int64_t m, int64_t n, int64_t nnz, const uint64_t* rp, const uint64_t* ci,
+                 const double* val, const double* x, double* y);
+int hn_be_spmm(hn_backend* be, int64_t m, int64_t nnz, const uint64_t* rp, const uint64_t* ci, const double* val,
+               int64_t nb, const double* B, int64_t k, double* C);
+int hn_be_dot(hn_backend* be, int64_t n, const double* a, const double* b, double* out);
+int hn_be_axpy(hn_backend* be, int64_t n, double alpha, const double* x, double* y);
+int hn_be_norm_inf(hn_backend* be, int64_t n, const double* v, double* out);
+int hn_be_kernel_executions(hn_backend* be, uint64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -167,6 +167,53 @@ int hn_ada_numeric(const hn_pattern* P, const double* d_dev, double reg, double*
                    double* dyn_reg_dev, void* stream);
 int hn_pattern_destroy(hn_pattern* P);
 
+/* ---- Mehrotra predictor-corrector iteration kernels ----
+ * (InteriorPointSolver::solve's loop, core/lp/interior_point.cpp:507-708)
+ * Device scalar block: double scal[HN_IPM_NSCAL]; the FLAGS slot holds uint64
+ * bits (1: a direction or dlam entry is not finite, :617-627 / :676-686;
+ * 2: the updated x or z has a negative or non-finite entry, :698-708). */
+#define HN_IPM_NRP 0   /* ||M x - b||_inf */
+#define HN_IPM_NRD 1   /* ||M^T lam + z - c||_inf */
+#define HN_IPM_MU 2    /* x^T z / n */
+#define HN_IPM_AP 3    /* primal step length */
+#define HN_IPM_AD 4    /* dual step length */
+#define HN_IPM_MUAFF 5 /* affine complementarity */
+#define HN_IPM_SIGMA 6 /* centring parameter */
+#define HN_IPM_FLAGS 7
+#define HN_IPM_NSCAL 8
+
+/* mx = M x; rp = mx - b; rd = M^T lam + z - c; then mu, ||rp||_inf,
+ * ||rd||_inf into scal, D = x / z clamped to (0, 1e10] and Drd = D rd
+ * (:507-539, :584). All vectors device, n = cols, m = rows. FLAGS bits are
+ * sticky: the caller clears the slot before a solve. */
+int hn_ipm_residuals(const hn_csr* M, const double* x_dev, const double* lam_dev, const double* z_dev,
+                     const double* b_dev, const double* c_dev, double* mx_dev, double* rp_dev,
+                     double* rd_dev, double* D_dev, double* Drd_dev, double* scal_dev, void* stream);
+/* rhs = -rp - M Drd + mx (normal-equation right-hand side, :585-600). */
+int hn_ipm_rhs(const hn_csr* M, const double* Drd_dev, const double* rp_dev, const double* mx_dev,
+               double* rhs_dev, void* stream);
+/* t = M^T dlam; dx = D (t + rd) - x (+ corr if non-null); dz = -(t + rd)
+ * (:607-615 predictor, :666-673 corrector). */
+int hn_ipm_direction(const hn_csr* M, const double* dlam_dev, const double* D_dev, const double* rd_dev,
+                     const double* x_dev, const double* corr_dev, double* dx_dev, double* dz_dev,
+                     void* stream);
+/* scal[AP] = max_step(x, dx), scal[AD] = max_step(z, dz) (:134-142) and the
+ * non-finite guard over dx, dz (n) and dlam (m) into FLAGS bit 1. */
+int hn_ipm_step_lengths(int64_t n, int64_t m, const double* x_dev, const double* dx_dev,
+                        const double* z_dev, const double* dz_dev, const double* dlam_dev,
+                        double* scal_dev, void* stream);
+/* mu_aff and sigma from the current steps (:632-643), zs = (sigma mu - dx dz)
+ * * (1/z) (:645-651) and rhs = rhs_pred - M zs (:652-659). */
+int hn_ipm_corrector(const hn_csr* M, const double* x_dev, const double* dx_dev, const double* z_dev,
+                     const double* dz_dev, const double* rhs_pred_dev, double* zs_dev, double* rhs_dev,
+                     double* scal_dev, void* stream);
+/* x += ap dx; z += ad dz; lam += ad dlam; guard into FLAGS bit 2 (:690-708). */
+int hn_ipm_update(int64_t n, int64_t m, double* x_dev, const double* dx_dev, double* z_dev,
+                  const double* dz_dev, double* lam_dev, const double* dlam_dev, double* scal_dev,
+                  void* stream);
+/* *result_dev = min(1, 0.99 * min_{d_i<0} -v_i/d_i) (max_step, :134-142). */
+int hn_max_step(int64_t n, const double* v_dev, const double* d_dev, double* result_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

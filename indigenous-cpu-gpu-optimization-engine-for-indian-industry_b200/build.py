@@ -24,7 +24,9 @@ HOSTLIB = os.path.join(HERE, "libhn_host.so")
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+# -fmad=false: every a*b+c rounds the product and the sum separately, as the
+# reference's x86-64 build does, so elementwise results match it bit for bit.
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
            "-I", INCLUDE, "-I", CSRC]
 
 
@@ -62,18 +64,29 @@ def build_cuda(verbose: bool = False, ptxas_info: bool = False) -> str:
 
 
 def build_host(verbose: bool = False) -> str | None:
+    """Host C++ layer: each source compiled separately (the dense LDL^T may
+    contract to FMA; the IPM's scalar arithmetic must not, to match the
+    reference's rounding), then linked against libhn_sm100.so."""
     srcs = sorted(glob.glob(os.path.join(HOST, "*.cpp")))
     if not srcs:
         return None
-    hdrs = glob.glob(os.path.join(HOST, "*.hpp")) + [os.path.join(INCLUDE, "hn_sm100.h")]
-    if _stale(HOSTLIB, srcs + hdrs + [LIB]):
-        cxx = os.environ.get("CXX", "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++")
-        cmd = [cxx, "-O3", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-march=x86-64-v3",
-               "-ffp-contract=off", "-I", INCLUDE, "-I", HOST, *srcs, "-o", HOSTLIB,
-               "-L", HERE, "-lhn_sm100", "-Wl,-rpath,$ORIGIN", "-lpthread"]
-        if verbose:
-            print(" ".join(cmd))
-        _run(cmd)
+    hdrs = glob.glob(os.path.join(HOST, "*.hpp")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else os.environ.get("CXX", "g++")
+    os.makedirs(BUILD, exist_ok=True)
+    objs = []
+    for src in srcs:
+        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+        objs.append(obj)
+        if _stale(obj, [src] + hdrs):
+            contract = "-ffp-contract=fast" if os.path.basename(src) == "hn_ldlt.cpp" else "-ffp-contract=off"
+            cmd = [cxx, "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-march=x86-64-v3", contract,
+                   "-I", INCLUDE, "-I", HOST, "-c", src, "-o", obj]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
+    if _stale(HOSTLIB, objs + [LIB]):
+        _run([cxx, "-shared", "-fopenmp", "-o", HOSTLIB, *objs, "-L", HERE, "-lhn_sm100",
+              "-Wl,-rpath,$ORIGIN", "-lpthread"])
     return HOSTLIB
 
 

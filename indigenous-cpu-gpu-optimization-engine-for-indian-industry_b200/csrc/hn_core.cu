@@ -42,7 +42,7 @@ Workspace& workspace(cudaStream_t s) {
     auto it = g_ctx.ws.find(s);
     if (it != g_ctx.ws.end()) return it->second;
     Workspace w;
-    w.partials = dmalloc<double>(2 * kMaxReduceBlocks + 8);
+    w.partials = dmalloc<double>(4 * kMaxReduceBlocks + 8);
     w.counter = dmalloc<unsigned>(4);
     check_cuda(cudaMemsetAsync(w.counter, 0, 4 * sizeof(unsigned), s), "workspace init");
     check_cuda(cudaStreamSynchronize(s), "workspace init sync");

@@ -156,6 +156,24 @@ __device__ __forceinline__ double block_max(double v, double* sh) {
 }
 
 template <int THREADS>
+__device__ __forceinline__ double block_min(double v, double* sh) {
+    constexpr int W = THREADS / 32;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = INFINITY;
+    if (wid == 0) {
+        r = lane < W ? sh[lane] : INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r = fmin(r, __shfl_down_sync(0xffffffffu, r, o));
+    }
+    return r;
+}
+
+template <int THREADS>
 __device__ __forceinline__ int64_t block_sum_i64(int64_t v, int64_t* sh) {
     constexpr int W = THREADS / 32;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -277,4 +295,15 @@ struct hn_pattern {
     int32_t* ci = nullptr;       // nnz
     int64_t* diag_pos = nullptr; // m
     unsigned long long* maxdiag = nullptr;  // scratch: max diagonal as ordered bits
+    // scatter map of the numeric phase: contribution q of row i (entries e of
+    // row i in order, then the rows k of column j_e in order) lands in slot
+    // map[q] of N, or -- with kMulti set -- in the ordered-sum scratch
+    int64_t nq = 0;
+    int64_t* qrow = nullptr;     // m+1: first contribution of each row
+    uint32_t* map = nullptr;     // nq
+    int64_t nms = 0;             // slots with several contributions (+ every diagonal)
+    int64_t* mpos = nullptr;     // nms: N position (bit 62 set for a diagonal)
+    int32_t* mbeg = nullptr;     // nms+1: scratch range of each such slot
+    int64_t nmq = 0;             // contributions into those slots
+    double* scratch = nullptr;   // nmq
 };

@@ -79,6 +79,13 @@ SIGNATURES = {
     "hn_pattern_device": [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)],
     "hn_ada_numeric": [_vp, _vp, C.c_double, _vp, _vp, _vp],
     "hn_pattern_destroy": [_vp],
+    "hn_ipm_residuals": [_vp] + [_vp] * 11 + [_vp],
+    "hn_ipm_rhs": [_vp, _vp, _vp, _vp, _vp, _vp],
+    "hn_ipm_direction": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "hn_ipm_step_lengths": [_i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "hn_ipm_corrector": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "hn_ipm_update": [_i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "hn_max_step": [_i64, _vp, _vp, _vp, _vp],
 }
 _RESTYPE = {"hn_last_error": C.c_char_p}
 
@@ -282,3 +289,154 @@ def nrm2(n, v, out, stream=None) -> None:
 
 def exported_symbols() -> list[str]:
     return list(SIGNATURES)
+
+
+# ---------------------------------------------------------------- host layer (libhn_host.so)
+INTERRUPT_CB = C.CFUNCTYPE(C.c_int, C.c_void_p)
+
+
+class IpmOptions(C.Structure):
+    _fields_ = [("max_iterations", C.c_int), ("time_limit_seconds", C.c_double), ("convergence_tol", C.c_double),
+                ("complementarity_tol", C.c_double), ("regularization", C.c_double), ("device", C.c_int),
+                ("verbose", C.c_int), ("interrupt_cb", INTERRUPT_CB), ("interrupt_user", C.c_void_p)]
+
+
+class IpmResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int64), ("objective", C.c_double),
+                ("solve_time_ms", C.c_double), ("device_ms", C.c_double), ("factor_ms", C.c_double),
+                ("solve_ms", C.c_double), ("nnz_normal", C.c_int64)]
+
+
+HOST_SIGNATURES = {
+    "hn_ipm_default_options": (None, [C.POINTER(IpmOptions)]),
+    "hn_lp_solve": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, C.POINTER(C.c_int), _f64p, _f64p,
+                              C.c_int, C.c_double, C.POINTER(IpmOptions), C.POINTER(IpmResult), _f64p]),
+    "hn_host_last_error": (C.c_char_p, []),
+    "hn_be_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
+    "hn_be_destroy": (C.c_int, [_vp]),
+    "hn_be_spmv": (C.c_int, [_vp, _i64, _i64, _u64p, _u64p, _f64p, _i64, _f64p, _f64p]),
+    "hn_be_spmv_t": (C.c_int, [_vp, _i64, _i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p]),
+    "hn_be_spmm": (C.c_int, [_vp, _i64, _i64, _u64p, _u64p, _f64p, _i64, _f64p, _i64, _f64p]),
+    "hn_be_dot": (C.c_int, [_vp, _i64, _f64p, _f64p, _f64p]),
+    "hn_be_axpy": (C.c_int, [_vp, _i64, C.c_double, _f64p, _f64p]),
+    "hn_be_norm_inf": (C.c_int, [_vp, _i64, _f64p, _f64p]),
+    "hn_be_kernel_executions": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+}
+_host = None
+
+STATUS = ["UNKNOWN", "OPTIMAL", "INFEASIBLE", "UNBOUNDED", "SUBOPTIMAL", "TIME_LIMIT", "ITER_LIMIT",
+          "NUMERICAL_ERROR", "INTERRUPTED"]
+
+
+def host() -> C.CDLL:
+    global _host
+    if _host is not None:
+        return _host
+    load()
+    if not os.path.exists(HOST_LIB_PATH):
+        raise FileNotFoundError(f"{HOST_LIB_PATH} is missing: build it with build.py")
+    lib = C.CDLL(HOST_LIB_PATH)
+    for name, (res, args) in HOST_SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _host = lib
+    return lib
+
+
+def host_check(status: int) -> None:
+    if status != HN_OK:
+        raise HnError(status, host().hn_host_last_error().decode(errors="replace"))
+
+
+def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=0.0, max_iter=100,
+             time_limit=0.0, device=0, interrupt=None, verbose=False):
+    """GPU IPM on an LP given as CSR (rows EQ and x >= 0 unless told otherwise)."""
+    m, n = int(lp["m"]), int(lp["n"])
+    rp, ci, val = u64(lp["rp"]), u64(lp["ci"]), f64(lp["val"])
+    c, b = f64(lp["c"]), f64(lp["b"])
+    sense = np.ascontiguousarray(np.full(m, 2) if sense is None else sense, dtype=np.int32)
+    lb = f64(np.zeros(n) if lb is None else lb)
+    ub = f64(np.full(n, np.inf) if ub is None else ub)
+    opt = IpmOptions()
+    host().hn_ipm_default_options(C.byref(opt))
+    opt.max_iterations = max_iter
+    opt.time_limit_seconds = time_limit
+    opt.device = device
+    opt.verbose = int(verbose)
+    cb = INTERRUPT_CB(lambda _u: int(bool(interrupt()))) if interrupt is not None else INTERRUPT_CB()
+    opt.interrupt_cb = cb
+    res = IpmResult()
+    x = np.zeros(n)
+    host_check(host().hn_lp_solve(m, n, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
+                                  _p(c, C.c_double), _p(b, C.c_double), sense.ctypes.data_as(C.POINTER(C.c_int)),
+                                  _p(lb, C.c_double), _p(ub, C.c_double), int(maximize), float(obj_offset),
+                                  C.byref(opt), C.byref(res), _p(x, C.c_double)))
+    err = host().hn_host_last_error().decode(errors="replace")
+    return {"status": res.status, "status_name": STATUS[res.status], "objective": res.objective,
+            "iterations": res.iterations, "time_ms": res.solve_time_ms, "device_ms": res.device_ms,
+            "factor_ms": res.factor_ms, "solve_ms": res.solve_ms, "nnz_normal": res.nnz_normal, "x": x,
+            "error": err}
+
+
+class Backend:
+    """hn::execution::B200Backend (IComputeBackend) through the host C ABI."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        host_check(host().hn_be_create(device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            host().hn_be_destroy(self.h)
+            self.h = None
+
+    def spmv(self, rp, ci, val, x):
+        rp, ci, val, x = u64(rp), u64(ci), f64(val), f64(x)
+        m = rp.shape[0] - 1
+        y = np.empty(m)
+        host_check(host().hn_be_spmv(self.h, m, val.shape[0], _p(rp, C.c_uint64), _p(ci, C.c_uint64),
+                                     _p(val, C.c_double), x.shape[0], _p(x, C.c_double), _p(y, C.c_double)))
+        return y
+
+    def spmv_t(self, rp, ci, val, x, n):
+        rp, ci, val, x = u64(rp), u64(ci), f64(val), f64(x)
+        m = rp.shape[0] - 1
+        y = np.empty(n)
+        host_check(host().hn_be_spmv_t(self.h, m, n, val.shape[0], _p(rp, C.c_uint64), _p(ci, C.c_uint64),
+                                       _p(val, C.c_double), _p(x, C.c_double), _p(y, C.c_double)))
+        return y
+
+    def spmm(self, rp, ci, val, B, k):
+        rp, ci, val, B = u64(rp), u64(ci), f64(val), f64(B)
+        m = rp.shape[0] - 1
+        Cm = np.empty(m * k)
+        host_check(host().hn_be_spmm(self.h, m, val.shape[0], _p(rp, C.c_uint64), _p(ci, C.c_uint64),
+                                     _p(val, C.c_double), B.shape[0] // max(k, 1), _p(B, C.c_double), k,
+                                     _p(Cm, C.c_double)))
+        return Cm
+
+    def dot(self, a, b):
+        a, b = f64(a), f64(b)
+        out = C.c_double()
+        host_check(host().hn_be_dot(self.h, min(a.shape[0], b.shape[0]), _p(a, C.c_double), _p(b, C.c_double),
+                                    C.byref(out)))
+        return out.value
+
+    def axpy(self, alpha, x, y):
+        x, y = f64(x), f64(y).copy()
+        host_check(host().hn_be_axpy(self.h, min(x.shape[0], y.shape[0]), alpha, _p(x, C.c_double),
+                                     _p(y, C.c_double)))
+        return y
+
+    def norm_inf(self, v):
+        v = f64(v)
+        out = C.c_double()
+        host_check(host().hn_be_norm_inf(self.h, v.shape[0], _p(v, C.c_double), C.byref(out)))
+        return out.value
+
+    def kernel_executions(self):
+        out = C.c_uint64()
+        host_check(host().hn_be_kernel_executions(self.h, C.byref(out)))
+        return out.value

@@ -1,0 +1,173 @@
+// C ABI of the host layer (include/hn_host.h).
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "hn_backend.hpp"
+#include "hn_host.h"
+#include "hn_lp.hpp"
+#include "hn_sm100.h"
+
+namespace {
+thread_local std::string g_err;
+
+template <class F>
+int wrap(F&& f) {
+    try {
+        f();
+        return HN_OK;
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return HN_ERR_INVALID_ARG;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return HN_ERR_CUDA;
+    }
+}
+
+template <class T>
+std::vector<T> vec(const T* p, int64_t n) {
+    return n > 0 ? std::vector<T>(p, p + n) : std::vector<T>();
+}
+}  // namespace
+
+struct hn_backend {
+    hn::execution::B200Backend be;
+    explicit hn_backend(int d) : be(d) {}
+};
+
+extern "C" {
+
+void hn_ipm_default_options(hn_ipm_options* o) {
+    o->max_iterations = 100;
+    o->time_limit_seconds = 0.0;
+    o->convergence_tol = 1e-8;
+    o->complementarity_tol = 1e-8;
+    o->regularization = 1e-8;
+    o->device = 0;
+    o->verbose = 0;
+    o->interrupt_cb = nullptr;
+    o->interrupt_user = nullptr;
+}
+
+const char* hn_host_last_error(void) { return g_err.c_str(); }
+
+int hn_lp_solve(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, const double* val, const double* c,
+                const double* b, const int* sense, const double* lb, const double* ub, int maximize,
+                double obj_offset, const hn_ipm_options* opt, hn_ipm_result* res, double* x_out) {
+    return wrap([&] {
+        if (m < 0 || n < 0 || !rp || !res) throw std::invalid_argument("bad arguments");
+        hn::model::LpProblem p;
+        p.num_rows = (std::size_t)m;
+        p.num_cols = (std::size_t)n;
+        p.row_ptr.assign(rp, rp + m + 1);
+        p.col_indices.assign(ci, ci + rp[m]);
+        p.values.assign(val, val + rp[m]);
+        p.objective = vec(c, n);
+        p.lower = vec(lb, n);
+        p.upper = vec(ub, n);
+        p.rhs = vec(b, m);
+        for (int64_t i = 0; i < m; ++i)
+            p.sense.push_back(sense[i] == 0 ? hn::model::ConstraintSense::LE
+                                            : sense[i] == 1 ? hn::model::ConstraintSense::GE
+                                                            : hn::model::ConstraintSense::EQ);
+        p.obj_sense = maximize ? hn::model::ObjectiveSense::MAXIMIZE : hn::model::ObjectiveSense::MINIMIZE;
+        p.obj_offset = obj_offset;
+        hn::lp::InteriorPointOptions o;
+        if (opt) {
+            o.max_iterations = opt->max_iterations;
+            o.time_limit_seconds = opt->time_limit_seconds;
+            o.convergence_tol = opt->convergence_tol;
+            o.complementarity_tol = opt->complementarity_tol;
+            o.regularization = opt->regularization;
+            o.device = opt->device;
+            o.verbose = opt->verbose != 0;
+            if (opt->interrupt_cb) {
+                auto cb = opt->interrupt_cb;
+                void* user = opt->interrupt_user;
+                o.interrupt_callback = [cb, user]() { return cb(user) != 0; };
+            }
+        }
+        hn::lp::InteriorPointSolver solver(o);
+        auto r = solver.solve(p);
+        res->status = static_cast<int>(r.status);
+        res->iterations = (int64_t)r.iterations;
+        res->objective = r.objective_value;
+        res->solve_time_ms = r.solve_time_ms;
+        res->device_ms = r.device_ms;
+        res->factor_ms = r.factor_ms;
+        res->solve_ms = r.solve_ms;
+        res->nnz_normal = (int64_t)r.nnz_normal;
+        if (x_out && r.primal.size() == (std::size_t)n) std::memcpy(x_out, r.primal.data(), 8 * n);
+        g_err = r.error;
+    });
+}
+
+int hn_be_create(int device, hn_backend** out) {
+    return wrap([&] {
+        auto* b = new hn_backend(device);
+        b->be.initialize();
+        if (!b->be.is_available()) {
+            std::string e = b->be.last_error();
+            delete b;
+            throw std::runtime_error("B200 backend unavailable: " + e);
+        }
+        *out = b;
+    });
+}
+
+int hn_be_destroy(hn_backend* be) {
+    return wrap([&] { delete be; });
+}
+
+int hn_be_spmv(hn_backend* be, int64_t m, int64_t nnz, const uint64_t* rp, const uint64_t* ci, const double* val,
+               int64_t nx, const double* x, double* y) {
+    return wrap([&] {
+        std::vector<double> v = vec(val, nnz), xx = vec(x, nx), yy;
+        std::vector<std::size_t> c(ci, ci + nnz), r(rp, rp + m + 1);
+        be->be.spmv(v, c, r, xx, yy);
+        std::memcpy(y, yy.data(), 8 * yy.size());
+    });
+}
+
+int hn_be_spmv_t(hn_backend* be, int64_t m, int64_t n, int64_t nnz, const uint64_t* rp, const uint64_t* ci,
+                 const double* val, const double* x, double* y) {
+    return wrap([&] {
+        std::vector<double> v = vec(val, nnz), xx = vec(x, m), yy;
+        std::vector<std::size_t> c(ci, ci + nnz), r(rp, rp + m + 1);
+        be->be.spmv_t(v, c, r, (std::size_t)n, xx, yy);
+        std::memcpy(y, yy.data(), 8 * yy.size());
+    });
+}
+
+int hn_be_spmm(hn_backend* be, int64_t m, int64_t nnz, const uint64_t* rp, const uint64_t* ci, const double* val,
+               int64_t nb, const double* B, int64_t k, double* C) {
+    return wrap([&] {
+        std::vector<double> v = vec(val, nnz), bb = vec(B, nb * k), cc;
+        std::vector<std::size_t> c(ci, ci + nnz), r(rp, rp + m + 1);
+        be->be.spmm(v, c, r, bb, cc, (std::size_t)k);
+        std::memcpy(C, cc.data(), 8 * cc.size());
+    });
+}
+
+int hn_be_dot(hn_backend* be, int64_t n, const double* a, const double* b, double* out) {
+    return wrap([&] { *out = be->be.dot(vec(a, n), vec(b, n)); });
+}
+
+int hn_be_axpy(hn_backend* be, int64_t n, double alpha, const double* x, double* y) {
+    return wrap([&] {
+        std::vector<double> yy = vec(y, n);
+        be->be.axpy(alpha, vec(x, n), yy);
+        std::memcpy(y, yy.data(), 8 * n);
+    });
+}
+
+int hn_be_norm_inf(hn_backend* be, int64_t n, const double* v, double* out) {
+    return wrap([&] { *out = be->be.norm_inf(vec(v, n)); });
+}
+
+int hn_be_kernel_executions(hn_backend* be, uint64_t* out) {
+    return wrap([&] { *out = be->be.gpu_kernel_executions(); });
+}
+
+}  // extern "C"

@@ -1,0 +1,520 @@
+// GPU Mehrotra predictor-corrector IPM: host control flow of
+// lp::InteriorPointSolver::solve (core/lp/interior_point.cpp:402-886), with
+// the iterate, residuals, directions, step lengths and A D A^T assembly on
+// the B200 (include/hn_sm100.h) and the normal-equation factorisation on the
+// host (DenseLDLT). Only scalars, N's values and the m-vectors of the two
+// normal-equation solves cross PCIe each iteration.
+#include <omp.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <unordered_set>
+
+#include "hn_lp.hpp"
+#include "hn_sm100.h"
+
+namespace hn::lp {
+namespace {
+
+using model::ConstraintSense;
+using model::ProblemStatus;
+
+void ck(int st, const char* what) {
+    if (st != HN_OK) throw std::runtime_error(std::string(what) + ": " + hn_last_error());
+}
+
+// ---- standard form (interior_point.cpp:29-49, 202-373) ----
+struct VarInfo {
+    std::vector<int> slots;
+    std::vector<double> signs;
+    std::vector<double> shifts;
+    double fixed = 0.0;
+    bool is_fixed = false;
+};
+
+struct StandardForm {
+    std::size_t m = 0, n = 0;
+    std::vector<std::size_t> rp, ci;
+    std::vector<double> val, rhs, c, col_scale;
+    double offset = 0.0;
+    std::vector<VarInfo> var_info;
+};
+
+struct Trip {
+    std::size_t r, c;
+    double v;
+};
+
+// CSR from triplets with SparseMatrix::from_triplets semantics
+// (core/numerical/sparse_matrix.cpp:8-53, 230-262): sort by (row, col),
+// sum equal keys, drop exact zero sums.
+void csr_from_triplets(std::size_t rows, std::vector<Trip>& t, std::vector<std::size_t>& rp,
+                       std::vector<std::size_t>& ci, std::vector<double>& val) {
+    std::stable_sort(t.begin(), t.end(), [](const Trip& a, const Trip& b) {
+        return a.r != b.r ? a.r < b.r : a.c < b.c;
+    });
+    rp.assign(rows + 1, 0);
+    ci.clear();
+    val.clear();
+    std::size_t k = 0;
+    for (std::size_t i = 0; i < rows; ++i) {
+        while (k < t.size() && t[k].r == i) {
+            const std::size_t c = t[k].c;
+            double s = t[k].v;
+            ++k;
+            while (k < t.size() && t[k].r == i && t[k].c == c) s += t[k++].v;
+            if (s != 0.0) {
+                ci.push_back(c);
+                val.push_back(s);
+            }
+        }
+        rp[i + 1] = ci.size();
+    }
+}
+
+// remove_duplicate_rows (interior_point.cpp:79-132): a row equal to an
+// earlier one in entries (sorted), sense and rhs bits is dropped.
+model::LpProblem remove_duplicate_rows(const model::LpProblem& p) {
+    if (p.num_rows == 0) return p;
+    std::unordered_set<std::string> seen;
+    std::vector<std::size_t> keep;
+    for (std::size_t i = 0; i < p.num_rows; ++i) {
+        std::vector<std::pair<std::size_t, double>> ent;
+        for (std::size_t k = p.row_ptr[i]; k < p.row_ptr[i + 1]; ++k) ent.emplace_back(p.col_indices[k], p.values[k]);
+        std::sort(ent.begin(), ent.end());
+        std::string key;
+        for (const auto& e : ent) {
+            std::uint64_t bv;
+            std::memcpy(&bv, &e.second, 8);
+            key += std::to_string(e.first) + ':' + std::to_string(bv) + ';';
+        }
+        std::uint64_t br;
+        std::memcpy(&br, &p.rhs[i], 8);
+        key += '|' + std::to_string(static_cast<int>(p.sense[i])) + ':' + std::to_string(br);
+        if (seen.insert(key).second) keep.push_back(i);
+    }
+    if (keep.size() == p.num_rows) return p;
+    model::LpProblem q = p;
+    q.num_rows = keep.size();
+    q.row_ptr.assign(1, 0);
+    q.col_indices.clear();
+    q.values.clear();
+    q.sense.clear();
+    q.rhs.clear();
+    for (std::size_t i : keep) {
+        std::vector<std::pair<std::size_t, double>> ent;
+        for (std::size_t k = p.row_ptr[i]; k < p.row_ptr[i + 1]; ++k) ent.emplace_back(p.col_indices[k], p.values[k]);
+        std::sort(ent.begin(), ent.end());
+        for (const auto& e : ent) {
+            q.col_indices.push_back(e.first);
+            q.values.push_back(e.second);
+        }
+        q.row_ptr.push_back(q.col_indices.size());
+        q.sense.push_back(p.sense[i]);
+        q.rhs.push_back(p.rhs[i]);
+    }
+    return q;
+}
+
+StandardForm build_standard_form(const model::LpProblem& p, double feas_tol) {
+    StandardForm f;
+    const std::size_t n = p.num_cols, norig = p.num_rows;
+    const bool negate = p.obj_sense == model::ObjectiveSense::MAXIMIZE;
+    std::vector<double> cbase(n);
+    for (std::size_t j = 0; j < n; ++j) cbase[j] = negate ? -p.objective[j] : p.objective[j];
+    f.var_info.resize(n);
+    std::size_t nslots = 0, ntle = 0, m_ub = 0;
+    for (std::size_t j = 0; j < n; ++j) {
+        const double lb = p.lower[j], ub = p.upper[j];
+        VarInfo& v = f.var_info[j];
+        if (std::isfinite(lb) && std::isfinite(ub) && std::abs(ub - lb) <= feas_tol) {
+            v.is_fixed = true;
+            v.fixed = lb;
+            f.offset += cbase[j] * lb;
+        } else if (std::isfinite(lb)) {
+            v.slots.push_back(static_cast<int>(nslots++));
+            v.signs.push_back(1.0);
+            v.shifts.push_back(lb);
+            f.offset += cbase[j] * lb;
+            if (std::isfinite(ub)) ++m_ub;
+        } else if (std::isfinite(ub)) {
+            v.slots.push_back(static_cast<int>(nslots++));
+            v.signs.push_back(-1.0);
+            v.shifts.push_back(ub);
+            f.offset += cbase[j] * ub;
+        } else {
+            v.slots.push_back(static_cast<int>(nslots++));
+            v.signs.push_back(1.0);
+            v.shifts.push_back(0.0);
+            v.slots.push_back(static_cast<int>(nslots++));
+            v.signs.push_back(-1.0);
+            v.shifts.push_back(0.0);
+        }
+    }
+    for (std::size_t i = 0; i < norig; ++i)
+        if (p.sense[i] == ConstraintSense::LE || p.sense[i] == ConstraintSense::GE) ++ntle;
+    const std::size_t m_rows = norig + m_ub, ncols = nslots + ntle + m_ub;
+    f.m = m_rows;
+    f.n = ncols;
+    f.rhs.assign(m_rows, 0.0);
+    f.c.assign(ncols, 0.0);
+    for (std::size_t j = 0; j < n; ++j)
+        for (std::size_t s = 0; s < f.var_info[j].slots.size(); ++s)
+            f.c[f.var_info[j].slots[s]] = f.var_info[j].signs[s] > 0 ? cbase[j] : -cbase[j];
+    std::vector<double> gamma(norig, 1.0);
+    for (std::size_t i = 0; i < norig; ++i) {
+        double rowmax = 0.0;
+        for (std::size_t k = p.row_ptr[i]; k < p.row_ptr[i + 1]; ++k) rowmax = std::max(rowmax, std::abs(p.values[k]));
+        if (rowmax > 0.0) gamma[i] = 1.0 / rowmax;
+    }
+    std::vector<Trip> trips;
+    std::size_t next_slack = nslots;
+    for (std::size_t i = 0; i < norig; ++i) {
+        double const_i = 0.0;
+        const bool flip = p.sense[i] == ConstraintSense::GE;
+        for (std::size_t k = p.row_ptr[i]; k < p.row_ptr[i + 1]; ++k) {
+            const std::size_t j = p.col_indices[k];
+            const double a = gamma[i] * p.values[k];
+            const VarInfo& v = f.var_info[j];
+            if (v.is_fixed) {
+                const_i += a * v.fixed;
+            } else {
+                for (std::size_t s = 0; s < v.slots.size(); ++s) {
+                    trips.push_back({i, static_cast<std::size_t>(v.slots[s]), flip ? -a * v.signs[s] : a * v.signs[s]});
+                    const_i += a * v.shifts[s];
+                }
+            }
+        }
+        if (p.sense[i] == ConstraintSense::LE || p.sense[i] == ConstraintSense::GE)
+            trips.push_back({i, next_slack++, gamma[i]});
+        f.rhs[i] = flip ? (-gamma[i] * p.rhs[i] + const_i) : (gamma[i] * p.rhs[i] - const_i);
+    }
+    std::size_t next_ub_row = norig;
+    for (std::size_t j = 0; j < n; ++j) {
+        const double lb = p.lower[j], ub = p.upper[j];
+        if (std::isfinite(lb) && std::isfinite(ub) && std::abs(ub - lb) > feas_tol) {
+            const std::size_t gi = static_cast<std::size_t>(f.var_info[j].slots[0]);
+            trips.push_back({next_ub_row, gi, 1.0});
+            trips.push_back({next_ub_row, next_slack++, 1.0});
+            f.rhs[next_ub_row] = ub - lb;
+            ++next_ub_row;
+        }
+    }
+    csr_from_triplets(m_rows, trips, f.rp, f.ci, f.val);
+    // column scaling (:346-370)
+    f.col_scale.assign(ncols, 1.0);
+    std::vector<double> colmax(ncols, 0.0);
+    for (std::size_t k = 0; k < f.val.size(); ++k) colmax[f.ci[k]] = std::max(colmax[f.ci[k]], std::abs(f.val[k]));
+    for (std::size_t j = 0; j < ncols; ++j)
+        if (colmax[j] > 0.0) f.col_scale[j] = 1.0 / colmax[j];
+    std::vector<Trip> scaled;
+    scaled.reserve(f.val.size());
+    for (std::size_t i = 0; i < m_rows; ++i)
+        for (std::size_t k = f.rp[i]; k < f.rp[i + 1]; ++k) scaled.push_back({i, f.ci[k], f.val[k] * f.col_scale[f.ci[k]]});
+    csr_from_triplets(m_rows, scaled, f.rp, f.ci, f.val);
+    for (std::size_t j = 0; j < ncols; ++j) f.c[j] *= f.col_scale[j];
+    return f;
+}
+
+std::vector<double> to_original_primal(const StandardForm& f, const std::vector<double>& y) {
+    // :375-396
+    const std::size_t n = f.var_info.size();
+    std::vector<double> primal(n, 0.0);
+    for (std::size_t j = 0; j < n; ++j) {
+        const VarInfo& v = f.var_info[j];
+        if (v.is_fixed) {
+            primal[j] = v.fixed;
+            continue;
+        }
+        double val = 0.0;
+        for (std::size_t s = 0; s < v.slots.size(); ++s) {
+            const int gi = v.slots[s];
+            if (gi < 0 || static_cast<std::size_t>(gi) >= f.col_scale.size()) continue;
+            val += v.signs[s] * f.col_scale[gi] * y[gi];
+            if (s == 0) val += v.shifts[s];
+        }
+        primal[j] = val;
+    }
+    return primal;
+}
+
+// Device buffer owning helper.
+struct DevBuf {
+    void* p = nullptr;
+    explicit DevBuf(std::size_t bytes) { ck(hn_malloc(&p, bytes ? bytes : 8), "hn_malloc"); }
+    ~DevBuf() {
+        if (p) hn_free(p);
+    }
+    double* d() const { return static_cast<double*>(p); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+};
+
+using Clock = std::chrono::steady_clock;
+double ms_since(Clock::time_point t) { return std::chrono::duration<double, std::milli>(Clock::now() - t).count(); }
+
+// The normal matrix on the host: the device pattern (CSR, both triangles)
+// plus its values, kept for the refinement products, and a dense lower
+// triangle for the factorisation.
+struct HostNormal {
+    std::size_t m = 0;
+    std::vector<uint64_t> rp, ci;
+    std::vector<double> val;
+    std::vector<double> dense;
+    void to_dense() {
+        dense.assign(m * m, 0.0);
+        for (std::size_t i = 0; i < m; ++i)
+            for (uint64_t k = rp[i]; k < rp[i + 1]; ++k)
+                if (ci[k] <= i) dense[i * m + ci[k]] = val[k];
+    }
+    // y = N x with SparseMatrix::multiply's order (sparse_matrix.cpp:142-149)
+    void multiply(const std::vector<double>& x, std::vector<double>& y) const {
+        y.assign(m, 0.0);
+        for (std::size_t i = 0; i < m; ++i) {
+            double s = 0.0;
+            for (uint64_t k = rp[i]; k < rp[i + 1]; ++k) s += val[k] * x[ci[k]];
+            y[i] = s;
+        }
+    }
+};
+
+// iterative_refinement(fac, N, x, rhs) with its defaults 1e-10 / 5 sweeps
+// (core/numerical/refinement.cpp:7-37).
+void refine(const DenseLDLT& fac, const HostNormal& N, std::vector<double>& x, const std::vector<double>& rhs) {
+    const std::size_t n = x.size();
+    double norm_rhs = 0.0;
+    for (double v : rhs) norm_rhs = std::max(norm_rhs, std::abs(v));
+    if (norm_rhs == 0.0 || norm_rhs != norm_rhs) return;
+    std::vector<double> ax, r(n);
+    for (int it = 0; it < 5; ++it) {
+        N.multiply(x, ax);
+        double rel = 0.0;
+        for (std::size_t i = 0; i < n; ++i) rel = std::max(rel, std::abs(rhs[i] - ax[i]));
+        rel /= norm_rhs;
+        if (rel <= 1e-10) break;
+        for (std::size_t i = 0; i < n; ++i) r[i] = rhs[i] - ax[i];
+        fac.solve(r);
+        for (std::size_t i = 0; i < n; ++i) x[i] += r[i];
+    }
+}
+
+constexpr std::size_t kMaxDenseRows = 12000;
+
+}  // namespace
+
+InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) {
+    const auto start = Clock::now();
+    InteriorPointResult result;
+    const auto& O = options_;
+    if (problem.num_cols == 0) {
+        result.status = ProblemStatus::OPTIMAL;
+        result.objective_value = problem.obj_offset;
+        return result;
+    }
+    try {
+        const model::LpProblem cleaned = remove_duplicate_rows(problem);
+        const StandardForm f = build_standard_form(cleaned, O.feasibility_tol);
+        if (f.n == 0) {
+            result.status = ProblemStatus::OPTIMAL;
+            result.objective_value = f.offset;
+            result.primal = to_original_primal(f, {});
+            return result;
+        }
+        if (f.m == 0) {
+            bool unbounded = false;
+            for (double cj : f.c)
+                if (cj < -1e-9) unbounded = true;  // optimality_tol of industrial_defaults
+            result.status = unbounded ? ProblemStatus::UNBOUNDED : ProblemStatus::OPTIMAL;
+            result.primal = to_original_primal(f, std::vector<double>(f.n, 0.0));
+            double obj = problem.obj_offset;
+            for (std::size_t j = 0; j < problem.num_cols; ++j) obj += problem.objective[j] * result.primal[j];
+            result.objective_value = obj;
+            return result;
+        }
+        if (f.m > kMaxDenseRows)
+            throw std::runtime_error("standard form has " + std::to_string(f.m) +
+                                     " rows; the host dense factorisation supports up to 12000");
+        const std::size_t m = f.m, n = f.n;
+        ck(hn_init(O.device), "hn_init");
+        hn_csr* M = nullptr;
+        ck(hn_csr_create((int64_t)m, (int64_t)n, reinterpret_cast<const uint64_t*>(f.rp.data()),
+                         reinterpret_cast<const uint64_t*>(f.ci.data()), f.val.data(), 0, &M),
+           "hn_csr_create");
+        std::unique_ptr<hn_csr, int (*)(hn_csr*)> Mh(M, hn_csr_destroy);
+        hn_pattern* P = nullptr;
+        ck(hn_ada_symbolic(M, &P), "hn_ada_symbolic");
+        std::unique_ptr<hn_pattern, int (*)(hn_pattern*)> Ph(P, hn_pattern_destroy);
+        HostNormal N;
+        N.m = m;
+        int64_t pm = 0, pnnz = 0;
+        ck(hn_pattern_info(P, &pm, &pnnz), "hn_pattern_info");
+        N.rp.resize(m + 1);
+        N.ci.resize((std::size_t)pnnz);
+        N.val.resize((std::size_t)pnnz);
+        ck(hn_pattern_export(P, N.rp.data(), N.ci.data()), "hn_pattern_export");
+        result.nnz_normal = (std::size_t)pnnz;
+
+        // start point (:439-453)
+        double b_norm = 1.0, c_norm = 1.0;
+        for (double v : f.rhs) b_norm = std::max(b_norm, std::abs(v));
+        for (double v : f.c) c_norm = std::max(c_norm, std::abs(v));
+        std::vector<double> hx(n, b_norm + 1.0), hz(n), hlam(m, 0.0);
+        for (std::size_t j = 0; j < n; ++j) hz[j] = std::max(c_norm + 1.0, std::abs(f.c[j]));
+
+        DevBuf x(8 * n), z(8 * n), lam(8 * m), b(8 * m), c(8 * n), mx(8 * m), rp(8 * m), rd(8 * n), D(8 * n),
+            Drd(8 * n), rhs_pred(8 * m), rhs(8 * m), dlam(8 * m), dx(8 * n), dz(8 * n), zs(8 * n),
+            nval(8 * (std::size_t)pnnz), scal(8 * HN_IPM_NSCAL), dyn(8);
+        void* st = nullptr;  // legacy default stream
+        ck(hn_memcpy_h2d(x.p, hx.data(), 8 * n, st), "H2D");
+        ck(hn_memcpy_h2d(z.p, hz.data(), 8 * n, st), "H2D");
+        ck(hn_memcpy_h2d(lam.p, hlam.data(), 8 * m, st), "H2D");
+        ck(hn_memcpy_h2d(b.p, f.rhs.data(), 8 * m, st), "H2D");
+        ck(hn_memcpy_h2d(c.p, f.c.data(), 8 * n, st), "H2D");
+        ck(hn_memset(scal.p, 0, 8 * HN_IPM_NSCAL, st), "memset");
+        double sc[HN_IPM_NSCAL];
+        auto read_scal = [&]() { ck(hn_memcpy_d2h(sc, scal.p, sizeof(sc), st), "D2H scal"); };
+        auto flags = [&]() {
+            std::uint64_t fl;
+            std::memcpy(&fl, &sc[HN_IPM_FLAGS], 8);
+            return fl;
+        };
+
+        bool done = false, time_up = false, interrupted = false, numerical_error = false;
+        auto deadline_passed = [&]() {
+            return O.time_limit_seconds > 0.0 && ms_since(start) >= O.time_limit_seconds * 1e3;
+        };
+        DenseLDLT fac;
+        std::vector<double> hrhs(m), hdlam(m);
+        auto solve_normal = [&](const DevBuf& rhs_dev) {
+            auto t = Clock::now();
+            ck(hn_memcpy_d2h(hrhs.data(), rhs_dev.p, 8 * m, st), "D2H rhs");
+            hdlam = hrhs;
+            fac.solve(hdlam);
+            refine(fac, N, hdlam, hrhs);
+            ck(hn_memcpy_h2d(dlam.p, hdlam.data(), 8 * m, st), "H2D dlam");
+            result.solve_ms += ms_since(t);
+        };
+
+        const std::size_t max_it = static_cast<std::size_t>(O.max_iterations);
+        std::size_t iter = 0;
+        for (iter = 0; iter < max_it; ++iter) {
+            if (O.interrupt_callback && O.interrupt_callback()) {
+                interrupted = true;
+                break;
+            }
+            if (deadline_passed()) {
+                time_up = true;
+                break;
+            }
+            auto t0 = Clock::now();
+            ck(hn_ipm_residuals(M, x.d(), lam.d(), z.d(), b.d(), c.d(), mx.d(), rp.d(), rd.d(), D.d(), Drd.d(),
+                                scal.d(), st),
+               "hn_ipm_residuals");
+            read_scal();
+            const double mu = sc[HN_IPM_MU];
+            if (sc[HN_IPM_NRP] < O.convergence_tol && sc[HN_IPM_NRD] < O.convergence_tol && mu < O.complementarity_tol) {
+                done = true;
+                result.device_ms += ms_since(t0);
+                break;
+            }
+            ck(hn_ada_numeric(P, D.d(), O.regularization, nval.d(), dyn.d(), st), "hn_ada_numeric");
+            ck(hn_memcpy_d2h(N.val.data(), nval.p, 8 * (std::size_t)pnnz, st), "D2H N");
+            result.device_ms += ms_since(t0);
+            if (deadline_passed()) {
+                time_up = true;
+                break;
+            }
+            auto tf = Clock::now();
+            N.to_dense();
+            fac.factorize(N.dense, m, O.singular_tol);
+            result.factor_ms += ms_since(tf);
+            if (deadline_passed()) {
+                time_up = true;
+                break;
+            }
+            t0 = Clock::now();
+            ck(hn_ipm_rhs(M, Drd.d(), rp.d(), mx.d(), rhs_pred.d(), st), "hn_ipm_rhs");
+            result.device_ms += ms_since(t0);
+            solve_normal(rhs_pred);
+            t0 = Clock::now();
+            ck(hn_ipm_direction(M, dlam.d(), D.d(), rd.d(), x.d(), nullptr, dx.d(), dz.d(), st), "hn_ipm_direction");
+            ck(hn_ipm_step_lengths((int64_t)n, (int64_t)m, x.d(), dx.d(), z.d(), dz.d(), dlam.d(), scal.d(), st),
+               "hn_ipm_step_lengths");
+            read_scal();
+            if (flags() & 1ull) {
+                numerical_error = true;
+                break;
+            }
+            ck(hn_ipm_corrector(M, x.d(), dx.d(), z.d(), dz.d(), rhs_pred.d(), zs.d(), rhs.d(), scal.d(), st),
+               "hn_ipm_corrector");
+            result.device_ms += ms_since(t0);
+            solve_normal(rhs);
+            t0 = Clock::now();
+            ck(hn_ipm_direction(M, dlam.d(), D.d(), rd.d(), x.d(), zs.d(), dx.d(), dz.d(), st), "hn_ipm_direction");
+            ck(hn_ipm_step_lengths((int64_t)n, (int64_t)m, x.d(), dx.d(), z.d(), dz.d(), dlam.d(), scal.d(), st),
+               "hn_ipm_step_lengths");
+            read_scal();
+            if (flags() & 1ull) {
+                numerical_error = true;
+                break;
+            }
+            ck(hn_ipm_update((int64_t)n, (int64_t)m, x.d(), dx.d(), z.d(), dz.d(), lam.d(), dlam.d(), scal.d(), st),
+               "hn_ipm_update");
+            read_scal();
+            result.device_ms += ms_since(t0);
+            if (flags() & 2ull) {
+                numerical_error = true;
+                break;
+            }
+            if (O.verbose)
+                std::fprintf(stderr, "IPM it=%zu mu=%g rp=%g rd=%g ap=%g ad=%g\n", iter, mu, sc[HN_IPM_NRP],
+                             sc[HN_IPM_NRD], sc[HN_IPM_AP], sc[HN_IPM_AD]);
+            result.iterations = iter + 1;
+        }
+        double last_nrp = 0.0;
+        {
+            ck(hn_ipm_residuals(M, x.d(), lam.d(), z.d(), b.d(), c.d(), mx.d(), rp.d(), rd.d(), D.d(), Drd.d(),
+                                scal.d(), st),
+               "hn_ipm_residuals");
+            read_scal();
+            last_nrp = sc[HN_IPM_NRP];
+            // relaxed acceptance after the loop (:727-753); crossover is not
+            // part of this solver, so the strict 1e-4 primal threshold applies
+            if (!done && !interrupted && sc[HN_IPM_NRP] < 1e-4 && sc[HN_IPM_NRD] < 1e-4 && sc[HN_IPM_MU] < 1e-4)
+                done = true;
+        }
+        ck(hn_memcpy_d2h(hx.data(), x.p, 8 * n, st), "D2H x");
+        std::vector<double> primal = to_original_primal(f, hx);
+        double obj = 0.0;
+        bool obj_ok = std::isfinite(problem.obj_offset);
+        for (std::size_t j = 0; j < problem.num_cols && obj_ok; ++j) {
+            const double term = problem.objective[j] * primal[j];
+            if (!std::isfinite(term)) obj_ok = false;
+            obj += term;
+        }
+        if (obj_ok) obj += problem.obj_offset;
+        if (!obj_ok) numerical_error = true;
+        result.objective_value = obj_ok ? obj : 0.0;
+        result.primal = primal;
+        result.dual.assign(problem.num_rows, 0.0);
+        const bool feasible_incumbent = last_nrp <= O.feasibility_tol;
+        result.status = numerical_error ? ProblemStatus::NUMERICAL_ERROR
+                        : interrupted   ? ProblemStatus::INTERRUPTED
+                        : done          ? ProblemStatus::OPTIMAL
+                        : feasible_incumbent ? ProblemStatus::SUBOPTIMAL
+                        : time_up            ? ProblemStatus::TIME_LIMIT
+                                             : ProblemStatus::ITER_LIMIT;
+    } catch (const std::exception& e) {
+        result.status = ProblemStatus::NUMERICAL_ERROR;
+        result.error = e.what();
+    }
+    result.solve_time_ms = ms_since(start);
+    return result;
+}
+
+}  // namespace hn::lp

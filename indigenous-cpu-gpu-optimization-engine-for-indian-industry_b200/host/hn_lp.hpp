@@ -1,0 +1,118 @@
+// Host-side LP types and the GPU interior-point solver.
+//
+// The solver mirrors HyperNova's lp::InteriorPointSolver
+// (core/lp/interior_point.hpp:16-54, interior_point.cpp:402-886): the same
+// options, statuses, standard form, starting point, Mehrotra predictor-
+// corrector steps and exit logic, with every vector resident on the B200 and
+// the iteration's sparse and elementwise work in the sm_100a library
+// (include/hn_sm100.h). The normal-equation factorisation stays on the host
+// (dense LDL^T with the reference's pivot clamp, hn_ldlt.cpp).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <functional>
+#include <limits>
+#include <string>
+#include <vector>
+
+namespace hn::model {
+
+// Same enumerators, same order as hypernova::model (core/model/problem.hpp:24-45).
+enum class ConstraintSense { LE, GE, EQ };
+enum class ObjectiveSense { MINIMIZE, MAXIMIZE };
+enum class ProblemStatus {
+    UNKNOWN,
+    OPTIMAL,
+    INFEASIBLE,
+    UNBOUNDED,
+    SUBOPTIMAL,
+    TIME_LIMIT,
+    ITER_LIMIT,
+    NUMERICAL_ERROR,
+    INTERRUPTED
+};
+
+// The parts of model::Problem the IPM reads (problem.hpp:79-93): constraint
+// matrix as CSR, per-variable bounds and costs, per-row sense and rhs.
+struct LpProblem {
+    std::size_t num_rows = 0;
+    std::size_t num_cols = 0;
+    std::vector<std::size_t> row_ptr{0};
+    std::vector<std::size_t> col_indices;
+    std::vector<double> values;
+    std::vector<double> objective;
+    std::vector<double> lower;
+    std::vector<double> upper;
+    std::vector<ConstraintSense> sense;
+    std::vector<double> rhs;
+    ObjectiveSense obj_sense = ObjectiveSense::MINIMIZE;
+    double obj_offset = 0.0;
+};
+
+}  // namespace hn::model
+
+namespace hn::lp {
+
+struct InteriorPointOptions {
+    int max_iterations = 100;
+    double time_limit_seconds = 0.0;
+    double convergence_tol = 1e-8;
+    double complementarity_tol = 1e-8;
+    double regularization = 1e-8;
+    // Tolerances the reference takes from ToleranceConfig::industrial_defaults
+    // (core/numerical/tolerance.hpp:60-75).
+    double feasibility_tol = 1e-9;
+    double singular_tol = 1e-10;
+    std::function<bool()> interrupt_callback;
+    int device = 0;
+    bool verbose = false;
+};
+
+struct InteriorPointResult {
+    model::ProblemStatus status = model::ProblemStatus::UNKNOWN;
+    double objective_value = 0.0;
+    std::vector<double> primal;
+    std::vector<double> dual;
+    std::size_t iterations = 0;
+    double solve_time_ms = 0.0;
+    // phase times (ms) of the whole solve
+    double device_ms = 0.0;
+    double factor_ms = 0.0;
+    double solve_ms = 0.0;
+    std::size_t nnz_normal = 0;
+    std::string error;
+};
+
+class InteriorPointSolver {
+public:
+    explicit InteriorPointSolver(const InteriorPointOptions& options = InteriorPointOptions())
+        : options_(options) {}
+    InteriorPointResult solve(const model::LpProblem& problem);
+    const InteriorPointOptions& options() const { return options_; }
+    void set_options(const InteriorPointOptions& o) { options_ = o; }
+
+private:
+    InteriorPointOptions options_;
+};
+
+// Dense LDL^T of a symmetric m x m matrix (lower triangle, row-major) with the
+// pivot rule of SparseCholesky::numeric_factorization
+// (core/numerical/factorization.cpp:1299-1305): a pivot <= singular_tol is
+// replaced by singular_tol. Multithreaded (OpenMP), blocked right-looking.
+class DenseLDLT {
+public:
+    // a: m*m row-major; only the lower triangle is read; overwritten by L.
+    bool factorize(std::vector<double>& a, std::size_t m, double singular_tol);
+    void solve(std::vector<double>& x) const;  // in place
+    std::size_t size() const { return m_; }
+    bool singular() const { return singular_; }
+
+private:
+    std::vector<double> L_;
+    std::vector<double> D_;
+    std::size_t m_ = 0;
+    bool singular_ = false;
+};
+
+}  // namespace hn::lp

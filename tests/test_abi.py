@@ -15,27 +15,39 @@ import hnb200
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_symbols():
+# header -> the library that must export its symbols
+HEADERS = {"hn_sm100.h": hnb200.LIB_PATH, "hn_host.h": hnb200.HOST_LIB_PATH}
+
+
+def declared_symbols(header=None):
     names = set()
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        if header and os.path.basename(h) != header:
+            continue
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names |= set(re.findall(r"^\s*(?:const\s+)?\w+\**\s+\**(hn_\w+)\s*\(", text, flags=re.M))
     return sorted(names)
 
 
+def test_every_header_has_a_library():
+    assert {os.path.basename(h) for h in glob.glob(os.path.join(ROOT, "include", "*.h"))} <= set(HEADERS)
+
+
 def test_header_declares_symbols():
-    assert len(declared_symbols()) >= 30
+    assert len(declared_symbols("hn_sm100.h")) >= 30 and len(declared_symbols("hn_host.h")) >= 10
 
 
 def test_library_exports_every_declared_symbol():
-    lib = C.CDLL(hnb200.LIB_PATH)
-    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
-    assert not missing, missing
+    for header, path in HEADERS.items():
+        lib = C.CDLL(path)
+        missing = [s for s in declared_symbols(header) if not hasattr(lib, s)]
+        assert not missing, (header, missing)
 
 
 def test_binding_covers_every_declared_symbol():
-    assert set(declared_symbols()) <= set(hnb200.SIGNATURES), set(declared_symbols()) - set(hnb200.SIGNATURES)
+    bound = set(hnb200.SIGNATURES) | set(hnb200.HOST_SIGNATURES)
+    assert set(declared_symbols()) <= bound, set(declared_symbols()) - bound
 
 
 def test_calls_before_init_fail_cleanly():

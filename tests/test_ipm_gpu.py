@@ -1,0 +1,302 @@
+"""GPU: the Mehrotra iteration kernels and the GPU IPM against the reference.
+
+Kernel by kernel, each fused step is checked against the oracle restatement
+of the lines of core/lp/interior_point.cpp it implements (elementwise results
+bit-exact: the library is built without FMA contraction, like the
+reference's x86-64 build; products normwise 1e-12). Whole solves must give
+the reference's status and its objective within 1e-8 relative
+(InteriorPointSolver::solve with crossover off, golden fixtures produced by
+the reference), plus the behaviour pins of tests/unit/test_lp.cpp.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import lpgen
+import oracle as O
+import refcases as R
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(__file__)
+GOLD = np.load(os.path.join(HERE, "golden", "reference_golden.npz"))
+NSCAL = 8
+AP, AD, MU, NRP, NRD, MUAFF, SIGMA, FLAGS = 3, 4, 2, 0, 1, 5, 6, 7
+
+
+def tens(torch, a):
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
+
+
+@pytest.fixture(scope="module")
+def setup(hn, torch_cuda):
+    torch = torch_cuda
+    lp = lpgen.scaled_problem(lpgen.lp_uniform(2000, 5000, 8, seed=0))
+    m, n = lp["m"], lp["n"]
+    A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
+    rng = np.random.default_rng(5)
+    st = {"x": rng.uniform(0.1, 3.0, n), "z": rng.uniform(0.1, 3.0, n), "lam": rng.standard_normal(m)}
+    st["z"][::97] = 1e-14  # drives D above the 1e10 clamp
+    return lp, A, st
+
+
+def lib(hn):
+    return hn.load()
+
+
+def test_residuals_and_scaling(hn, torch_cuda, setup):
+    torch = torch_cuda
+    lp, A, st = setup
+    m, n = lp["m"], lp["n"]
+    x, z, lam = tens(torch, st["x"]), tens(torch, st["z"]), tens(torch, st["lam"])
+    b, c = tens(torch, lp["b"]), tens(torch, lp["c"])
+    mx, rp, rd, D, Drd = (torch.empty(k, dtype=torch.float64, device="cuda") for k in (m, m, n, n, n))
+    scal = torch.zeros(NSCAL, dtype=torch.float64, device="cuda")
+    hn.check(lib(hn).hn_ipm_residuals(A.h, x.data_ptr(), lam.data_ptr(), z.data_ptr(), b.data_ptr(), c.data_ptr(),
+                                      mx.data_ptr(), rp.data_ptr(), rd.data_ptr(), D.data_ptr(), Drd.data_ptr(),
+                                      scal.data_ptr(), None))
+    torch.cuda.synchronize()
+    rp_h, rd_h, mx_h = rp.cpu().numpy(), rd.cpu().numpy(), mx.cpu().numpy()
+    Mx = O.multiply(lp["rp"], lp["ci"], lp["val"], st["x"])
+    R.normwise_close(mx_h, Mx, lp["rp"], lp["ci"], lp["val"], st["x"])
+    assert np.array_equal(rp_h, mx_h - lp["b"])                                      # :512
+    t = O.matvec_t(lp["rp"], lp["ci"], lp["val"], st["lam"], n)
+    rpT, ciT, valT = O.transposed(lp["rp"], lp["ci"], lp["val"], n)
+    rows = np.repeat(np.arange(n), np.diff(rpT))
+    scale = np.bincount(rows, weights=np.abs(valT * st["lam"][ciT]), minlength=n)
+    err = np.abs(rd_h - ((t + st["z"]) - lp["c"]))                                  # :514-515
+    assert np.all(err <= 1e-12 * (scale + np.abs(st["z"]) + np.abs(lp["c"])))
+    Dref = st["x"] / st["z"]                                                         # :532-539
+    Dref[~(Dref >= 0.0) | ~np.isfinite(Dref) | (Dref > 1e10)] = 1e10
+    assert np.array_equal(D.cpu().numpy(), Dref)
+    assert np.array_equal(Drd.cpu().numpy(), Dref * rd_h)
+    s = scal.cpu().numpy()
+    assert s[NRP] == O.norm_inf(rp_h) and s[NRD] == O.norm_inf(rd_h)
+    assert abs(s[MU] - O.dot(st["x"], st["z"]) / n) <= 1e-13 * s[MU]
+
+
+def test_direction_steps_corrector_update(hn, torch_cuda, setup):
+    torch = torch_cuda
+    lp, A, st = setup
+    m, n = lp["m"], lp["n"]
+    rng = np.random.default_rng(9)
+    D_h = rng.uniform(0.01, 10, n)
+    rd_h = rng.standard_normal(n)
+    dlam_h = rng.standard_normal(m)
+    x, z, lam = tens(torch, st["x"]), tens(torch, st["z"]), tens(torch, st["lam"])
+    D, rd, dlam = tens(torch, D_h), tens(torch, rd_h), tens(torch, dlam_h)
+    dx, dz, zs = (torch.empty(n, dtype=torch.float64, device="cuda") for _ in range(3))
+    pred, rhs = tens(torch, rng.standard_normal(m)), torch.empty(m, dtype=torch.float64, device="cuda")
+    scal = torch.zeros(NSCAL, dtype=torch.float64, device="cuda")
+    scal[MU] = 0.37
+    L = lib(hn)
+    hn.check(L.hn_ipm_direction(A.h, dlam.data_ptr(), D.data_ptr(), rd.data_ptr(), x.data_ptr(), None,
+                                dx.data_ptr(), dz.data_ptr(), None))
+    t = torch.empty(n, dtype=torch.float64, device="cuda")
+    A.spmv(dlam, t, trans=1)
+    torch.cuda.synchronize()
+    u = t.cpu().numpy() + rd_h
+    assert np.array_equal(dx.cpu().numpy(), D_h * u - st["x"])                      # :609-615
+    assert np.array_equal(dz.cpu().numpy(), -u)
+    hn.check(L.hn_ipm_step_lengths(n, m, x.data_ptr(), dx.data_ptr(), z.data_ptr(), dz.data_ptr(),
+                                   dlam.data_ptr(), scal.data_ptr(), None))
+    s = scal.cpu().numpy()
+    dx_h, dz_h = dx.cpu().numpy(), dz.cpu().numpy()
+    assert s[AP] == O.max_step(st["x"], dx_h) and s[AD] == O.max_step(st["z"], dz_h)  # :629-630
+    assert s[FLAGS] == 0.0
+    hn.check(L.hn_ipm_corrector(A.h, x.data_ptr(), dx.data_ptr(), z.data_ptr(), dz.data_ptr(), pred.data_ptr(),
+                                zs.data_ptr(), rhs.data_ptr(), scal.data_ptr(), None))
+    s = scal.cpu().numpy()
+    mu_aff = O.dot(st["x"] + s[AP] * dx_h, st["z"] + s[AD] * dz_h) / n             # :632-636
+    assert abs(s[MUAFF] - mu_aff) <= 1e-12 * abs(mu_aff)
+    sig = min(max((s[MUAFF] / 0.37) ** 3, 0.1), 0.9)                                 # :638-643
+    assert abs(s[SIGMA] - sig) <= 4e-16 * sig
+    zs_ref = (s[SIGMA] * 0.37 - dx_h * dz_h) * (1.0 / st["z"])                     # :645-651
+    assert np.array_equal(zs.cpu().numpy(), zs_ref)
+    Mz = O.multiply(lp["rp"], lp["ci"], lp["val"], zs_ref)                         # :652-656
+    rows = np.repeat(np.arange(m), np.diff(lp["rp"]))
+    scale = np.bincount(rows, weights=np.abs(lp["val"] * zs_ref[lp["ci"]]), minlength=m)
+    pred_h = pred.cpu().numpy()
+    assert np.all(np.abs(rhs.cpu().numpy() - (pred_h - Mz)) <= 1e-12 * (scale + np.abs(pred_h)))
+    hn.check(L.hn_ipm_update(n, m, x.data_ptr(), dx.data_ptr(), z.data_ptr(), dz.data_ptr(), lam.data_ptr(),
+                             dlam.data_ptr(), scal.data_ptr(), None))
+    assert np.array_equal(x.cpu().numpy(), st["x"] + s[AP] * dx_h)                  # :690-696
+    assert np.array_equal(z.cpu().numpy(), st["z"] + s[AD] * dz_h)
+    assert np.array_equal(lam.cpu().numpy(), st["lam"] + s[AD] * dlam_h)
+
+
+def test_guards_raise_flags(hn, torch_cuda):
+    torch = torch_cuda
+    n, m = 1000, 10
+    x = torch.ones(n, dtype=torch.float64, device="cuda")
+    dx = torch.zeros(n, dtype=torch.float64, device="cuda")
+    dx[17] = float("nan")
+    dlam = torch.zeros(m, dtype=torch.float64, device="cuda")
+    scal = torch.zeros(NSCAL, dtype=torch.float64, device="cuda")
+    L = lib(hn)
+    hn.check(L.hn_ipm_step_lengths(n, m, x.data_ptr(), dx.data_ptr(), x.data_ptr(), dx.data_ptr(),
+                                   dlam.data_ptr(), scal.data_ptr(), None))
+    torch.cuda.synchronize()
+    assert scal.cpu().numpy().view(np.uint64)[FLAGS] & 1
+    scal.zero_()
+    scal[AP] = 1.0
+    scal[AD] = 1.0
+    dx.fill_(-2.0)  # x + dx < 0 -> guard of :698-708
+    hn.check(L.hn_ipm_update(n, m, x.data_ptr(), dx.data_ptr(), x.data_ptr(), dx.data_ptr(), dlam.data_ptr(),
+                             dlam.data_ptr(), scal.data_ptr(), None))
+    torch.cuda.synchronize()
+    assert scal.cpu().numpy().view(np.uint64)[FLAGS] & 2
+
+
+def test_max_step_matches_reference_function(hn, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(4)
+    v, d = rng.uniform(0.1, 2, 100000), rng.standard_normal(100000)
+    out = torch.empty(1, dtype=torch.float64, device="cuda")
+    hn.check(lib(hn).hn_max_step(100000, tens(torch, v).data_ptr(), tens(torch, d).data_ptr(), out.data_ptr(), None))
+    torch.cuda.synchronize()
+    assert out.item() == O.max_step(v, d)
+
+
+def rel(a, b):
+    return abs(a - b) / (1.0 + abs(b))
+
+
+@pytest.mark.parametrize("name,args", [("ipm_60x150", (60, 150, 8, 3)), ("ipm_200x500", (200, 500, 8, 4))])
+def test_gpu_ipm_matches_reference_golden(hn, name, args):
+    g = GOLD[name]
+    r = hn.lp_solve(lpgen.lp_uniform(*args))
+    assert r["status"] == int(g[0]), r
+    assert rel(r["objective"], g[1]) <= 1e-8, (r["objective"], g[1])
+    assert abs(r["iterations"] - int(g[2])) <= 3
+
+
+def test_gpu_ipm_config0_matches_reference():
+    path = os.path.join(HERE, "golden", "reference_ipm_c0.json")
+    if not os.path.exists(path):
+        pytest.skip("reference result for the m=2000 LP not generated")
+    import hnb200 as hn
+
+    ref = json.load(open(path))["lp_uniform_2000_5000_8_seed0"]
+    r = hn.lp_solve(lpgen.lp_uniform(2000, 5000, 8, 0))
+    assert r["status"] == ref["status"] and rel(r["objective"], ref["objective"]) <= 1e-8, (r, ref)
+
+
+def two_var_lp():
+    # test_lp.cpp:244-258: max x1 + 2 x2, x1 + x2 <= 10, x1 (+0 x2) <= 5, 0 <= x <= 10
+    lp = {"m": 2, "n": 2, "rp": np.array([0, 2, 4]), "ci": np.array([0, 1, 0, 1]),
+          "val": np.array([1.0, 1.0, 1.0, 0.0]), "b": np.array([10.0, 5.0]), "c": np.array([1.0, 2.0])}
+    return lp, dict(sense=np.array([0, 0]), ub=np.array([10.0, 10.0]), maximize=True)
+
+
+def test_known_answer_simple_lp(hn):
+    lp, kw = two_var_lp()
+    r = hn.lp_solve(lp, **kw)
+    assert r["status_name"] == "OPTIMAL" and abs(r["objective"] - 20.0) < 1e-6
+    if O.ref() is not None:
+        g = O.ref_ipm_solve(lp, **kw)
+        assert g["status"] == r["status"] and rel(r["objective"], g["objective"]) <= 1e-8
+
+
+def test_known_answer_larger_lp(hn):
+    # InteriorPointTest.LargerLP (test_lp.cpp:261-285)
+    rp, ci = [0], []
+    for _ in range(20):
+        ci += list(range(0, 50, 5))
+        rp.append(len(ci))
+    lp = {"m": 20, "n": 50, "rp": np.array(rp), "ci": np.array(ci), "val": np.ones(len(ci)),
+          "b": np.full(20, 10.0), "c": np.ones(50)}
+    kw = dict(sense=np.zeros(20), ub=np.full(50, 100.0), maximize=True)
+    r = hn.lp_solve(lp, **kw)
+    assert r["status_name"] == "OPTIMAL"
+    if O.ref() is not None:
+        g = O.ref_ipm_solve(lp, **kw)
+        assert g["status"] == r["status"] and rel(r["objective"], g["objective"]) <= 1e-8
+
+
+def test_iteration_limit_reports_incumbent(hn):
+    # IterationLimitReportsIncumbent (test_lp.cpp:306-325)
+    lp, kw = two_var_lp()
+    r = hn.lp_solve(lp, max_iter=1, **kw)
+    assert r["status_name"] == "ITER_LIMIT" and r["x"].shape == (2,) and r["objective"] != 0.0
+
+
+def test_interrupt_callback(hn):
+    # InterruptCallback (test_lp.cpp:287-304)
+    lp, kw = two_var_lp()
+    r = hn.lp_solve(lp, interrupt=lambda: True, **kw)
+    assert r["status_name"] == "INTERRUPTED"
+
+
+def test_time_limit(hn):
+    lp = lpgen.lp_uniform(2000, 5000, 8, 0)
+    r = hn.lp_solve(lp, time_limit=1e-6)
+    assert r["status_name"] in ("TIME_LIMIT", "SUBOPTIMAL")
+
+
+def test_nonfinite_guard_never_returns_nan(hn):
+    # NonfiniteGuardNeverReturnsNaN (test_lp.cpp:402-434)
+    n = 12
+    rp, ci, val = [0], [], []
+    for i in range(6):
+        ci += list(range(n))
+        val += [1e6 * (j + 1) for j in range(n)]
+        rp.append(len(ci))
+    lp = {"m": 6, "n": n, "rp": np.array(rp), "ci": np.array(ci), "val": np.array(val),
+          "b": np.array([1e7 * (i + 1) for i in range(6)]), "c": np.array([1e11 * (i + 1) for i in range(n)])}
+    r = hn.lp_solve(lp, sense=np.zeros(6), ub=np.full(n, 1e8), maximize=True)
+    assert r["status_name"] != "UNKNOWN"
+    assert np.isfinite(r["objective"]) and np.all(np.isfinite(r["x"]))
+
+
+def test_bounded_and_ge_rows_match_reference(hn):
+    if O.ref() is None:
+        pytest.skip("oracle/_ref not built")
+    lp = lpgen.lp_uniform(150, 400, 6, seed=12)
+    rng = np.random.default_rng(3)
+    sense = rng.integers(0, 3, size=150)
+    b = lp["b"] + np.where(sense == 0, 1.0, np.where(sense == 1, -1.0, 0.0))
+    ub = np.where(rng.random(400) < 0.3, lp["x0"] + 1.0, np.inf)
+    lp2 = dict(lp, b=b)
+    g = O.ref_ipm_solve(lp2, sense=sense, ub=ub)
+    r = hn.lp_solve(lp2, sense=sense, ub=ub)
+    assert r["status"] == g["status"] and rel(r["objective"], g["objective"]) <= 1e-8, (r["objective"], g)
+
+
+# ---------------------------------------------------------------- IComputeBackend contract
+def test_backend_reference_cases(hn):
+    be = hn.Backend()
+    for args in [(1500, 1200, 0.003, 77), (300, 800, 0.08, 4242)]:  # test_gpu_backend.cpp:211-234
+        rp, ci, val, x = R.make_problem(*args)
+        R.expect_close(be.spmv(rp, ci, val, x), O.multiply(rp, ci, val, x), 1e-10)
+    rp, ci, val, _ = R.make_problem(400, 300, 0.05, 2024)                      # :260-277
+    B = R.uniform(8, 300 * 5, -1.0, 1.0)
+    R.expect_close(be.spmm(rp, ci, val, B, 5), O.spmm(rp, ci, val, B, 5), 1e-10)
+    y = be.spmv(np.array([0]), np.zeros(0), np.zeros(0), np.zeros(0))       # EmptyMatrixIsSafe :126-131
+    assert y.shape == (0,)
+    rng = np.random.default_rng(2)
+    a, b = rng.standard_normal(20000), rng.standard_normal(20000)
+    assert abs(be.dot(a, b) - O.dot(a, b)) <= 1e-12 * np.abs(a * b).sum()
+    assert np.array_equal(be.axpy(0.5, a, b), O.axpy(0.5, a, b))
+    assert be.norm_inf(a) == O.norm_inf(a)
+    assert be.kernel_executions() > 0
+    be.close()
+
+
+def test_backend_residency_reused(hn):
+    # MatrixResidencyIsReused (:279-292): the second call uploads nothing
+    be = hn.Backend()
+    rp, ci, val, x = R.make_problem(2000, 1500, 0.03, 555)
+    y1 = be.spmv(rp, ci, val, x)
+    free1 = hn.device_info().free_mem
+    y2 = be.spmv(rp, ci, val, x)
+    free2 = hn.device_info().free_mem
+    assert free2 <= free1 + (1 << 20) and free2 >= free1 - (1 << 20)
+    assert np.array_equal(y1, y2)
+    # new contents, same shape: not served from the stale copy
+    y3 = be.spmv(rp, ci, val * 2.0, x)
+    R.expect_close(y3, 2.0 * y1, 1e-12)
+    t = be.spmv_t(rp, ci, val, np.ones(2000), 1500)
+    R.expect_close(t, O.tmultiply(rp, ci, val, np.ones(2000), 1500), 1e-12)
+    be.close()
