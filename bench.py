@@ -96,10 +96,11 @@ def dist_setup():
     return rank, world, local
 
 
-def make_inputs(seed: int):
+def make_inputs(seed: int, scale: int = 1):
     import lpgen
 
-    lp = lpgen.scaled_problem(lpgen.lp_zipf(seed=seed))
+    lp = lpgen.scaled_problem(lpgen.lp_zipf(m=200_000 // scale, n=500_000 // scale, seed=seed,
+                                            target_nnz=5_000_000 // scale))
     rng = np.random.default_rng(seed + 1)
     m, n = lp["m"], lp["n"]
     vec = {"x": rng.uniform(0.5, 2.0, n), "z": rng.uniform(0.5, 2.0, n), "lam": rng.standard_normal(m)}
@@ -249,9 +250,79 @@ def run_ours(args, rank, world, local):
                          "peak_source": how, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None},
             "clocks": clk,
         }
+        if not args.no_ipm:
+            result["plain_ipm"] = plain_ipm()
         if not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(lp, vec, threads=os.cpu_count() or 1, reps=1)
     return result
+
+
+def plain_ipm():
+    """One solve of the m=2000, n=5000, 8 nonzeros/column LP (seed 0) by the
+    plain GPU IPM (crossover off), against the reference's stored result."""
+    import hnb200 as hn
+    import lpgen
+
+    lp = lpgen.lp_uniform(2000, 5000, 8, 0)
+    r = hn.lp_solve(lp)
+    ref = None
+    gp = os.path.join(ROOT, "tests", "golden", "reference_ipm_c0.json")
+    if os.path.exists(gp):
+        ref = json.load(open(gp))["lp_uniform_2000_5000_8_seed0"]
+    out = {"lp": "m=2000 n=5000 8 nnz/col seed 0", "status": r["status_name"], "iterations": r["iterations"],
+           "objective": r["objective"], "ms": round(r["time_ms"], 1), "solves_per_s": round(1e3 / r["time_ms"], 3),
+           "factor_ms": round(r["factor_ms"], 1), "device_ms": round(r["device_ms"], 1),
+           "host_threads": os.cpu_count()}
+    if ref:
+        out["reference"] = {"status": ref["status"], "objective": ref["objective"], "iterations": ref["iterations"],
+                            "ms": round(ref["time_ms"], 1), "rel_obj_diff": abs(r["objective"] - ref["objective"]) /
+                            (1.0 + abs(ref["objective"]))}
+    return out
+
+
+def run_only(args, local):
+    """Single kernel group on the same LP (profiling aid). spmv / spmv_t flush
+    L2 between launches by writing a 256 MB buffer; ada streams 11.6 GB."""
+    import torch
+
+    import hnb200 as hn
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    torch.zeros(1, device=dev)
+    hn.init(local)
+    lp, vec = make_inputs(1000, args.scale)
+    m, n = lp["m"], lp["n"]
+    A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    flush = torch.empty(32 * 1024 * 1024, dtype=torch.float64, device=dev)
+    if args.only == "ada":
+        P = hn.Pattern(A)
+        D = torch.as_tensor(vec["D"], device=dev)
+        nval = torch.empty(P.nnz, dtype=torch.float64, device=dev)
+        nbytes = step_bytes(m, n, A.nnz, A.nnz_t, P.nnz)["ada_numeric"]
+        fn = lambda: P.numeric(D, 1e-8, nval, None, sp)  # noqa: E731
+    else:
+        trans = 1 if args.only == "spmv_t" else 0
+        xin = torch.as_tensor(vec["lam"] if trans else vec["x"], device=dev)
+        yout = torch.empty(n if trans else m, dtype=torch.float64, device=dev)
+        nbytes = step_bytes(m, n, A.nnz, A.nnz_t, 0)["spmv_At" if trans else "spmv_A"] - (0 if trans else 8 * m)
+        fn = lambda: A.spmv(xin, yout, trans=trans, stream=sp)  # noqa: E731
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for _ in range(args.warmup):
+        flush.zero_()
+        fn()
+    for i in range(args.steps):
+        flush.zero_()
+        evs[i][0].record(stream)
+        fn()
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+    hbm, how = peaks()
+    return {"only": args.only, "scale": args.scale, "m": m, "n": n, "nnz": A.nnz, "ms": round(ms, 4), "bytes": nbytes, "GB/s": round(nbytes / (ms * 1e-3) / 1e9, 1),
+            "frac_of_" + how + "_hbm": round(nbytes / (ms * 1e-3) / 1e9 / hbm, 4)}
 
 
 def cpu_baseline(lp, vec, threads: int, reps: int):
@@ -306,6 +377,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", default="step", choices=["step", "spmv", "spmv_t", "ada"],
+                    help="time one kernel group alone (for profiling); 'step' is the measured workload")
+    ap.add_argument("--no-ipm", action="store_true", help="skip the plain GPU IPM solve on the m=2000 LP")
+    ap.add_argument("--scale", type=int, default=1, help="--only modes: shrink the LP by this factor (profiling)")
     args = ap.parse_args()
     rank, world, local = dist_setup()
     if args.impl == "reference":
@@ -320,7 +395,7 @@ def main():
 
         torch.cuda.set_device(local)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    out = run_ours(args, rank, world, local)
+    out = run_only(args, local) if args.only != "step" else run_ours(args, rank, world, local)
     if world > 1:
         import torch
 

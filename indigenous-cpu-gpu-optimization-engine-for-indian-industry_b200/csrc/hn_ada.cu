@@ -41,6 +41,7 @@ constexpr uint32_t kMulti = 0x80000000u;
 constexpr int64_t kDiagFlag = int64_t(1) << 62;
 constexpr int kEntryChunk = 512;  // row entries of A staged per pass of the numeric kernel
 constexpr int kStage = 6144;      // N row slots staged in shared memory (longer rows write directly)
+constexpr int kUnroll = 8;        // contributions per thread per trip of the numeric kernel
 
 __device__ __forceinline__ uint32_t bit_of(int k) { return 1u << (k & 31); }
 
@@ -278,26 +279,48 @@ __global__ void __launch_bounds__(kT) ada_stage_kernel(
             if (threadIdx.x == 0) s.cs[ne] = static_cast<int32_t>(total);
             __syncthreads();
             const int Qc = static_cast<int>(total);
-            for (int qq = threadIdx.x; qq < Qc; qq += kT) {
-                // entry of contribution qq: last t with cs[t] <= qq
-                int lo = 0, hi = ne - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (s.cs[mid] <= qq)
-                        lo = mid;
-                    else
-                        hi = mid - 1;
+            // kUnroll contributions per thread per trip: all their loads are
+            // issued before any is used, so each thread keeps 2*kUnroll loads
+            // in flight instead of one dependent pair
+            for (int base = 0; base < Qc; base += kT * kUnroll) {
+                uint32_t tgt[kUnroll];
+                double aT[kUnroll], coef[kUnroll], dd[kUnroll];
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    const int qq = base + u * kT + threadIdx.x;
+                    tgt[u] = 0u;
+                    aT[u] = 0.0;
+                    coef[u] = 0.0;
+                    dd[u] = 0.0;
+                    if (qq < Qc) {
+                        // entry of contribution qq: last t with cs[t] <= qq
+                        int lo = 0, hi = ne - 1;
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (s.cs[mid] <= qq)
+                                lo = mid;
+                            else
+                                hi = mid - 1;
+                        }
+                        const int p = s.pc[lo] + (qq - s.cs[lo]);
+                        tgt[u] = __ldcs(map + q0 + qq);
+                        aT[u] = __ldg(valT + p);
+                        coef[u] = s.a[lo];
+                        dd[u] = s.d[lo];
+                    }
                 }
-                const int p = s.pc[lo] + (qq - s.cs[lo]);
-                const uint32_t tgt = map[q0 + qq];
-                const double dj = s.d[lo];
-                const double v = (dj <= 0.0) ? 0.0 : (s.a[lo] * valT[p]) * dj;
-                if (tgt & kMulti)
-                    scratch[tgt & ~kMulti] = v;
-                else if (staged)
-                    stage[static_cast<int64_t>(tgt) - row0] = v;
-                else
-                    nval[tgt] = v;
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    const int qq = base + u * kT + threadIdx.x;
+                    if (qq >= Qc) continue;
+                    const double v = (dd[u] <= 0.0) ? 0.0 : (coef[u] * aT[u]) * dd[u];
+                    if (tgt[u] & kMulti)
+                        scratch[tgt[u] & ~kMulti] = v;
+                    else if (staged)
+                        stage[static_cast<int64_t>(tgt[u]) - row0] = v;
+                    else
+                        nval[tgt[u]] = v;
+                }
             }
             q0 += total;
             __syncthreads();

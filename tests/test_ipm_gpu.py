@@ -154,7 +154,8 @@ def test_max_step_matches_reference_function(hn, torch_cuda):
     rng = np.random.default_rng(4)
     v, d = rng.uniform(0.1, 2, 100000), rng.standard_normal(100000)
     out = torch.empty(1, dtype=torch.float64, device="cuda")
-    hn.check(lib(hn).hn_max_step(100000, tens(torch, v).data_ptr(), tens(torch, d).data_ptr(), out.data_ptr(), None))
+    vd, dd = tens(torch, v), tens(torch, d)  # keep both alive while the kernel runs
+    hn.check(lib(hn).hn_max_step(100000, vd.data_ptr(), dd.data_ptr(), out.data_ptr(), None))
     torch.cuda.synchronize()
     assert out.item() == O.max_step(v, d)
 
