@@ -24,7 +24,7 @@
 namespace hn {
 
 constexpr int kSpmvThreads = 256;
-constexpr int kSpmvIpt = 8;
+constexpr int kSpmvIpt = 7;  // odd: lanes reading their items from the product buffer fall on different banks
 constexpr int kSpmvTile = kSpmvThreads * kSpmvIpt;
 
 struct SpmvMat {
