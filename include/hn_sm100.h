@@ -214,6 +214,20 @@ int hn_ipm_update(int64_t n, int64_t m, double* x_dev, const double* dx_dev, dou
 /* *result_dev = min(1, 0.99 * min_{d_i<0} -v_i/d_i) (max_step, :134-142). */
 int hn_max_step(int64_t n, const double* v_dev, const double* d_dev, double* result_dev, void* stream);
 
+/* ---- SpMV for callers that cannot allocate device memory ----
+ * No counterpart in the reference. y = A x with A given as device CSR arrays
+ * (int32 row_ptr m+1, int32 col_idx and double values nnz, row_ptr[m] == nnz,
+ * column indices < n -- not checked on the device). It allocates nothing:
+ * the merge-path tile table and carries live in one fixed 2 MB __device__
+ * array, which bounds m + nnz to 117,440,512 (larger sizes fail with
+ * HN_ERR_INVALID_ARG). It is for callers whose device memory belongs to
+ * another allocator or that must not call cudaMalloc inside a solve loop.
+ * The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race. */
+int hn_spmv_noalloc(int64_t m, int64_t n, int64_t nnz, const int32_t* row_ptr_dev, const int32_t* col_idx_dev,
+                    const double* val_dev, const double* x_dev, double* y_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -86,6 +86,7 @@ SIGNATURES = {
     "hn_ipm_corrector": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "hn_ipm_update": [_i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "hn_max_step": [_i64, _vp, _vp, _vp, _vp],
+    "hn_spmv_noalloc": [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp],
 }
 _RESTYPE = {"hn_last_error": C.c_char_p}
 
