@@ -51,6 +51,23 @@ int hn_lp_solve(int64_t m, int64_t n, const uint64_t* row_ptr, const uint64_t* c
                 int maximize, double obj_offset, const hn_ipm_options* opt, hn_ipm_result* res, double* x_out);
 const char* hn_host_last_error(void);
 
+/* K LPs solved in lockstep by the batched GPU IPM (hn::lp::BatchInteriorPointSolver).
+ * Instance i: rows row_off[i]..row_off[i+1] of b/sense, columns
+ * col_off[i]..col_off[i+1] of c/lb/ub/x_out, nonzeros nnz_off[i]..nnz_off[i+1]
+ * of col_idx/val (column indices local to the instance), and row pointer
+ * entries row_off[i]+i .. row_off[i+1]+i+1 of row_ptr (local, starting at 0).
+ * Per-instance outputs: status (model::ProblemStatus), objective, iterations. */
+typedef struct hn_batch_stats {
+    int64_t rows, cols, nnz, nnz_normal;
+    int64_t iterations;
+    double total_ms, factor_ms, solve_ms;
+} hn_batch_stats;
+int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off, const int64_t* nnz_off,
+                      const uint64_t* row_ptr, const uint64_t* col_idx, const double* val, const double* c,
+                      const double* b, const int* sense, const double* lb, const double* ub, const int* maximize,
+                      const double* obj_offset, const hn_ipm_options* opt, int* status, double* objective,
+                      int64_t* iterations, double* x_out, hn_batch_stats* stats);
+
 /* B200Backend through C: the matrix arrives as the reference's three vectors
  * each call; the backend keeps it resident between calls. */
 typedef struct hn_backend hn_backend;

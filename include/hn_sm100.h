@@ -149,7 +149,9 @@ int hn_nrm2(int64_t n, const double* v_dev, double* result_dev, void* stream);
  * (build_normal_equations, interior_point.cpp:144-200)
  * Symbolic: the pattern of A A^T plus the full diagonal, both triangles,
  * columns sorted (the pattern the reference builds when every d_j > 0).
- * Needs the handle's A^T. m up to 1,500,000. */
+ * Needs the handle's A^T. Each row of N may reach at most 400,000 columns
+ * (the span from its smallest to its largest k; block-diagonal batches are
+ * limited by their largest block only), and nnz(N) < 2^31. */
 int hn_ada_symbolic(const hn_csr* A, hn_pattern** out);
 int hn_pattern_info(const hn_pattern* P, int64_t* m, int64_t* nnz);
 /* Host copy of the pattern: rp m+1, ci nnz (reference layout). */
@@ -213,6 +215,52 @@ int hn_ipm_update(int64_t n, int64_t m, double* x_dev, const double* dx_dev, dou
                   void* stream);
 /* *result_dev = min(1, 0.99 * min_{d_i<0} -v_i/d_i) (max_step, :134-142). */
 int hn_max_step(int64_t n, const double* v_dev, const double* d_dev, double* result_dev, void* stream);
+
+/* ---- batched Mehrotra IPM (many LPs advanced in lockstep) ----
+ * The instances are packed as one block-diagonal matrix: instance i owns rows
+ * row_off[i]..row_off[i+1] and columns col_off[i]..col_off[i+1] of M (an
+ * hn_csr with A^T) and the matching block of P = hn_ada_symbolic(M). The
+ * SpMV-based kernels above (hn_ipm_rhs, hn_ipm_direction) run unchanged on
+ * the packed vectors; these entry points add what is per instance. `scal`
+ * is double[K * HN_IPM_NSCAL] (one scalar block per instance), `status`
+ * int32[K] (0 = iterating, else a model::ProblemStatus value: 1 converged,
+ * 7 numerical error) and `iters` int32[K]; a non-zero status masks the
+ * instance out of the factorisation, solves and update. No reference
+ * counterpart exists (the reference solves one LP at a time,
+ * interior_point.cpp:402-886); each step restates the lines cited in the
+ * single-LP kernels. The normal equations are factorised on the GPU (dense
+ * blocked LDL^T per instance, pivot clamp of factorization.cpp:1299-1305). */
+typedef struct hn_batch hn_batch;
+int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_off_host, const hn_pattern* P,
+                    hn_batch** out);
+int hn_batch_destroy(hn_batch* B);
+/* rp = M x - b, rd = M^T lam + z - c, per-instance mu / norms, D, Drd; an
+ * iterating instance that meets the tolerances becomes status 1 with
+ * iters = iter (:507-539). */
+int hn_batch_residuals(hn_batch* B, const hn_csr* M, const double* x_dev, const double* lam_dev,
+                       const double* z_dev, const double* b_dev, const double* c_dev, double* mx_dev, double* rp_dev,
+                       double* rd_dev, double* D_dev, double* Drd_dev, double* scal_dev, int32_t* status_dev,
+                       int32_t* iters_dev, int iter, double tol, double ctol, void* stream);
+/* N = A D A^T + dyn_reg_i I per instance (:144-200), then the dense LDL^T of
+ * every iterating instance. nval_dev: nnz(P) doubles. */
+int hn_batch_factor(hn_batch* B, const double* D_dev, double reg, double singular_tol, double* nval_dev,
+                    const int32_t* status_dev, void* stream);
+/* x = N^-1 rhs per iterating instance, with iterative refinement against N
+ * (refinement.cpp:7-37: <= 5 sweeps, 1e-10 relative). */
+int hn_batch_solve(hn_batch* B, const double* nval_dev, const double* rhs_dev, double* x_dev,
+                   const int32_t* status_dev, void* stream);
+/* per-instance step lengths (:134-142) and non-finite guard (:617-627). */
+int hn_batch_steps(hn_batch* B, const double* x_dev, const double* dx_dev, const double* z_dev,
+                   const double* dz_dev, const double* dlam_dev, double* scal_dev, int32_t* status_dev, void* stream);
+/* per-instance mu_aff, sigma, zs, then rhs = rhs_pred - M zs (:632-659). */
+int hn_batch_corrector(hn_batch* B, const hn_csr* M, const double* x_dev, const double* dx_dev, const double* z_dev,
+                       const double* dz_dev, const double* rhs_pred_dev, double* zs_dev, double* rhs_dev,
+                       double* scal_dev, const int32_t* status_dev, void* stream);
+/* x += ap dx, z += ad dz, lam += ad dlam for iterating instances; iters = iter+1,
+ * or status 7 on a negative / non-finite iterate (:690-708). */
+int hn_batch_update(hn_batch* B, double* x_dev, const double* dx_dev, double* z_dev, const double* dz_dev,
+                    double* lam_dev, const double* dlam_dev, const double* scal_dev, int32_t* status_dev,
+                    int32_t* iters_dev, int iter, void* stream);
 
 /* ---- SpMV for callers that cannot allocate device memory ----
  * No counterpart in the reference. y = A x with A given as device CSR arrays

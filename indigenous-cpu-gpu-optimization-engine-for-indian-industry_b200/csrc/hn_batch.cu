@@ -1,0 +1,792 @@
+// Batched Mehrotra IPM: many LPs of uneven sizes advanced in lockstep.
+//
+// The instances are packed as one block-diagonal CSR M = diag(M_1 .. M_K)
+// (rows row_off[i]..row_off[i+1], columns col_off[i]..col_off[i+1]), so the
+// merge-path SpMVs with their IPM epilogues, the device A^T and the A D A^T
+// assembly run on the whole batch in single launches (the assembly's
+// per-row windows keep its bitmaps to one block). What differs per instance
+// lives here:
+//   - reductions per instance (one CTA each): mu, ||rp||_inf, ||rd||_inf, step
+//     lengths, mu_aff, sigma -- the scalars of interior_point.cpp:517-530,
+//     :629-643, :683-684 -- in a K x HN_IPM_NSCAL block, plus a per-instance
+//     status word (0 = iterating) that masks converged or failed instances out
+//     of the factorisation, the solves and the update;
+//   - dyn_reg = max(reg, 1e-12 * max diag) per instance (:188-196);
+//   - the normal-equation factorisation: each instance's N block is scattered
+//     into a dense lower triangle and factorised by a blocked LDL^T on the GPU
+//     with the reference's pivot clamp (factorization.cpp:1299-1305), level-
+//     synchronously: per 32-column block step one launch factorises every
+//     instance's diagonal block and panel, one launch spreads all instances'
+//     trailing tiles over the GPU. This is a deliberate deviation from keeping
+//     factorisations on the host: thousands of factorisations per iteration
+//     do not fit in host time;
+//   - the two triangular solves and iterative refinement
+//     (refinement.cpp:7-37: up to 5 sweeps, stop at 1e-10 relative) per
+//     instance, with N x as one merge-path SpMV over the packed N.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "hn_spmv.cuh"
+
+struct hn_batch {
+    int64_t K = 0, m = 0, n = 0;
+    const hn_pattern* P = nullptr;
+    int64_t* row_off = nullptr;  // K+1
+    int64_t* col_off = nullptr;  // K+1
+    int32_t* row_inst = nullptr; // m
+    int64_t* dn_off = nullptr;   // K+1, offsets of the dense blocks
+    int32_t* order = nullptr;    // instances by decreasing size
+    double* dense = nullptr;     // sum m_i^2
+    double* dD = nullptr;        // LDL^T pivots, m
+    unsigned* ticket = nullptr;  // queue counters
+    int32_t* refine = nullptr;   // per-instance refinement flag (1 = keep sweeping)
+    int32_t* nref = nullptr;     // number of instances still refining
+    // N as an SpMV operand (int32 row pointer copy + merge-path tables)
+    int32_t* nrp = nullptr;
+    int64_t ntiles = 0;
+    int32_t *tile_row = nullptr, *tile_nz = nullptr, *carry_row = nullptr, *head_row = nullptr;
+    double *carry_val = nullptr, *head_val = nullptr;
+    double* r = nullptr;         // refinement residual, m
+    double* ax = nullptr;        // N x, m
+    // level schedule of the blocked factorisation: at block step s the
+    // instances order[0 .. cnt[s]) still have a block; step_pairs (offset
+    // pair_off[s]) holds, per such instance, the cumulative count of trailing
+    // 32x32 tile pairs, so one launch spreads every instance's tiles over the GPU
+    int64_t nsteps = 0;
+    std::vector<int32_t> step_cnt;       // host, nsteps
+    std::vector<int64_t> step_pairs_h;   // host, total pairs per step
+    std::vector<int64_t> pair_off_h;     // host, nsteps+1 offsets into step_pairs
+    int64_t* step_pairs = nullptr;       // device, cumulative pairs per (step, instance)
+};
+
+namespace hn {
+namespace {
+
+constexpr int kT = 256;
+constexpr int kNb = 32;
+constexpr int S_NRP = HN_IPM_NRP, S_NRD = HN_IPM_NRD, S_MU = HN_IPM_MU, S_AP = HN_IPM_AP, S_AD = HN_IPM_AD,
+              S_MUAFF = HN_IPM_MUAFF, S_SIGMA = HN_IPM_SIGMA;
+constexpr int ST_RUN = 0, ST_OPTIMAL = 1, ST_NUMERICAL = 7;
+
+__device__ __forceinline__ bool fin(double v) { return isfinite(v); }
+
+// ---- per-instance reductions ----
+__global__ void __launch_bounds__(kT) batch_prep_kernel(const int64_t* __restrict__ row_off,
+                                                        const int64_t* __restrict__ col_off,
+                                                        const double* __restrict__ x, const double* __restrict__ z,
+                                                        const double* __restrict__ rd, const double* __restrict__ rp,
+                                                        double* __restrict__ D, double* __restrict__ Drd,
+                                                        double* __restrict__ scal, int32_t* __restrict__ status,
+                                                        int32_t* __restrict__ iters, int iter, double tol,
+                                                        double ctol) {
+    __shared__ double sh[32];
+    const int64_t i = blockIdx.x;
+    const int64_t c0 = col_off[i], c1 = col_off[i + 1], r0 = row_off[i], r1 = row_off[i + 1];
+    double smu = 0.0, mrd = 0.0, mrp = 0.0;
+    for (int64_t j = c0 + threadIdx.x; j < c1; j += kT) {
+        const double xj = x[j], zj = z[j], r = rd[j];
+        smu += xj * zj;
+        mrd = fmax(mrd, fabs(r));
+        double d = xj / zj;
+        if (!(d >= 0.0) || !fin(d) || d > 1e10) d = 1e10;  // interior_point.cpp:532-539
+        D[j] = d;
+        Drd[j] = d * r;
+    }
+    for (int64_t k = r0 + threadIdx.x; k < r1; k += kT) mrp = fmax(mrp, fabs(rp[k]));
+    smu = block_sum<kT>(smu, sh);
+    mrd = block_max<kT>(mrd, sh);
+    mrp = block_max<kT>(mrp, sh);
+    if (threadIdx.x == 0) {
+        const double mu = smu / static_cast<double>(c1 - c0);
+        double* s = scal + i * HN_IPM_NSCAL;
+        s[S_MU] = mu;
+        s[S_NRD] = mrd;
+        s[S_NRP] = mrp;
+        if (status[i] == ST_RUN && mrp < tol && mrd < tol && mu < ctol) {  // :525-530
+            status[i] = ST_OPTIMAL;
+            iters[i] = iter;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kT) batch_steps_kernel(const int64_t* __restrict__ row_off,
+                                                         const int64_t* __restrict__ col_off,
+                                                         const double* __restrict__ x, const double* __restrict__ dx,
+                                                         const double* __restrict__ z, const double* __restrict__ dz,
+                                                         const double* __restrict__ dlam, double* __restrict__ scal,
+                                                         int32_t* __restrict__ status) {
+    __shared__ double sh[32];
+    __shared__ int s_bad;
+    const int64_t i = blockIdx.x;
+    if (status[i] != ST_RUN) return;
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    const int64_t c0 = col_off[i], c1 = col_off[i + 1], r0 = row_off[i], r1 = row_off[i + 1];
+    double ap = 1.0, ad = 1.0;
+    bool bad = false;
+    for (int64_t j = c0 + threadIdx.x; j < c1; j += kT) {
+        const double a = dx[j], b = dz[j];
+        if (a < 0.0) ap = fmin(ap, -x[j] / a);
+        if (b < 0.0) ad = fmin(ad, -z[j] / b);
+        bad |= !fin(a) || !fin(b);
+    }
+    for (int64_t k = r0 + threadIdx.x; k < r1; k += kT) bad |= !fin(dlam[k]);
+    if (bad) s_bad = 1;
+    ap = block_min<kT>(ap, sh);
+    ad = block_min<kT>(ad, sh);
+    if (threadIdx.x == 0) {
+        double* s = scal + i * HN_IPM_NSCAL;
+        const double sp = 0.99 * ap, sq = 0.99 * ad;  // max_step, :134-142
+        s[S_AP] = sp < 1.0 ? sp : 1.0;
+        s[S_AD] = sq < 1.0 ? sq : 1.0;
+        if (s_bad) status[i] = ST_NUMERICAL;  // :617-627, :676-686
+    }
+}
+
+// mu_aff, sigma and zs = (sigma mu - dx dz) (1/z) of one instance per CTA.
+__global__ void __launch_bounds__(kT) batch_corr_kernel(const int64_t* __restrict__ col_off,
+                                                        const double* __restrict__ x, const double* __restrict__ dx,
+                                                        const double* __restrict__ z, const double* __restrict__ dz,
+                                                        double* __restrict__ scal, const int32_t* __restrict__ status,
+                                                        double* __restrict__ zs) {
+    __shared__ double sh[32];
+    __shared__ double s_sm;
+    const int64_t i = blockIdx.x;
+    const int64_t c0 = col_off[i], c1 = col_off[i + 1];
+    double* s = scal + i * HN_IPM_NSCAL;
+    if (status[i] != ST_RUN) {
+        for (int64_t j = c0 + threadIdx.x; j < c1; j += kT) zs[j] = 0.0;
+        return;
+    }
+    const double ap = s[S_AP], ad = s[S_AD];
+    double acc = 0.0;
+    for (int64_t j = c0 + threadIdx.x; j < c1; j += kT) acc += (x[j] + ap * dx[j]) * (z[j] + ad * dz[j]);
+    acc = block_sum<kT>(acc, sh);
+    if (threadIdx.x == 0) {
+        const double mu_aff = acc / static_cast<double>(c1 - c0);  // :632-636
+        const double mu = s[S_MU];
+        double sigma;
+        if (!fin(mu_aff) || mu_aff < 0.0 || !(mu > 0.0)) {
+            sigma = 0.5;
+        } else {
+            const double r = pow(mu_aff / fmax(mu, 1e-300), 3.0);
+            sigma = r < 0.1 ? 0.1 : (r > 0.9 ? 0.9 : r);  // :638-643
+        }
+        s[S_MUAFF] = mu_aff;
+        s[S_SIGMA] = sigma;
+        s_sm = sigma * mu;
+    }
+    __syncthreads();
+    const double sm = s_sm;
+    for (int64_t j = c0 + threadIdx.x; j < c1; j += kT) {
+        const double zinv = 1.0 / z[j];
+        zs[j] = (sm - dx[j] * dz[j]) * zinv;  // :645-651
+    }
+}
+
+__global__ void __launch_bounds__(kT) batch_update_kernel(const int64_t* __restrict__ row_off,
+                                                          const int64_t* __restrict__ col_off, double* __restrict__ x,
+                                                          const double* __restrict__ dx, double* __restrict__ z,
+                                                          const double* __restrict__ dz, double* __restrict__ lam,
+                                                          const double* __restrict__ dlam,
+                                                          const double* __restrict__ scal,
+                                                          int32_t* __restrict__ status, int32_t* __restrict__ iters,
+                                                          int iter) {
+    __shared__ int s_bad;
+    const int64_t i = blockIdx.x;
+    if (status[i] != ST_RUN) return;
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    const int64_t c0 = col_off[i], c1 = col_off[i + 1], r0 = row_off[i], r1 = row_off[i + 1];
+    const double ap = scal[i * HN_IPM_NSCAL + S_AP], ad = scal[i * HN_IPM_NSCAL + S_AD];
+    bool bad = false;
+    for (int64_t j = c0 + threadIdx.x; j < c1; j += kT) {
+        const double xn = x[j] + ap * dx[j];
+        const double zn = z[j] + ad * dz[j];
+        x[j] = xn;
+        z[j] = zn;
+        bad |= xn < 0.0 || zn < 0.0 || !fin(xn) || !fin(zn);  // :698-708
+    }
+    for (int64_t k = r0 + threadIdx.x; k < r1; k += kT) lam[k] += ad * dlam[k];
+    if (bad) s_bad = 1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_bad)
+            status[i] = ST_NUMERICAL;
+        else
+            iters[i] = iter + 1;
+    }
+}
+
+// ---- normal equations per instance ----
+__global__ void __launch_bounds__(kT) batch_reg_kernel(const int64_t* __restrict__ row_off,
+                                                       const int64_t* __restrict__ diag_pos, double reg,
+                                                       const int32_t* __restrict__ status, double* __restrict__ nval) {
+    __shared__ double sh[32];
+    __shared__ double s_dyn;
+    const int64_t i = blockIdx.x;
+    if (status[i] != ST_RUN) return;
+    const int64_t r0 = row_off[i], r1 = row_off[i + 1];
+    double md = 0.0;
+    for (int64_t r = r0 + threadIdx.x; r < r1; r += kT) md = fmax(md, nval[diag_pos[r]]);  // NaN ignored
+    md = block_max<kT>(md, sh);
+    if (threadIdx.x == 0) {
+        const double dyn = 1e-12 * md;
+        s_dyn = (reg < dyn) ? dyn : reg;  // std::max(regularization, 1e-12 * max_diag)
+    }
+    __syncthreads();
+    const double dyn = s_dyn;
+    for (int64_t r = r0 + threadIdx.x; r < r1; r += kT) nval[diag_pos[r]] += dyn;
+}
+
+// One warp per packed row: zero the dense lower row, then scatter N's entries.
+__global__ void batch_dense_kernel(int64_t m, const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_inst,
+                                   const int64_t* __restrict__ dn_off, const int32_t* __restrict__ status,
+                                   const int64_t* __restrict__ rpN, const int32_t* __restrict__ ciN,
+                                   const double* __restrict__ nval, double* __restrict__ dense) {
+    const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= m) return;
+    const int inst = row_inst[r];
+    if (status[inst] != ST_RUN) return;
+    const int64_t b0 = row_off[inst], mi = row_off[inst + 1] - b0, lr = r - b0;
+    double* row = dense + dn_off[inst] + lr * mi;
+    for (int64_t c = lane; c <= lr; c += 32) row[c] = 0.0;
+    __syncwarp();
+    for (int64_t p = rpN[r] + lane; p < rpN[r + 1]; p += 32) {
+        const int64_t c = (int64_t)ciN[p] - b0;
+        if (c >= 0 && c <= lr) row[c] = nval[p];
+    }
+}
+
+// Blocked right-looking LDL^T, level-synchronous over the batch: block step s
+// runs two launches for every instance that still has a block s --
+//   batch_ldlt_panel_kernel: one CTA per instance factorises the 32x32
+//     diagonal block (pivot clamp of factorization.cpp:1299-1305) and solves
+//     the panel below it, one row per thread;
+//   batch_ldlt_update_kernel: all instances' trailing 32x32 tiles
+//     A_rc -= sum_q (L_rq D_q) L_cq, spread over every CTA of the GPU.
+__global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, const int64_t* __restrict__ row_off,
+                                                              const int64_t* __restrict__ dn_off,
+                                                              const int32_t* __restrict__ order,
+                                                              const int32_t* __restrict__ status,
+                                                              double* __restrict__ dense, double* __restrict__ dD,
+                                                              double tol) {
+    __shared__ double sA[kNb][kNb + 1];
+    __shared__ double sD[kNb];
+    const int tid = threadIdx.x;
+    const int inst = order[blockIdx.x];
+    if (status[inst] != ST_RUN) return;
+    const int64_t r0 = row_off[inst];
+    const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int k0 = s * kNb;
+    if (k0 >= m) return;
+    const int nb = min(kNb, m - k0), k1 = k0 + nb;
+    double* A = dense + dn_off[inst];
+    for (int idx = tid; idx < kNb * kNb; idx += kT) {
+        const int r = idx / kNb, c = idx % kNb;
+        sA[r][c] = (r < nb && c <= r) ? A[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
+    }
+    __syncthreads();
+    for (int j = 0; j < nb; ++j) {
+        if (tid == 0) {
+            double d = sA[j][j];
+            if (d <= tol) d = tol;  // SparseCholesky pivot clamp
+            sD[j] = d;
+        }
+        __syncthreads();
+        for (int r = j + 1 + tid; r < nb; r += kT) sA[r][j] = sA[r][j] / sD[j];
+        __syncthreads();
+        const int w = nb - j - 1;
+        for (int idx = tid; idx < w * w; idx += kT) {
+            const int rr = j + 1 + idx / w, cc = j + 1 + idx % w;
+            if (cc <= rr) sA[rr][cc] -= (sA[rr][j] * sD[j]) * sA[cc][j];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < nb * nb; idx += kT) {
+        const int r = idx / nb, c = idx % nb;
+        if (c < r) A[(int64_t)(k0 + r) * m + k0 + c] = sA[r][c];
+    }
+    if (tid < nb) dD[r0 + k0 + tid] = sD[tid];
+    // panel below: L[r, k0:k1] = A[r, k0:k1] (L_blk D)^-T
+    for (int r = k1 + tid; r < m; r += kT) {
+        double lv[kNb];
+        double* Ar = A + (int64_t)r * m + k0;
+#pragma unroll
+        for (int c = 0; c < kNb; ++c) lv[c] = (c < nb) ? Ar[c] : 0.0;
+#pragma unroll
+        for (int c = 0; c < kNb; ++c) {
+            if (c < nb) {
+                double v = lv[c];
+#pragma unroll
+                for (int q = 0; q < c; ++q) v -= (lv[q] * sD[q]) * sA[c][q];
+                lv[c] = v / sD[c];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < kNb; ++c)
+            if (c < nb) Ar[c] = lv[c];
+    }
+}
+
+__global__ void __launch_bounds__(kT) batch_ldlt_update_kernel(int s, int cnt, int64_t npairs,
+                                                               const int64_t* __restrict__ pairs,
+                                                               const int64_t* __restrict__ row_off,
+                                                               const int64_t* __restrict__ dn_off,
+                                                               const int32_t* __restrict__ order,
+                                                               const int32_t* __restrict__ status,
+                                                               double* __restrict__ dense,
+                                                               const double* __restrict__ dD) {
+    __shared__ double sW[kNb][kNb + 1];
+    __shared__ double sL[kNb][kNb + 1];
+    const int tid = threadIdx.x;
+    const int k0 = s * kNb;
+    for (int64_t pidx = blockIdx.x; pidx < npairs; pidx += gridDim.x) {
+        // instance of this pair: first b with pairs[b] > pidx (pairs is inclusive)
+        int lo = 0, hi = cnt - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (pairs[mid] <= pidx)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        const int inst = order[lo];
+        if (status[inst] != ST_RUN) continue;  // uniform across the CTA
+        const int64_t local = pidx - (lo > 0 ? pairs[lo - 1] : 0);
+        const int64_t r0 = row_off[inst];
+        const int m = static_cast<int>(row_off[inst + 1] - r0);
+        const int nb = min(kNb, m - k0), k1 = k0 + nb;
+        int ti = static_cast<int>((sqrt(8.0 * (double)local + 1.0) - 1.0) * 0.5);
+        while ((int64_t)(ti + 1) * (ti + 2) / 2 <= local) ++ti;
+        while ((int64_t)ti * (ti + 1) / 2 > local) --ti;
+        const int tj = static_cast<int>(local - (int64_t)ti * (ti + 1) / 2);
+        const int rb = k1 + ti * kNb, cb = k1 + tj * kNb;
+        double* A = dense + dn_off[inst];
+        const double* Dv = dD + r0 + k0;
+        __syncthreads();
+        for (int idx = tid; idx < kNb * kNb; idx += kT) {
+            const int rr = idx / kNb, q = idx % kNb;
+            const bool okr = rb + rr < m && q < nb, okc = cb + rr < m && q < nb;
+            sW[rr][q] = okr ? A[(int64_t)(rb + rr) * m + k0 + q] * Dv[q] : 0.0;
+            sL[rr][q] = okc ? A[(int64_t)(cb + rr) * m + k0 + q] : 0.0;
+        }
+        __syncthreads();
+        const int rr = tid >> 3, cc0 = (tid & 7) * 4;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+        for (int q = 0; q < kNb; ++q) {
+            const double w = sW[rr][q];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc[u] += w * sL[cc0 + u][q];
+        }
+        const int gr = rb + rr;
+        if (gr < m) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int gc = cb + cc0 + u;
+                if (gc <= gr) A[(int64_t)gr * m + gc] -= acc[u];
+            }
+        }
+    }
+}
+
+// Solve N_i x = b in place for every instance flagged in `mask` (status
+// running and, when refine != nullptr, refine[i] != 0): L y = b, y /= D,
+// L^T x = y, blocked by 32 with warp-sequential diagonal blocks.
+__global__ void __launch_bounds__(kT) batch_solve_kernel(int64_t K, const int64_t* __restrict__ row_off,
+                                                         const int64_t* __restrict__ dn_off,
+                                                         const int32_t* __restrict__ order,
+                                                         const int32_t* __restrict__ status,
+                                                         const int32_t* __restrict__ refine,
+                                                         const double* __restrict__ dense,
+                                                         const double* __restrict__ dD, double* __restrict__ xv,
+                                                         unsigned* ticket) {
+    __shared__ double sx[kNb];
+    __shared__ double sacc[kT / 32][kNb];
+    __shared__ double sB[kNb][kNb + 1];
+    __shared__ unsigned s_item;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(ticket, 1u);
+        __syncthreads();
+        const unsigned item = s_item;
+        if (item >= K) break;
+        const int inst = order[item];
+        if (status[inst] != ST_RUN || (refine && !refine[inst])) continue;
+        const int64_t r0 = row_off[inst];
+        const int m = static_cast<int>(row_off[inst + 1] - r0);
+        const double* L = dense + dn_off[inst];
+        const double* Dv = dD + r0;
+        double* x = xv + r0;
+        // forward: L y = b (unit lower)
+        for (int k0 = 0; k0 < m; k0 += kNb) {
+            const int nb = min(kNb, m - k0), k1 = k0 + nb;
+            for (int idx = tid; idx < nb * nb; idx += kT) {
+                const int r = idx / nb, c = idx % nb;
+                sB[r][c] = L[(int64_t)(k0 + r) * m + k0 + c];
+            }
+            __syncthreads();
+            if (warp == 0) {
+                double v = lane < nb ? x[k0 + lane] : 0.0;
+                for (int j = 0; j < nb; ++j) {
+                    const double yj = __shfl_sync(0xffffffffu, v, j);
+                    if (lane > j && lane < nb) v -= sB[lane][j] * yj;
+                }
+                if (lane < nb) {
+                    x[k0 + lane] = v;
+                    sx[lane] = v;
+                }
+            }
+            __syncthreads();
+            for (int r = k1 + tid; r < m; r += kT) {
+                const double* Lr = L + (int64_t)r * m + k0;
+                double s = 0.0;
+                for (int q = 0; q < nb; ++q) s += Lr[q] * sx[q];
+                x[r] -= s;
+            }
+            __syncthreads();
+        }
+        for (int r = tid; r < m; r += kT) x[r] /= Dv[r];
+        __syncthreads();
+        // backward: L^T x = y
+        for (int k1 = m; k1 > 0; k1 -= kNb) {
+            const int k0 = max(0, k1 - kNb), nb = k1 - k0;
+            double acc = 0.0;
+            if (lane < nb)
+                for (int c = k1 + warp; c < m; c += kT / 32) acc += L[(int64_t)c * m + k0 + lane] * x[c];
+            sacc[warp][lane] = acc;
+            for (int idx = tid; idx < nb * nb; idx += kT) {
+                const int r = idx / nb, c = idx % nb;
+                sB[r][c] = L[(int64_t)(k0 + r) * m + k0 + c];
+            }
+            __syncthreads();
+            if (warp == 0) {
+                double v = 0.0;
+                if (lane < nb) {
+                    double t = 0.0;
+                    for (int w = 0; w < kT / 32; ++w) t += sacc[w][lane];
+                    v = x[k0 + lane] - t;
+                }
+                for (int j = nb - 1; j >= 0; --j) {
+                    const double xj = __shfl_sync(0xffffffffu, v, j);
+                    if (lane < j) v -= sB[j][lane] * xj;
+                }
+                if (lane < nb) x[k0 + lane] = v;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Refinement bookkeeping per instance (refinement.cpp:15-30): with r = rhs - N x,
+// rel = max|r| / max|rhs|; an instance keeps sweeping while rel > 1e-10 and
+// sweeps remain; a sweeping instance's r is then solved and added to x.
+__global__ void __launch_bounds__(kT) batch_refine_check_kernel(const int64_t* __restrict__ row_off,
+                                                                const int32_t* __restrict__ status,
+                                                                const double* __restrict__ rhs,
+                                                                const double* __restrict__ ax, double* __restrict__ r,
+                                                                int32_t* __restrict__ refine, int32_t* nref) {
+    __shared__ double sh[32];
+    const int64_t i = blockIdx.x;
+    if (status[i] != ST_RUN || !refine[i]) return;
+    const int64_t r0 = row_off[i], r1 = row_off[i + 1];
+    double nb = 0.0, nr = 0.0;
+    for (int64_t k = r0 + threadIdx.x; k < r1; k += kT) {
+        const double b = rhs[k], d = b - ax[k];
+        nb = fmax(nb, fabs(b));
+        nr = fmax(nr, fabs(d));
+        r[k] = d;
+    }
+    nb = block_max<kT>(nb, sh);
+    nr = block_max<kT>(nr, sh);
+    if (threadIdx.x == 0) {
+        const bool go = nb != 0.0 && nb == nb && nr / nb > 1e-10;
+        refine[i] = go ? 1 : 0;
+        if (go) atomicAdd(nref, 1);
+    }
+}
+
+__global__ void __launch_bounds__(kT) batch_refine_start_kernel(const int64_t* __restrict__ row_off,
+                                                                const int32_t* __restrict__ status,
+                                                                const double* __restrict__ rhs,
+                                                                int32_t* __restrict__ refine) {
+    __shared__ double sh[32];
+    const int64_t i = blockIdx.x;
+    const int64_t r0 = row_off[i], r1 = row_off[i + 1];
+    double nb = 0.0;
+    for (int64_t k = r0 + threadIdx.x; k < r1; k += kT) nb = fmax(nb, fabs(rhs[k]));
+    nb = block_max<kT>(nb, sh);
+    // a zero or NaN right-hand side is not refined (refinement.cpp:17-18); fmax drops NaN,
+    // so look for one explicitly
+    __shared__ int s_nan;
+    if (threadIdx.x == 0) s_nan = 0;
+    __syncthreads();
+    for (int64_t k = r0 + threadIdx.x; k < r1; k += kT)
+        if (rhs[k] != rhs[k]) s_nan = 1;
+    __syncthreads();
+    if (threadIdx.x == 0) refine[i] = (status[i] == ST_RUN && nb != 0.0 && !s_nan) ? 1 : 0;
+}
+
+__global__ void batch_axpy_masked_kernel(int64_t m, const int32_t* __restrict__ row_inst,
+                                         const int32_t* __restrict__ status, const int32_t* __restrict__ refine,
+                                         const double* __restrict__ r, double* __restrict__ x) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const int inst = row_inst[k];
+    if (status[inst] == ST_RUN && refine[inst]) x[k] += r[k];
+}
+
+__global__ void row_inst_kernel(int64_t K, const int64_t* __restrict__ row_off, int32_t* __restrict__ row_inst) {
+    const int64_t i = blockIdx.x;
+    for (int64_t r = row_off[i] + threadIdx.x; r < row_off[i + 1]; r += blockDim.x) row_inst[r] = (int32_t)i;
+}
+
+__global__ void narrow_rp_kernel(int64_t n, const int64_t* __restrict__ in, int32_t* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = static_cast<int32_t>(in[i]);
+}
+
+void free_batch(hn_batch* B) {
+    if (!B) return;
+    for (void* p : {(void*)B->row_off, (void*)B->col_off, (void*)B->row_inst, (void*)B->dn_off, (void*)B->order,
+                    (void*)B->dense, (void*)B->dD, (void*)B->ticket, (void*)B->refine, (void*)B->nref, (void*)B->nrp,
+                    (void*)B->tile_row, (void*)B->tile_nz, (void*)B->carry_row, (void*)B->head_row,
+                    (void*)B->carry_val, (void*)B->head_val, (void*)B->r, (void*)B->ax, (void*)B->step_pairs})
+        dfree(p);
+    delete B;
+}
+
+SpmvMat n_mat(const hn_batch* B, const double* nval) {
+    return SpmvMat{(int)B->m, (int)B->P->nnz, B->nrp, B->P->ci, nval, B->tile_row, B->tile_nz, B->carry_row,
+                   B->carry_val, B->head_row, B->head_val, B->ntiles};
+}
+
+void reset_ticket(hn_batch* B, cudaStream_t s) {
+    check_cuda(cudaMemsetAsync(B->ticket, 0, sizeof(unsigned), s), "memset ticket");
+}
+
+void solve_all(hn_batch* B, const int32_t* status, const int32_t* refine, double* x, cudaStream_t s) {
+    reset_ticket(B, s);
+    const int grid = (int)std::min<int64_t>(B->K, (int64_t)ctx().sm_count * 4);
+    batch_solve_kernel<<<grid, kT, 0, s>>>(B->K, B->row_off, B->dn_off, B->order, status, refine, B->dense, B->dD, x,
+                                           B->ticket);
+    launched("batch_solve_kernel");
+}
+
+}  // namespace
+}  // namespace hn
+
+using namespace hn;
+
+extern "C" {
+
+int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_off_host, const hn_pattern* P,
+                    hn_batch** out) {
+    return guard("hn_batch_create", [&] {
+        require_init();
+        if (K <= 0 || !row_off_host || !col_off_host || !P || !out) fail(HN_ERR_INVALID_ARG, "bad arguments");
+        *out = nullptr;
+        const int64_t m = row_off_host[K], n = col_off_host[K];
+        if (m != P->m) fail(HN_ERR_INVALID_ARG, "row offsets do not match the pattern");
+        std::vector<int64_t> dn(K + 1, 0);
+        std::vector<int32_t> order(K);
+        for (int64_t i = 0; i < K; ++i) {
+            const int64_t mi = row_off_host[i + 1] - row_off_host[i];
+            const int64_t ni = col_off_host[i + 1] - col_off_host[i];
+            if (mi < 1 || ni < 1) fail(HN_ERR_INVALID_ARG, "every instance needs a row and a column");
+            dn[i + 1] = dn[i] + mi * mi;
+            order[i] = static_cast<int32_t>(i);
+        }
+        std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+            return row_off_host[a + 1] - row_off_host[a] > row_off_host[b + 1] - row_off_host[b];
+        });
+        hn_batch* B = new hn_batch();
+        cudaStream_t s = nullptr;
+        try {
+            B->K = K;
+            B->m = m;
+            B->n = n;
+            B->P = P;
+            B->row_off = dmalloc<int64_t>(K + 1);
+            B->col_off = dmalloc<int64_t>(K + 1);
+            B->dn_off = dmalloc<int64_t>(K + 1);
+            B->order = dmalloc<int32_t>(K);
+            B->row_inst = dmalloc<int32_t>(m);
+            B->dense = dmalloc<double>(dn[K]);
+            B->dD = dmalloc<double>(m);
+            B->ticket = dmalloc<unsigned>(1);
+            B->refine = dmalloc<int32_t>(K);
+            B->nref = dmalloc<int32_t>(1);
+            B->r = dmalloc<double>(m);
+            B->ax = dmalloc<double>(m);
+            B->nrp = dmalloc<int32_t>(m + 1);
+            check_cuda(cudaMemcpy(B->row_off, row_off_host, sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice), "H2D");
+            check_cuda(cudaMemcpy(B->col_off, col_off_host, sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice), "H2D");
+            check_cuda(cudaMemcpy(B->dn_off, dn.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice), "H2D");
+            check_cuda(cudaMemcpy(B->order, order.data(), sizeof(int32_t) * K, cudaMemcpyHostToDevice), "H2D");
+            row_inst_kernel<<<(unsigned)K, 256, 0, s>>>(K, B->row_off, B->row_inst);
+            launched("row_inst_kernel");
+            narrow_rp_kernel<<<(unsigned)((m + 1 + 255) / 256), 256, 0, s>>>(m + 1, P->rp, B->nrp);
+            launched("narrow_rp_kernel");
+            make_tile_table(B->nrp, m, P->nnz, &B->ntiles, &B->tile_row, &B->tile_nz, &B->carry_row, &B->carry_val,
+                            &B->head_row, &B->head_val, s);
+            // level schedule (instances in decreasing size: the ones with a block
+            // at step s form a prefix of `order`)
+            const int64_t mmax = row_off_host[order[0] + 1] - row_off_host[order[0]];
+            B->nsteps = (mmax + kNb - 1) / kNb;
+            B->pair_off_h.assign(1, 0);
+            std::vector<int64_t> flat;
+            for (int64_t st = 0; st < B->nsteps; ++st) {
+                int32_t cnt = 0;
+                int64_t acc = 0;
+                for (int64_t b = 0; b < K; ++b) {
+                    const int64_t mi = row_off_host[order[b] + 1] - row_off_host[order[b]];
+                    if (mi <= st * kNb) break;
+                    const int64_t rest = mi - std::min<int64_t>(mi, (st + 1) * kNb);
+                    const int64_t T = (rest + kNb - 1) / kNb;
+                    acc += T * (T + 1) / 2;
+                    flat.push_back(acc);
+                    ++cnt;
+                }
+                B->step_cnt.push_back(cnt);
+                B->step_pairs_h.push_back(acc);
+                B->pair_off_h.push_back((int64_t)flat.size());
+            }
+            B->step_pairs = dmalloc<int64_t>(flat.size());
+            check_cuda(cudaMemcpy(B->step_pairs, flat.data(), sizeof(int64_t) * flat.size(), cudaMemcpyHostToDevice),
+                       "H2D schedule");
+            check_cuda(cudaStreamSynchronize(s), "batch create sync");
+        } catch (...) {
+            free_batch(B);
+            throw;
+        }
+        *out = B;
+    });
+}
+
+int hn_batch_destroy(hn_batch* B) {
+    return guard("hn_batch_destroy", [&] {
+        if (!B) return;
+        require_init();
+        cudaDeviceSynchronize();
+        free_batch(B);
+    });
+}
+
+int hn_batch_residuals(hn_batch* B, const hn_csr* M, const double* x, const double* lam, const double* z,
+                       const double* b, const double* c, double* mx, double* rp, double* rd, double* D, double* Drd,
+                       double* scal, int32_t* status, int32_t* iters, int iter, double tol, double ctol,
+                       void* stream) {
+    return guard("hn_batch_residuals", [&] {
+        require_init();
+        if (!B || !M || !M->has_t) fail(HN_ERR_INVALID_ARG, "bad arguments");
+        cudaStream_t s = as_stream(stream);
+        spmv_launch(spmv_mat(M, 0), x, EpiResidual{b, mx, rp}, s);
+        spmv_launch(spmv_mat(M, 1), lam, EpiDualResidual{z, c, rd}, s);
+        batch_prep_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, B->col_off, x, z, rd, rp, D, Drd, scal, status,
+                                                        iters, iter, tol, ctol);
+        launched("batch_prep_kernel");
+    });
+}
+
+int hn_batch_factor(hn_batch* B, const double* D, double reg, double singular_tol, double* nval,
+                    const int32_t* status, void* stream) {
+    return guard("hn_batch_factor", [&] {
+        require_init();
+        if (!B || !D || !nval || !status) fail(HN_ERR_INVALID_ARG, "bad arguments");
+        cudaStream_t s = as_stream(stream);
+        ada_numeric_unregularised(B->P, D, nval, s);
+        batch_reg_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, B->P->diag_pos, reg, status, nval);
+        launched("batch_reg_kernel");
+        batch_dense_kernel<<<(unsigned)((B->m * 32 + 255) / 256), 256, 0, s>>>(
+            B->m, B->row_off, B->row_inst, B->dn_off, status, B->P->rp, B->P->ci, nval, B->dense);
+        launched("batch_dense_kernel");
+        for (int64_t st = 0; st < B->nsteps; ++st) {
+            const int cnt = B->step_cnt[st];
+            batch_ldlt_panel_kernel<<<cnt, kT, 0, s>>>((int)st, B->row_off, B->dn_off, B->order, status, B->dense,
+                                                       B->dD, singular_tol);
+            launched("batch_ldlt_panel_kernel");
+            const int64_t np = B->step_pairs_h[st];
+            if (np > 0) {
+                const int grid = (int)std::min<int64_t>(np, (int64_t)ctx().sm_count * 8);
+                batch_ldlt_update_kernel<<<grid, kT, 0, s>>>((int)st, cnt, np, B->step_pairs + B->pair_off_h[st],
+                                                             B->row_off, B->dn_off, B->order, status, B->dense,
+                                                             B->dD);
+                launched("batch_ldlt_update_kernel");
+            }
+        }
+    });
+}
+
+int hn_batch_solve(hn_batch* B, const double* nval, const double* rhs, double* x, const int32_t* status,
+                   void* stream) {
+    return guard("hn_batch_solve", [&] {
+        require_init();
+        if (!B || !nval || !rhs || !x || !status) fail(HN_ERR_INVALID_ARG, "bad arguments");
+        cudaStream_t s = as_stream(stream);
+        check_cuda(cudaMemcpyAsync(x, rhs, sizeof(double) * B->m, cudaMemcpyDeviceToDevice, s), "copy rhs");
+        solve_all(B, status, nullptr, x, s);
+        batch_refine_start_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, status, rhs, B->refine);
+        launched("batch_refine_start_kernel");
+        const SpmvMat N = n_mat(B, nval);
+        for (int sweep = 0; sweep < 5; ++sweep) {
+            spmv_launch(N, x, EpiAxpby{1.0, 0.0, B->ax}, s);
+            check_cuda(cudaMemsetAsync(B->nref, 0, sizeof(int32_t), s), "memset");
+            batch_refine_check_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, status, rhs, B->ax, B->r, B->refine,
+                                                                    B->nref);
+            launched("batch_refine_check_kernel");
+            int32_t left = 0;
+            check_cuda(cudaMemcpyAsync(&left, B->nref, sizeof(left), cudaMemcpyDeviceToHost, s), "D2H");
+            check_cuda(cudaStreamSynchronize(s), "refine sync");
+            if (left == 0) break;
+            solve_all(B, status, B->refine, B->r, s);
+            batch_axpy_masked_kernel<<<(unsigned)((B->m + 255) / 256), 256, 0, s>>>(B->m, B->row_inst, status,
+                                                                                    B->refine, B->r, x);
+            launched("batch_axpy_masked_kernel");
+        }
+    });
+}
+
+int hn_batch_steps(hn_batch* B, const double* x, const double* dx, const double* z, const double* dz,
+                   const double* dlam, double* scal, int32_t* status, void* stream) {
+    return guard("hn_batch_steps", [&] {
+        require_init();
+        if (!B) fail(HN_ERR_INVALID_ARG, "null batch");
+        cudaStream_t s = as_stream(stream);
+        batch_steps_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, B->col_off, x, dx, z, dz, dlam, scal, status);
+        launched("batch_steps_kernel");
+    });
+}
+
+int hn_batch_corrector(hn_batch* B, const hn_csr* M, const double* x, const double* dx, const double* z,
+                       const double* dz, const double* rhs_pred, double* zs, double* rhs, double* scal,
+                       const int32_t* status, void* stream) {
+    return guard("hn_batch_corrector", [&] {
+        require_init();
+        if (!B || !M) fail(HN_ERR_INVALID_ARG, "bad arguments");
+        cudaStream_t s = as_stream(stream);
+        batch_corr_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->col_off, x, dx, z, dz, scal, status, zs);
+        launched("batch_corr_kernel");
+        spmv_launch(spmv_mat(M, 0), zs, EpiCorrRhs{rhs_pred, rhs}, s);
+    });
+}
+
+int hn_batch_update(hn_batch* B, double* x, const double* dx, double* z, const double* dz, double* lam,
+                    const double* dlam, const double* scal, int32_t* status, int32_t* iters, int iter,
+                    void* stream) {
+    return guard("hn_batch_update", [&] {
+        require_init();
+        if (!B) fail(HN_ERR_INVALID_ARG, "null batch");
+        cudaStream_t s = as_stream(stream);
+        batch_update_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, B->col_off, x, dx, z, dz, lam, dlam, scal,
+                                                          status, iters, iter);
+        launched("batch_update_kernel");
+    });
+}
+
+}  // extern "C"

@@ -371,6 +371,12 @@ void convert_csr(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci,
 }
 
 }  // namespace
+
+void make_tile_table(const int32_t* rp, int64_t m, int64_t nnz, int64_t* ntiles, int32_t** trow, int32_t** tnz,
+                     int32_t** crow, double** cval, int32_t** hrow, double** hval, cudaStream_t s) {
+    build_tiles(rp, m, nnz, *ntiles, *trow, *tnz, *crow, *cval, *hrow, *hval, s);
+}
+
 }  // namespace hn
 
 using namespace hn;

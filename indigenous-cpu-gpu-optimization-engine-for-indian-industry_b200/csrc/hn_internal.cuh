@@ -104,6 +104,16 @@ void reduce_dot(int64_t n, const double* a, const double* b, double* out, cudaSt
 void reduce_nrm2(int64_t n, const double* a, double* out, cudaStream_t s);
 void reduce_maxabs(int64_t n, const double* a, double* out, cudaStream_t s);
 
+// Merge-path tile table + carry buffers for a CSR with int32 row pointer rp
+// (m rows, nnz nonzeros); allocates the six arrays (hn_csr.cu).
+void make_tile_table(const int32_t* rp, int64_t m, int64_t nnz, int64_t* ntiles, int32_t** trow, int32_t** tnz,
+                     int32_t** crow, double** cval, int32_t** hrow, double** hval, cudaStream_t s);
+
+// A D A^T numeric without the regularisation step (hn_ada.cu): N's values
+// with every diagonal still un-regularised. Used by the batched IPM, which
+// regularises each instance's block with its own dyn_reg.
+void ada_numeric_unregularised(const hn_pattern* P, const double* d, double* nval, cudaStream_t s);
+
 // ---------------------------------------------------------------- device helpers
 __device__ __forceinline__ double ld_stream(const double* p) {
     double v;
@@ -295,15 +305,15 @@ struct hn_pattern {
     int32_t* ci = nullptr;       // nnz
     int64_t* diag_pos = nullptr; // m
     unsigned long long* maxdiag = nullptr;  // scratch: max diagonal as ordered bits
-    // scatter map of the numeric phase: contribution q of row i (entries e of
-    // row i in order, then the rows k of column j_e in order) lands in slot
-    // map[q] of N, or -- with kMulti set -- in the ordered-sum scratch
-    int64_t nq = 0;
-    int64_t* qrow = nullptr;     // m+1: first contribution of each row
-    uint32_t* map = nullptr;     // nq
-    int64_t nms = 0;             // slots with several contributions (+ every diagonal)
-    int64_t* mpos = nullptr;     // nms: N position (bit 62 set for a diagonal)
-    int32_t* mbeg = nullptr;     // nms+1: scratch range of each such slot
-    int64_t nmq = 0;             // contributions into those slots
-    double* scratch = nullptr;   // nmq
+    // gather map of the numeric phase: for slot t of N, gmap[t] = (p, e) --
+    // its single term (A_ij A_kj) d_j comes from A^T entry p and A entry e --
+    // or (kMulti | ms, 0) for a slot with several terms, whose (p, e) pairs
+    // are mlist[mbeg[ms] .. mbeg[ms+1]) in column order
+    int64_t nq = 0;                  // terms in total (sum over columns of count^2)
+    uint2* gmap = nullptr;           // nnz
+    int64_t nms = 0;                 // slots with several terms (+ every diagonal)
+    int64_t* mpos = nullptr;         // nms: N position (bit 62 set for a diagonal)
+    int32_t* mbeg = nullptr;         // nms+1
+    int64_t nmq = 0;                 // terms into those slots
+    uint2* mlist = nullptr;          // nmq
 };

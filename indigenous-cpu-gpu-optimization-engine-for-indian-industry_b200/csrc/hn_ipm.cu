@@ -26,52 +26,6 @@ namespace {
 
 constexpr int kT = 256;
 
-struct EpiResidual {
-    const double* b;
-    double* mx;
-    double* rp;
-    __device__ __forceinline__ void operator()(int r, double s) const {
-        mx[r] = s;
-        rp[r] = s - b[r];
-    }
-};
-
-struct EpiDualResidual {
-    const double* z;
-    const double* c;
-    double* rd;
-    __device__ __forceinline__ void operator()(int j, double s) const { rd[j] = (s + z[j]) - c[j]; }
-};
-
-struct EpiRhs {
-    const double* rp;
-    const double* mx;
-    double* rhs;
-    __device__ __forceinline__ void operator()(int i, double s) const { rhs[i] = ((-rp[i]) - s) + mx[i]; }
-};
-
-struct EpiCorrRhs {
-    const double* pred;
-    double* rhs;
-    __device__ __forceinline__ void operator()(int i, double s) const { rhs[i] = pred[i] - s; }
-};
-
-struct EpiDirection {
-    const double* D;
-    const double* rd;
-    const double* x;
-    const double* corr;
-    double* dx;
-    double* dz;
-    __device__ __forceinline__ void operator()(int j, double s) const {
-        const double u = s + rd[j];
-        double v = D[j] * u - x[j];
-        if (corr) v = v + corr[j];
-        dx[j] = v;
-        dz[j] = -u;
-    }
-};
-
 __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 
 __device__ __forceinline__ unsigned long long* flags_of(double* scal) {

@@ -6,10 +6,12 @@
 // Zipf-skewed A^T rows of the large configuration and the Poisson rows of A
 // alike). Inside a tile each thread walks kSpmvIpt consecutive items.
 //
-// Per tile: coalesced loads of col_idx/values (L1 no-allocate: they stream
-// once) and gathers of x (cached) fill a shared-memory product buffer; the
-// threads walk their items, finishing rows that end in their range; partial
-// rows are combined through a shared carry array in thread order. A row that
+// Per tile: the row ends go to shared memory; each thread finds where the
+// path enters and leaves its items (two binary searches), loads the products
+// of its contiguous nonzeros straight into registers (col_idx, values, then
+// the x gathers -- through L1, so a warp's neighbouring ranges share sectors),
+// and walks its items, finishing rows that end in its range; partial rows are
+// combined through a shared carry array in thread order. A row that
 // began in an earlier tile leaves its in-tile part in head_val and is
 // finished by a second, tiny kernel that adds the earlier tiles' carries in
 // tile order. Every row's sum therefore has a fixed association order, so
@@ -24,7 +26,7 @@
 namespace hn {
 
 constexpr int kSpmvThreads = 256;
-constexpr int kSpmvIpt = 7;  // odd: lanes reading their items from the product buffer fall on different banks
+constexpr int kSpmvIpt = 7;
 constexpr int kSpmvTile = kSpmvThreads * kSpmvIpt;
 
 struct SpmvMat {
@@ -53,10 +55,24 @@ inline SpmvMat spmv_mat(const hn_csr* A, int trans) {
     return M;
 }
 
+// Merge-path coordinate of tile-local diagonal `diag`: rows consumed (return)
+// and nonzeros consumed (diag - return), from the tile's row ends in shared memory.
+__device__ __forceinline__ int tile_search(const int32_t* s_rowend, int k0, int diag, int nrows_t, int nnz_t) {
+    int lo = diag - nnz_t > 0 ? diag - nnz_t : 0;
+    int hi = diag < nrows_t ? diag : nrows_t;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (s_rowend[mid] <= k0 + diag - mid - 1)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
 template <class Epi>
 __global__ void __launch_bounds__(kSpmvThreads) spmv_tile_kernel(SpmvMat a, const double* __restrict__ x,
                                                                  Epi epi) {
-    __shared__ double s_prod[kSpmvTile];
     __shared__ int32_t s_rowend[kSpmvTile + 1];
     __shared__ int32_t s_crow[kSpmvThreads];
     __shared__ double s_cval[kSpmvThreads];
@@ -77,59 +93,54 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_tile_kernel(SpmvMat a, cons
         const int r = r0 + i;
         s_rowend[i] = (r < a.m) ? __ldg(a.rp + r + 1) : INT_MAX;
     }
-    {
-        int cidx[kSpmvIpt];
-        double v[kSpmvIpt];
-#pragma unroll
-        for (int u = 0; u < kSpmvIpt; ++u) {
-            const int i = tid + u * kSpmvThreads;
-            if (i < nnz_t) {
-                cidx[u] = ld_stream(a.ci + k0 + i);
-                v[u] = ld_stream(a.val + k0 + i);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kSpmvIpt; ++u) {
-            const int i = tid + u * kSpmvThreads;
-            if (i < nnz_t) s_prod[i] = v[u] * __ldg(x + cidx[u]);
-        }
-    }
     __syncthreads();
 
+    // this thread's kSpmvIpt merge items: its nonzeros are the contiguous
+    // range [nz, nz_e) of the tile, found from the path at both ends
     const int total_t = nrows_t + nnz_t;
-    int diag = tid * kSpmvIpt;
-    if (diag > total_t) diag = total_t;
-    int diag_end = diag + kSpmvIpt;
-    if (diag_end > total_t) diag_end = total_t;
-    int lo = diag - nnz_t > 0 ? diag - nnz_t : 0;
-    int hi = diag < nrows_t ? diag : nrows_t;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (s_rowend[mid] <= k0 + diag - mid - 1)
-            lo = mid + 1;
-        else
-            hi = mid;
+    const int diag = min(tid * kSpmvIpt, total_t);
+    const int diag_end = min(diag + kSpmvIpt, total_t);
+    int row = tile_search(s_rowend, k0, diag, nrows_t, nnz_t);
+    int nz = diag - row;
+    const int row_e = tile_search(s_rowend, k0, diag_end, nrows_t, nnz_t);
+    const int cnt = (diag_end - row_e) - nz;
+
+    // products of those nonzeros, straight into registers (no shared buffer):
+    // column indices first, then values, then the gathers of x
+    double v[kSpmvIpt];
+    {
+        int c[kSpmvIpt];
+#pragma unroll
+        for (int u = 0; u < kSpmvIpt; ++u) c[u] = (u < cnt) ? __ldg(a.ci + k0 + nz + u) : 0;
+        double w[kSpmvIpt];
+#pragma unroll
+        for (int u = 0; u < kSpmvIpt; ++u) w[u] = (u < cnt) ? __ldg(a.val + k0 + nz + u) : 0.0;
+#pragma unroll
+        for (int u = 0; u < kSpmvIpt; ++u) v[u] = (u < cnt) ? w[u] * __ldg(x + c[u]) : 0.0;
     }
-    int row = lo;
-    int nz = diag - lo;
+
     double sum = 0.0;
     int first_row = -1;
     double first_val = 0.0;
-    for (int it = diag; it < diag_end; ++it) {
-        const bool take_nz = (nz < nnz_t) && (k0 + nz < s_rowend[row]);
-        if (take_nz) {
-            sum += s_prod[nz];
-            ++nz;
-        } else {
-            if (row >= nrows_t) break;  // unreachable on a consistent tile table
-            if (first_row < 0) {
-                first_row = row;
-                first_val = sum;
-            } else {
-                epi(r0 + row, sum);
+#pragma unroll
+    for (int it = 0; it < kSpmvIpt; ++it) {
+        if (diag + it < diag_end) {
+            const bool take_nz = (nz < nnz_t) && (k0 + nz < s_rowend[row]);
+            if (take_nz) {
+                sum += v[0];
+#pragma unroll
+                for (int q = 0; q < kSpmvIpt - 1; ++q) v[q] = v[q + 1];
+                ++nz;
+            } else if (row < nrows_t) {
+                if (first_row < 0) {
+                    first_row = row;
+                    first_val = sum;
+                } else {
+                    epi(r0 + row, sum);
+                }
+                sum = 0.0;
+                ++row;
             }
-            sum = 0.0;
-            ++row;
         }
     }
     s_crow[tid] = row;
@@ -196,6 +207,53 @@ struct EpiAxpby {
     double* y;
     __device__ __forceinline__ void operator()(int r, double s) const {
         y[r] = (beta == 0.0) ? alpha * s : alpha * s + beta * y[r];
+    }
+};
+
+// IPM epilogues (core/lp/interior_point.cpp line numbers in hn_ipm.cu)
+struct EpiResidual {
+    const double* b;
+    double* mx;
+    double* rp;
+    __device__ __forceinline__ void operator()(int r, double s) const {
+        mx[r] = s;
+        rp[r] = s - b[r];
+    }
+};
+
+struct EpiDualResidual {
+    const double* z;
+    const double* c;
+    double* rd;
+    __device__ __forceinline__ void operator()(int j, double s) const { rd[j] = (s + z[j]) - c[j]; }
+};
+
+struct EpiRhs {
+    const double* rp;
+    const double* mx;
+    double* rhs;
+    __device__ __forceinline__ void operator()(int i, double s) const { rhs[i] = ((-rp[i]) - s) + mx[i]; }
+};
+
+struct EpiCorrRhs {
+    const double* pred;
+    double* rhs;
+    __device__ __forceinline__ void operator()(int i, double s) const { rhs[i] = pred[i] - s; }
+};
+
+struct EpiDirection {
+    const double* D;
+    const double* rd;
+    const double* x;
+    const double* corr;
+    double* dx;
+    double* dz;
+    __device__ __forceinline__ void operator()(int j, double s) const {
+        const double u = s + rd[j];
+        double v = D[j] * u - x[j];
+        if (corr) v = v + corr[j];
+        dx[j] = v;
+        dz[j] = -u;
     }
 };
 

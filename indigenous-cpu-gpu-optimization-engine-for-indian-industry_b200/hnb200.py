@@ -87,6 +87,14 @@ SIGNATURES = {
     "hn_ipm_update": [_i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "hn_max_step": [_i64, _vp, _vp, _vp, _vp],
     "hn_spmv_noalloc": [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp],
+    "hn_batch_create": [_i64, _i64p, _i64p, _vp, C.POINTER(_vp)],
+    "hn_batch_destroy": [_vp],
+    "hn_batch_residuals": [_vp, _vp] + [_vp] * 13 + [C.c_int, C.c_double, C.c_double, _vp],
+    "hn_batch_factor": [_vp, _vp, C.c_double, C.c_double, _vp, _vp, _vp],
+    "hn_batch_solve": [_vp, _vp, _vp, _vp, _vp, _vp],
+    "hn_batch_steps": [_vp] + [_vp] * 7 + [_vp],
+    "hn_batch_corrector": [_vp, _vp] + [_vp] * 9 + [_vp],
+    "hn_batch_update": [_vp] + [_vp] * 9 + [C.c_int, _vp],
 }
 _RESTYPE = {"hn_last_error": C.c_char_p}
 
@@ -313,6 +321,9 @@ HOST_SIGNATURES = {
     "hn_lp_solve": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, C.POINTER(C.c_int), _f64p, _f64p,
                               C.c_int, C.c_double, C.POINTER(IpmOptions), C.POINTER(IpmResult), _f64p]),
     "hn_host_last_error": (C.c_char_p, []),
+    "hn_lp_solve_batch": (C.c_int, [_i64, _i64p, _i64p, _i64p, _u64p, _u64p, _f64p, _f64p, _f64p,
+                                    C.POINTER(C.c_int), _f64p, _f64p, C.POINTER(C.c_int), _f64p,
+                                    C.POINTER(IpmOptions), C.POINTER(C.c_int), _f64p, _i64p, _f64p, _vp]),
     "hn_be_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
     "hn_be_destroy": (C.c_int, [_vp]),
     "hn_be_spmv": (C.c_int, [_vp, _i64, _i64, _u64p, _u64p, _f64p, _i64, _f64p, _f64p]),
@@ -378,6 +389,52 @@ def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=
             "iterations": res.iterations, "time_ms": res.solve_time_ms, "device_ms": res.device_ms,
             "factor_ms": res.factor_ms, "solve_ms": res.solve_ms, "nnz_normal": res.nnz_normal, "x": x,
             "error": err}
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("rows", C.c_int64), ("cols", C.c_int64), ("nnz", C.c_int64), ("nnz_normal", C.c_int64),
+                ("iterations", C.c_int64), ("total_ms", C.c_double), ("factor_ms", C.c_double),
+                ("solve_ms", C.c_double)]
+
+
+def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs=None):
+    """Batched GPU IPM over a list of LP dicts (rows EQ, x >= 0 unless given)."""
+    K = len(lps)
+    row_off = np.zeros(K + 1, np.int64)
+    col_off = np.zeros(K + 1, np.int64)
+    nnz_off = np.zeros(K + 1, np.int64)
+    for i, lp in enumerate(lps):
+        row_off[i + 1] = row_off[i] + lp["m"]
+        col_off[i + 1] = col_off[i] + lp["n"]
+        nnz_off[i + 1] = nnz_off[i] + len(lp["ci"])
+    rp = u64(np.concatenate([np.asarray(lp["rp"], np.uint64) for lp in lps]))
+    ci = u64(np.concatenate([np.asarray(lp["ci"], np.uint64) for lp in lps]))
+    val = f64(np.concatenate([lp["val"] for lp in lps]))
+    c = f64(np.concatenate([lp["c"] for lp in lps]))
+    b = f64(np.concatenate([lp["b"] for lp in lps]))
+    sense = np.ascontiguousarray(np.concatenate(senses) if senses else np.full(row_off[-1], 2), dtype=np.int32)
+    lb = f64(np.concatenate(lbs) if lbs else np.zeros(col_off[-1]))
+    ub = f64(np.concatenate(ubs) if ubs else np.full(col_off[-1], np.inf))
+    maxi = np.zeros(K, np.int32)
+    off = np.zeros(K)
+    opt = IpmOptions()
+    host().hn_ipm_default_options(C.byref(opt))
+    opt.max_iterations = max_iter
+    opt.device = device
+    status = np.zeros(K, np.int32)
+    obj = np.zeros(K)
+    iters = np.zeros(K, np.int64)
+    x = np.zeros(col_off[-1])
+    st = BatchStats()
+    P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    host_check(host().hn_lp_solve_batch(K, P(row_off, C.c_int64), P(col_off, C.c_int64), P(nnz_off, C.c_int64),
+                                        P(rp, C.c_uint64), P(ci, C.c_uint64), P(val, C.c_double), P(c, C.c_double),
+                                        P(b, C.c_double), P(sense, C.c_int), P(lb, C.c_double), P(ub, C.c_double),
+                                        P(maxi, C.c_int), P(off, C.c_double), C.byref(opt), P(status, C.c_int),
+                                        P(obj, C.c_double), P(iters, C.c_int64), P(x, C.c_double),
+                                        C.cast(C.pointer(st), C.c_void_p)))
+    return {"status": status, "objective": obj, "iterations": iters, "x": x, "col_off": col_off,
+            "stats": {k: getattr(st, k) for k, _ in BatchStats._fields_}}
 
 
 class Backend:

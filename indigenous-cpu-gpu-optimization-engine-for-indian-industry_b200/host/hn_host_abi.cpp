@@ -103,6 +103,71 @@ int hn_lp_solve(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, co
     });
 }
 
+int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off, const int64_t* nnz_off,
+                      const uint64_t* rp, const uint64_t* ci, const double* val, const double* c, const double* b,
+                      const int* sense, const double* lb, const double* ub, const int* maximize,
+                      const double* obj_offset, const hn_ipm_options* opt, int* status, double* objective,
+                      int64_t* iterations, double* x_out, hn_batch_stats* stats) {
+    return wrap([&] {
+        if (K < 0 || !row_off || !col_off || !nnz_off || !status || !objective || !iterations)
+            throw std::invalid_argument("bad arguments");
+        std::vector<hn::model::LpProblem> probs((std::size_t)K);
+        for (int64_t i = 0; i < K; ++i) {
+            hn::model::LpProblem& p = probs[(std::size_t)i];
+            const int64_t m = row_off[i + 1] - row_off[i], n = col_off[i + 1] - col_off[i];
+            const uint64_t* r = rp + row_off[i] + i;
+            const int64_t e0 = nnz_off[i];
+            p.num_rows = (std::size_t)m;
+            p.num_cols = (std::size_t)n;
+            p.row_ptr.assign(r, r + m + 1);
+            p.col_indices.assign(ci + e0, ci + e0 + (int64_t)r[m]);
+            p.values.assign(val + e0, val + e0 + (int64_t)r[m]);
+            p.objective.assign(c + col_off[i], c + col_off[i + 1]);
+            p.lower.assign(lb + col_off[i], lb + col_off[i + 1]);
+            p.upper.assign(ub + col_off[i], ub + col_off[i + 1]);
+            p.rhs.assign(b + row_off[i], b + row_off[i + 1]);
+            for (int64_t k = row_off[i]; k < row_off[i + 1]; ++k)
+                p.sense.push_back(sense[k] == 0 ? hn::model::ConstraintSense::LE
+                                                : sense[k] == 1 ? hn::model::ConstraintSense::GE
+                                                                : hn::model::ConstraintSense::EQ);
+            p.obj_sense = (maximize && maximize[i]) ? hn::model::ObjectiveSense::MAXIMIZE
+                                                    : hn::model::ObjectiveSense::MINIMIZE;
+            p.obj_offset = obj_offset ? obj_offset[i] : 0.0;
+        }
+        hn::lp::InteriorPointOptions o;
+        if (opt) {
+            o.max_iterations = opt->max_iterations;
+            o.time_limit_seconds = opt->time_limit_seconds;
+            o.convergence_tol = opt->convergence_tol;
+            o.complementarity_tol = opt->complementarity_tol;
+            o.regularization = opt->regularization;
+            o.device = opt->device;
+        }
+        hn::lp::BatchInteriorPointSolver solver(o);
+        auto res = solver.solve(probs);
+        for (int64_t i = 0; i < K; ++i) {
+            const auto& r = res[(std::size_t)i];
+            status[i] = static_cast<int>(r.status);
+            objective[i] = r.objective_value;
+            iterations[i] = (int64_t)r.iterations;
+            if (x_out && r.primal.size() == probs[(std::size_t)i].num_cols)
+                std::memcpy(x_out + col_off[i], r.primal.data(), 8 * r.primal.size());
+        }
+        const auto& S = solver.stats();
+        if (stats) {
+            stats->rows = (int64_t)S.rows;
+            stats->cols = (int64_t)S.cols;
+            stats->nnz = (int64_t)S.nnz;
+            stats->nnz_normal = (int64_t)S.nnz_normal;
+            stats->iterations = S.iterations;
+            stats->total_ms = S.total_ms;
+            stats->factor_ms = S.factor_ms;
+            stats->solve_ms = S.solve_ms;
+        }
+        if (!S.error.empty()) throw std::runtime_error(S.error);
+    });
+}
+
 int hn_be_create(int device, hn_backend** out) {
     return wrap([&] {
         auto* b = new hn_backend(device);

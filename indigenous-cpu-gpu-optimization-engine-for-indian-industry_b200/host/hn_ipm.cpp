@@ -19,15 +19,7 @@
 #include "hn_sm100.h"
 
 namespace hn::lp {
-namespace {
-
-using model::ConstraintSense;
-using model::ProblemStatus;
-
-void ck(int st, const char* what) {
-    if (st != HN_OK) throw std::runtime_error(std::string(what) + ": " + hn_last_error());
-}
-
+namespace detail {
 // ---- standard form (interior_point.cpp:29-49, 202-373) ----
 struct VarInfo {
     std::vector<int> slots;
@@ -44,6 +36,19 @@ struct StandardForm {
     double offset = 0.0;
     std::vector<VarInfo> var_info;
 };
+
+}  // namespace detail
+using detail::StandardForm;
+using detail::VarInfo;
+
+namespace {
+
+using model::ConstraintSense;
+using model::ProblemStatus;
+
+void ck(int st, const char* what) {
+    if (st != HN_OK) throw std::runtime_error(std::string(what) + ": " + hn_last_error());
+}
 
 struct Trip {
     std::size_t r, c;
@@ -306,6 +311,62 @@ void refine(const DenseLDLT& fac, const HostNormal& N, std::vector<double>& x, c
 constexpr std::size_t kMaxDenseRows = 12000;
 
 }  // namespace
+
+void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol, PackedForm& out) {
+    const std::size_t K = problems.size();
+    std::vector<std::shared_ptr<StandardForm>> forms(K);
+    std::string err;
+#pragma omp parallel for schedule(dynamic, 8)
+    for (std::size_t i = 0; i < K; ++i) {
+        try {
+            auto f = std::make_shared<StandardForm>(build_standard_form(remove_duplicate_rows(problems[i]), feas_tol));
+            forms[i] = f;
+        } catch (const std::exception& e) {
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if (!err.empty()) throw std::runtime_error(err);
+    out = PackedForm{};
+    std::size_t nnz = 0;
+    for (std::size_t i = 0; i < K; ++i) {
+        const StandardForm& f = *forms[i];
+        if (f.m == 0 || f.n == 0)
+            throw std::invalid_argument("batch instance " + std::to_string(i) + " has an empty standard form");
+        out.row_off.push_back(out.row_off.back() + (int64_t)f.m);
+        out.col_off.push_back(out.col_off.back() + (int64_t)f.n);
+        nnz += f.val.size();
+    }
+    out.rp.reserve(out.row_off.back() + 1);
+    out.ci.reserve(nnz);
+    out.val.reserve(nnz);
+    for (std::size_t i = 0; i < K; ++i) {
+        const StandardForm& f = *forms[i];
+        const uint64_t cb = (uint64_t)out.col_off[i];
+        for (std::size_t r = 0; r < f.m; ++r) {
+            for (std::size_t k = f.rp[r]; k < f.rp[r + 1]; ++k) {
+                out.ci.push_back(cb + f.ci[k]);
+                out.val.push_back(f.val[k]);
+            }
+            out.rp.push_back(out.ci.size());
+        }
+        out.rhs.insert(out.rhs.end(), f.rhs.begin(), f.rhs.end());
+        out.c.insert(out.c.end(), f.c.begin(), f.c.end());
+        // start point per instance (:439-453)
+        double b_norm = 1.0, c_norm = 1.0;
+        for (double v : f.rhs) b_norm = std::max(b_norm, std::abs(v));
+        for (double v : f.c) c_norm = std::max(c_norm, std::abs(v));
+        for (std::size_t j = 0; j < f.n; ++j) {
+            out.x0.push_back(b_norm + 1.0);
+            out.z0.push_back(std::max(c_norm + 1.0, std::abs(f.c[j])));
+        }
+    }
+    out.forms = std::move(forms);
+}
+
+std::vector<double> to_original_primal_packed(const PackedForm& pf, std::size_t i, const std::vector<double>& y) {
+    return to_original_primal(*pf.forms[i], y);
+}
 
 InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) {
     const auto start = Clock::now();

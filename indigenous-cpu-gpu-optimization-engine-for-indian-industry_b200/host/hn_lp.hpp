@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <functional>
 #include <limits>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -94,6 +95,45 @@ public:
 
 private:
     InteriorPointOptions options_;
+};
+
+// ---- batched solver ----
+namespace detail {
+struct StandardForm;
+}
+
+// Standard forms of a batch packed block-diagonally (instance i: rows
+// row_off[i]..row_off[i+1], columns col_off[i]..col_off[i+1]) with their start
+// points; the matrix in the reference's CSR layout.
+struct PackedForm {
+    std::vector<int64_t> row_off{0}, col_off{0};
+    std::vector<uint64_t> rp{0}, ci;
+    std::vector<double> val, rhs, c, x0, z0;
+    std::vector<std::shared_ptr<detail::StandardForm>> forms;
+};
+void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol, PackedForm& out);
+std::vector<double> to_original_primal_packed(const PackedForm& pf, std::size_t i, const std::vector<double>& y);
+
+struct BatchStats {
+    std::size_t rows = 0, cols = 0, nnz = 0, nnz_normal = 0;
+    int iterations = 0;
+    double total_ms = 0.0, factor_ms = 0.0, solve_ms = 0.0;
+    std::vector<std::size_t> running_per_iter;
+    std::string error;
+};
+
+// Many LPs advanced in lockstep on the GPU (csrc/hn_batch.cu); each result
+// has the meaning of InteriorPointSolver::solve's for its instance.
+class BatchInteriorPointSolver {
+public:
+    explicit BatchInteriorPointSolver(const InteriorPointOptions& options = InteriorPointOptions())
+        : options_(options) {}
+    std::vector<InteriorPointResult> solve(const std::vector<model::LpProblem>& problems);
+    const BatchStats& stats() const { return stats_; }
+
+private:
+    InteriorPointOptions options_;
+    BatchStats stats_;
 };
 
 // Dense LDL^T of a symmetric m x m matrix (lower triangle, row-major) with the
