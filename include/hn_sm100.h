@@ -262,6 +262,47 @@ int hn_batch_update(hn_batch* B, double* x_dev, const double* dx_dev, double* z_
                     double* lam_dev, const double* dlam_dev, const double* scal_dev, int32_t* status_dev,
                     int32_t* iters_dev, int iter, void* stream);
 
+/* ---- revised-simplex pricing (core/lp/simplex.cpp) ----
+ * The per-iteration O(nnz + n) pricing work of SimplexSolver over the
+ * matrix's device A^T; FTRAN/BTRAN (the basis factorisation) stay on the host.
+ * All vectors are device pointers of the matrix's sizes. */
+
+/* rc = cost - A^T y, bit-identical to compute_reduced_costs
+ * (simplex.cpp:1225-1233) through SparseMatrix::transpose_multiply. */
+int hn_price_reduced_costs(const hn_csr* A, const double* y_dev, const double* cost_dev, double* rc_dev,
+                           void* stream);
+/* Devex reference-framework update of update_devex_weights
+ * (simplex.cpp:1235-1271): alpha = A^T u (u = e_leaving^T B^-1 from the
+ * host's BTRAN, written to alpha_dev, n doubles), s = max |alpha_j| over
+ * nonbasic j (nonbasis_dev[j] >= 0), and, when s != 0, for nonbasic j
+ * w_j = max(w_j, (alpha_j / s)^2). */
+int hn_price_devex_update(const hn_csr* A, const double* u_dev, const int32_t* nonbasis_dev, double* weights_dev,
+                          double* alpha_dev, void* stream);
+
+#define HN_PRICE_BLAND 0  /* first improving column (bland_rule, simplex.cpp:1328-1338) */
+#define HN_PRICE_RANKED 1 /* |rc|/sqrt(w) descending, index ascending (ranked_candidates, :1283-1308) */
+#define HN_PRICE_MAX_K 64
+/* Entering-column choice of select_entering_variable (simplex.cpp:1321-1361).
+ * Column j is improving when nonbasis[j] >= 0, it is not artificial
+ * (artificial_dev[j] == 0, or phase1 != 0, or artificial_dev NULL) and
+ * rc' < -optimality_tol with rc' = maximize ? -rc_j : rc_j. Writes to out_dev
+ * (device, k + 1 int64): out[0] = number of improving columns; for
+ * HN_PRICE_BLAND out[1] = the lowest improving index or -1; for
+ * HN_PRICE_RANKED (1 <= k <= HN_PRICE_MAX_K) out[1..k] = the first k of
+ * ranked_candidates' order (score |rc'|/sqrt(w_j), w_j replaced by 1 when not
+ * finite and positive, weights_dev NULL meaning all 1; ties by lower index),
+ * -1 past the end. Reduced costs must not be NaN (the reference's ordering
+ * is undefined there). */
+int hn_price_select(int64_t n, const double* rc_dev, const double* weights_dev, const int32_t* nonbasis_dev,
+                    const uint8_t* artificial_dev, int phase1, int maximize, double optimality_tol, int rule,
+                    int64_t k, int64_t* out_dev, void* stream);
+/* Dense columns cols[r] of A into out (device, m x k column-major), the
+ * vectors extract_column (simplex.cpp:25-35) builds for the ratio test and
+ * exact steepest-edge weights. Indices outside [0, n) leave their column zero
+ * and make the call fail with HN_ERR_INVALID_ARG (the call synchronises the
+ * stream to report it). */
+int hn_price_columns(const hn_csr* A, int64_t k, const int64_t* cols_dev, double* out_dev, void* stream);
+
 /* ---- SpMV for callers that cannot allocate device memory ----
  * No counterpart in the reference. y = A x with A given as device CSR arrays
  * (int32 row_ptr m+1, int32 col_idx and double values nnz, row_ptr[m] == nnz,

@@ -38,7 +38,7 @@ constexpr int kT = 256;
 constexpr int64_t kMaxBitmapWords = 12500;  // row reach <= 400,000 columns: four W-word arrays in 200 KB of shared memory
 constexpr uint32_t kMulti = 0x80000000u;
 constexpr int64_t kDiagFlag = int64_t(1) << 62;
-constexpr int kSlotsPerThread = 4;  // slots per thread per trip of the numeric kernel
+constexpr int kSlotsPerThread = 8;  // slots per thread per trip of the numeric kernel
 
 __device__ __forceinline__ uint32_t bit_of(int k) { return 1u << (k & 31); }
 
@@ -258,16 +258,22 @@ __global__ void __launch_bounds__(kT) ada_fill_kernel(
 }
 
 // ---- numeric ----
-__device__ __forceinline__ double term(uint2 pe, const double* __restrict__ val, const int32_t* __restrict__ ci,
-                                       const double* __restrict__ valT, const double* __restrict__ d) {
-    const double dj = __ldg(d + __ldg(ci + pe.y));
-    return (dj <= 0.0) ? 0.0 : (__ldg(val + pe.y) * __ldg(valT + pe.x)) * dj;  // columns with D_j <= 0 skipped
+// vd[e] = (A value e, d of its column): one 16-byte gather per term instead of
+// a value load plus a dependent column-index -> d chain.
+__global__ void ada_vd_kernel(int64_t nnz, const double* __restrict__ val, const int32_t* __restrict__ ci,
+                              const double* __restrict__ d, double2* __restrict__ vd) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x)
+        vd[e] = make_double2(val[e], __ldg(d + ci[e]));
+}
+
+__device__ __forceinline__ double term(uint2 pe, const double2* __restrict__ vd, const double* __restrict__ valT) {
+    const double2 q = __ldg(vd + pe.y);
+    return (q.y <= 0.0) ? 0.0 : (q.x * __ldg(valT + pe.x)) * q.y;  // columns with D_j <= 0 skipped
 }
 
 __global__ void __launch_bounds__(kT) ada_slot_kernel(int64_t nnz, const uint2* __restrict__ gmap,
-                                                      const double* __restrict__ val, const int32_t* __restrict__ ci,
-                                                      const double* __restrict__ valT, const double* __restrict__ d,
-                                                      double* __restrict__ nval) {
+                                                      const double2* __restrict__ vd,
+                                                      const double* __restrict__ valT, double* __restrict__ nval) {
     const int64_t stride = (int64_t)gridDim.x * kT * kSlotsPerThread;
     for (int64_t t0 = blockIdx.x * (int64_t)kT * kSlotsPerThread + threadIdx.x; t0 < nnz; t0 += stride) {
         uint2 g[kSlotsPerThread];
@@ -279,20 +285,19 @@ __global__ void __launch_bounds__(kT) ada_slot_kernel(int64_t nnz, const uint2* 
 #pragma unroll
         for (int u = 0; u < kSlotsPerThread; ++u) {
             const int64_t t = t0 + (int64_t)u * kT;
-            if (!(g[u].x & kMulti)) __stcs(nval + t, term(g[u], val, ci, valT, d));
+            if (!(g[u].x & kMulti)) __stcs(nval + t, term(g[u], vd, valT));
         }
     }
 }
 
 __global__ void ada_combine_kernel(int64_t nms, const int64_t* __restrict__ mpos, const int32_t* __restrict__ mbeg,
-                                   const uint2* __restrict__ mlist, const double* __restrict__ val,
-                                   const int32_t* __restrict__ ci, const double* __restrict__ valT,
-                                   const double* __restrict__ d, double* __restrict__ nval,
+                                   const uint2* __restrict__ mlist, const double2* __restrict__ vd,
+                                   const double* __restrict__ valT, double* __restrict__ nval,
                                    unsigned long long* maxdiag) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= nms) return;
     double s = 0.0;
-    for (int32_t u = mbeg[t]; u < mbeg[t + 1]; ++u) s += term(mlist[u], val, ci, valT, d);
+    for (int32_t u = mbeg[t]; u < mbeg[t + 1]; ++u) s += term(mlist[u], vd, valT);
     const int64_t mp = mpos[t];
     nval[mp & ~kDiagFlag] = s;
     if ((mp & kDiagFlag) && s > 0.0) atomicMax(maxdiag, static_cast<unsigned long long>(__double_as_longlong(s)));
@@ -312,7 +317,7 @@ __global__ void ada_reg_kernel(int m, const int64_t* __restrict__ diag_pos, doub
 void free_pattern(hn_pattern* P) {
     if (!P) return;
     for (void* p : {(void*)P->rp, (void*)P->ci, (void*)P->diag_pos, (void*)P->maxdiag, (void*)P->gmap,
-                    (void*)P->mpos, (void*)P->mbeg, (void*)P->mlist})
+                    (void*)P->mpos, (void*)P->mbeg, (void*)P->mlist, (void*)P->vd})
         dfree(p);
     delete P;
 }
@@ -329,13 +334,17 @@ void launch_numeric(const hn_pattern* P, const double* d, double* nval, cudaStre
     const int64_t per_block = (int64_t)kT * kSlotsPerThread;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P->nnz + per_block - 1) / per_block,
                                                                  (int64_t)ctx().sm_count * 16));
-    ada_slot_kernel<<<grid, kT, 0, s>>>(P->nnz, P->gmap, A->val, A->ci, A->valT, d, nval);
+    if (A->nnz > 0) {
+        const int gv = (int)std::min<int64_t>((A->nnz + kT - 1) / kT, (int64_t)ctx().sm_count * 16);
+        ada_vd_kernel<<<gv, kT, 0, s>>>(A->nnz, A->val, A->ci, d, P->vd);
+        launched("ada_vd_kernel");
+    }
+    ada_slot_kernel<<<grid, kT, 0, s>>>(P->nnz, P->gmap, P->vd, A->valT, nval);
     launched("ada_slot_kernel");
     check_cuda(cudaMemsetAsync(P->maxdiag, 0, sizeof(unsigned long long), s), "memset maxdiag");
     if (P->nms > 0) {
         ada_combine_kernel<<<(unsigned)((P->nms + 255) / 256), 256, 0, s>>>(P->nms, P->mpos, P->mbeg, P->mlist,
-                                                                            A->val, A->ci, A->valT, d, nval,
-                                                                            P->maxdiag);
+                                                                            P->vd, A->valT, nval, P->maxdiag);
         launched("ada_combine_kernel");
     }
 }
@@ -389,6 +398,7 @@ int hn_ada_symbolic(const hn_csr* A, hn_pattern** out) {
             P->rp = dmalloc<int64_t>(m + 1);
             P->diag_pos = dmalloc<int64_t>(m);
             P->maxdiag = dmalloc<unsigned long long>(1);
+            P->vd = dmalloc<double2>(A->nnz > 0 ? A->nnz : 1);
             nq = dmalloc<int64_t>(m + 1);
             nms = dmalloc<int64_t>(m + 1);
             nmq = dmalloc<int64_t>(m + 1);

@@ -261,32 +261,40 @@ __global__ void batch_dense_kernel(int64_t m, const int64_t* __restrict__ row_of
     }
 }
 
-// Blocked right-looking LDL^T, level-synchronous over the batch: block step s
-// runs two launches for every instance that still has a block s --
-//   batch_ldlt_panel_kernel: one CTA per instance factorises the 32x32
+// Blocked right-looking LDL^T, level-synchronous over the batch, in blocks of
+// kFb columns: block step s runs two launches for every instance that still
+// has a block s --
+//   batch_ldlt_panel_kernel: one CTA per instance factorises the kFb x kFb
 //     diagonal block (pivot clamp of factorization.cpp:1299-1305) and solves
 //     the panel below it, one row per thread;
-//   batch_ldlt_update_kernel: all instances' trailing 32x32 tiles
-//     A_rc -= sum_q (L_rq D_q) L_cq, spread over every CTA of the GPU.
+//   batch_ldlt_update_kernel: all instances' trailing kFb x kFb tiles
+//     A_rc -= sum_q (L_rq D_q) L_cq, spread over every CTA of the GPU, each
+//     thread accumulating a 4 x 4 block of the tile in registers.
+constexpr int kFb = 64;
+constexpr int kFbP = kFb + 1;  // padded smem row (conflict-free column walks)
+constexpr size_t kPanelSmem = sizeof(double) * (kFb * kFbP + kFb);
+constexpr size_t kUpdateSmem = sizeof(double) * 2 * kFb * kFbP;
+
 __global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, const int64_t* __restrict__ row_off,
                                                               const int64_t* __restrict__ dn_off,
                                                               const int32_t* __restrict__ order,
                                                               const int32_t* __restrict__ status,
                                                               double* __restrict__ dense, double* __restrict__ dD,
                                                               double tol) {
-    __shared__ double sA[kNb][kNb + 1];
-    __shared__ double sD[kNb];
+    extern __shared__ double smem[];
+    double(*sA)[kFbP] = reinterpret_cast<double(*)[kFbP]>(smem);
+    double* sD = smem + kFb * kFbP;
     const int tid = threadIdx.x;
     const int inst = order[blockIdx.x];
     if (status[inst] != ST_RUN) return;
     const int64_t r0 = row_off[inst];
     const int m = static_cast<int>(row_off[inst + 1] - r0);
-    const int k0 = s * kNb;
+    const int k0 = s * kFb;
     if (k0 >= m) return;
-    const int nb = min(kNb, m - k0), k1 = k0 + nb;
+    const int nb = min(kFb, m - k0), k1 = k0 + nb;
     double* A = dense + dn_off[inst];
-    for (int idx = tid; idx < kNb * kNb; idx += kT) {
-        const int r = idx / kNb, c = idx % kNb;
+    for (int idx = tid; idx < kFb * kFb; idx += kT) {
+        const int r = idx / kFb, c = idx % kFb;
         sA[r][c] = (r < nb && c <= r) ? A[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
     }
     __syncthreads();
@@ -313,12 +321,12 @@ __global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, const int64
     if (tid < nb) dD[r0 + k0 + tid] = sD[tid];
     // panel below: L[r, k0:k1] = A[r, k0:k1] (L_blk D)^-T
     for (int r = k1 + tid; r < m; r += kT) {
-        double lv[kNb];
+        double lv[kFb];
         double* Ar = A + (int64_t)r * m + k0;
 #pragma unroll
-        for (int c = 0; c < kNb; ++c) lv[c] = (c < nb) ? Ar[c] : 0.0;
+        for (int c = 0; c < kFb; ++c) lv[c] = (c < nb) ? Ar[c] : 0.0;
 #pragma unroll
-        for (int c = 0; c < kNb; ++c) {
+        for (int c = 0; c < kFb; ++c) {
             if (c < nb) {
                 double v = lv[c];
 #pragma unroll
@@ -327,7 +335,7 @@ __global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, const int64
             }
         }
 #pragma unroll
-        for (int c = 0; c < kNb; ++c)
+        for (int c = 0; c < kFb; ++c)
             if (c < nb) Ar[c] = lv[c];
     }
 }
@@ -340,10 +348,14 @@ __global__ void __launch_bounds__(kT) batch_ldlt_update_kernel(int s, int cnt, i
                                                                const int32_t* __restrict__ status,
                                                                double* __restrict__ dense,
                                                                const double* __restrict__ dD) {
-    __shared__ double sW[kNb][kNb + 1];
-    __shared__ double sL[kNb][kNb + 1];
+    extern __shared__ double smem[];
+    // k-major copies of the two panel slices: sW[q][r] = L[rb+r, k0+q] D_q,
+    // sL[q][c] = L[cb+c, k0+q]
+    double(*sW)[kFbP] = reinterpret_cast<double(*)[kFbP]>(smem);
+    double(*sL)[kFbP] = reinterpret_cast<double(*)[kFbP]>(smem + kFb * kFbP);
     const int tid = threadIdx.x;
-    const int k0 = s * kNb;
+    const int ty = tid >> 4, tx = tid & 15;
+    const int k0 = s * kFb;
     for (int64_t pidx = blockIdx.x; pidx < npairs; pidx += gridDim.x) {
         // instance of this pair: first b with pairs[b] > pidx (pairs is inclusive)
         int lo = 0, hi = cnt - 1;
@@ -359,36 +371,47 @@ __global__ void __launch_bounds__(kT) batch_ldlt_update_kernel(int s, int cnt, i
         const int64_t local = pidx - (lo > 0 ? pairs[lo - 1] : 0);
         const int64_t r0 = row_off[inst];
         const int m = static_cast<int>(row_off[inst + 1] - r0);
-        const int nb = min(kNb, m - k0), k1 = k0 + nb;
+        const int nb = min(kFb, m - k0), k1 = k0 + nb;
         int ti = static_cast<int>((sqrt(8.0 * (double)local + 1.0) - 1.0) * 0.5);
         while ((int64_t)(ti + 1) * (ti + 2) / 2 <= local) ++ti;
         while ((int64_t)ti * (ti + 1) / 2 > local) --ti;
         const int tj = static_cast<int>(local - (int64_t)ti * (ti + 1) / 2);
-        const int rb = k1 + ti * kNb, cb = k1 + tj * kNb;
+        const int rb = k1 + ti * kFb, cb = k1 + tj * kFb;
         double* A = dense + dn_off[inst];
         const double* Dv = dD + r0 + k0;
         __syncthreads();
-        for (int idx = tid; idx < kNb * kNb; idx += kT) {
-            const int rr = idx / kNb, q = idx % kNb;
+        for (int idx = tid; idx < kFb * kFb; idx += kT) {
+            const int rr = idx / kFb, q = idx % kFb;
             const bool okr = rb + rr < m && q < nb, okc = cb + rr < m && q < nb;
-            sW[rr][q] = okr ? A[(int64_t)(rb + rr) * m + k0 + q] * Dv[q] : 0.0;
-            sL[rr][q] = okc ? A[(int64_t)(cb + rr) * m + k0 + q] : 0.0;
+            sW[q][rr] = okr ? A[(int64_t)(rb + rr) * m + k0 + q] * Dv[q] : 0.0;
+            sL[q][rr] = okc ? A[(int64_t)(cb + rr) * m + k0 + q] : 0.0;
         }
         __syncthreads();
-        const int rr = tid >> 3, cc0 = (tid & 7) * 4;
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 8
-        for (int q = 0; q < kNb; ++q) {
-            const double w = sW[rr][q];
+        double acc[4][4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) acc[u] += w * sL[cc0 + u][q];
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+#pragma unroll 4
+        for (int q = 0; q < kFb; ++q) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = sW[q][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = sL[q][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
         }
-        const int gr = rb + rr;
-        if (gr < m) {
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int gc = cb + cc0 + u;
-                if (gc <= gr) A[(int64_t)gr * m + gc] -= acc[u];
+        for (int i = 0; i < 4; ++i) {
+            const int gr = rb + ty + 16 * i;
+            if (gr >= m) continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int gc = cb + tx + 16 * j;
+                if (gc <= gr) A[(int64_t)gr * m + gc] -= acc[i][j];
             }
         }
     }
@@ -638,7 +661,7 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
             // level schedule (instances in decreasing size: the ones with a block
             // at step s form a prefix of `order`)
             const int64_t mmax = row_off_host[order[0] + 1] - row_off_host[order[0]];
-            B->nsteps = (mmax + kNb - 1) / kNb;
+            B->nsteps = (mmax + kFb - 1) / kFb;
             B->pair_off_h.assign(1, 0);
             std::vector<int64_t> flat;
             for (int64_t st = 0; st < B->nsteps; ++st) {
@@ -646,9 +669,9 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
                 int64_t acc = 0;
                 for (int64_t b = 0; b < K; ++b) {
                     const int64_t mi = row_off_host[order[b] + 1] - row_off_host[order[b]];
-                    if (mi <= st * kNb) break;
-                    const int64_t rest = mi - std::min<int64_t>(mi, (st + 1) * kNb);
-                    const int64_t T = (rest + kNb - 1) / kNb;
+                    if (mi <= st * kFb) break;
+                    const int64_t rest = mi - std::min<int64_t>(mi, (st + 1) * kFb);
+                    const int64_t T = (rest + kFb - 1) / kFb;
                     acc += T * (T + 1) / 2;
                     flat.push_back(acc);
                     ++cnt;
@@ -658,6 +681,9 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
                 B->pair_off_h.push_back((int64_t)flat.size());
             }
             B->step_pairs = dmalloc<int64_t>(flat.size());
+            check_cuda(cudaFuncSetAttribute(batch_ldlt_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kUpdateSmem),
+                       "update kernel smem");
             check_cuda(cudaMemcpy(B->step_pairs, flat.data(), sizeof(int64_t) * flat.size(), cudaMemcpyHostToDevice),
                        "H2D schedule");
             check_cuda(cudaStreamSynchronize(s), "batch create sync");
@@ -708,13 +734,13 @@ int hn_batch_factor(hn_batch* B, const double* D, double reg, double singular_to
         launched("batch_dense_kernel");
         for (int64_t st = 0; st < B->nsteps; ++st) {
             const int cnt = B->step_cnt[st];
-            batch_ldlt_panel_kernel<<<cnt, kT, 0, s>>>((int)st, B->row_off, B->dn_off, B->order, status, B->dense,
+            batch_ldlt_panel_kernel<<<cnt, kT, kPanelSmem, s>>>((int)st, B->row_off, B->dn_off, B->order, status, B->dense,
                                                        B->dD, singular_tol);
             launched("batch_ldlt_panel_kernel");
             const int64_t np = B->step_pairs_h[st];
             if (np > 0) {
                 const int grid = (int)std::min<int64_t>(np, (int64_t)ctx().sm_count * 8);
-                batch_ldlt_update_kernel<<<grid, kT, 0, s>>>((int)st, cnt, np, B->step_pairs + B->pair_off_h[st],
+                batch_ldlt_update_kernel<<<grid, kT, kUpdateSmem, s>>>((int)st, cnt, np, B->step_pairs + B->pair_off_h[st],
                                                              B->row_off, B->dn_off, B->order, status, B->dense,
                                                              B->dD);
                 launched("batch_ldlt_update_kernel");

@@ -44,6 +44,7 @@ Workspace& workspace(cudaStream_t s) {
     Workspace w;
     w.partials = dmalloc<double>(4 * kMaxReduceBlocks + 8);
     w.counter = dmalloc<unsigned>(4);
+    w.select = dmalloc<unsigned long long>(kSelectWords);
     check_cuda(cudaMemsetAsync(w.counter, 0, 4 * sizeof(unsigned), s), "workspace init");
     check_cuda(cudaStreamSynchronize(s), "workspace init sync");
     return g_ctx.ws.emplace(s, w).first->second;
@@ -238,6 +239,7 @@ int hn_shutdown(void) {
         for (auto& kv : c.ws) {
             dfree(kv.second.partials);
             dfree(kv.second.counter);
+            dfree(kv.second.select);
             dfree(kv.second.staging_d);
             if (kv.second.staging_h) cudaFreeHost(kv.second.staging_h);
         }

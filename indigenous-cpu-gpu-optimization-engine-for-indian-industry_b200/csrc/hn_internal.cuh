@@ -45,7 +45,9 @@ struct Workspace {
     size_t staging_bytes = 0;
     double* staging_d = nullptr;   // device staging for *_host calls
     size_t staging_d_bytes = 0;
+    unsigned long long* select = nullptr;  // pricing selection state, kSelectWords words
 };
+constexpr int kSelectWords = 8;
 
 constexpr int kMaxReduceBlocks = 1184;  // 148 SMs x 8
 
@@ -316,4 +318,5 @@ struct hn_pattern {
     int32_t* mbeg = nullptr;         // nms+1
     int64_t nmq = 0;                 // terms into those slots
     uint2* mlist = nullptr;          // nmq
+    double2* vd = nullptr;           // nnz(A): (A value, d of its column), per numeric call
 };

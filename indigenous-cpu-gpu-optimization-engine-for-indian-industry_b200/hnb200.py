@@ -87,6 +87,10 @@ SIGNATURES = {
     "hn_ipm_update": [_i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "hn_max_step": [_i64, _vp, _vp, _vp, _vp],
     "hn_spmv_noalloc": [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp],
+    "hn_price_reduced_costs": [_vp, _vp, _vp, _vp, _vp],
+    "hn_price_devex_update": [_vp, _vp, _vp, _vp, _vp, _vp],
+    "hn_price_select": [_i64, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_double, C.c_int, _i64, _vp, _vp],
+    "hn_price_columns": [_vp, _i64, _vp, _vp, _vp],
     "hn_batch_create": [_i64, _i64p, _i64p, _vp, C.POINTER(_vp)],
     "hn_batch_destroy": [_vp],
     "hn_batch_residuals": [_vp, _vp] + [_vp] * 13 + [C.c_int, C.c_double, C.c_double, _vp],
@@ -294,6 +298,32 @@ def nrm_inf(n, v, out, stream=None) -> None:
 
 def nrm2(n, v, out, stream=None) -> None:
     check(load().hn_nrm2(n, _ptr(v), _ptr(out), _ptr(stream)))
+
+
+# ---- revised-simplex pricing (device vectors are torch CUDA tensors) ----
+PRICE_BLAND, PRICE_RANKED = 0, 1
+
+
+def price_reduced_costs(A: Csr, y, cost, rc, stream=None) -> None:
+    """rc = cost - A^T y (SimplexSolver::compute_reduced_costs)."""
+    check(load().hn_price_reduced_costs(A.h, _ptr(y), _ptr(cost), _ptr(rc), _ptr(stream)))
+
+
+def price_devex_update(A: Csr, u, nonbasis, weights, alpha, stream=None) -> None:
+    """Devex weights from the BTRAN row u (SimplexSolver::update_devex_weights)."""
+    check(load().hn_price_devex_update(A.h, _ptr(u), _ptr(nonbasis), _ptr(weights), _ptr(alpha), _ptr(stream)))
+
+
+def price_select(n, rc, weights, nonbasis, artificial, out, phase1=False, maximize=False, tol=1e-9,
+                 rule=PRICE_RANKED, k=1, stream=None) -> None:
+    """Entering-column choice into out (device int64, k+1): count, then indices."""
+    check(load().hn_price_select(n, _ptr(rc), _ptr(weights), _ptr(nonbasis), _ptr(artificial), int(phase1),
+                                 int(maximize), tol, rule, k, _ptr(out), _ptr(stream)))
+
+
+def price_columns(A: Csr, cols, out, stream=None) -> None:
+    """Dense columns of A (m x k, column-major) for the given device int64 indices."""
+    check(load().hn_price_columns(A.h, int(cols.numel()), _ptr(cols), _ptr(out), _ptr(stream)))
 
 
 def exported_symbols() -> list[str]:

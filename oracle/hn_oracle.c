@@ -307,3 +307,99 @@ void hno_merge_tiles(int64_t m, int64_t nnz, const int32_t* rp, int64_t items, i
         tile_nz[t] = (int32_t)(diag - lo);
     }
 }
+
+/* ---------------------------------------------------------------- pricing */
+
+void hno_price_reduced_costs(int64_t m, int64_t n, const int64_t* rp, const int64_t* ci, const double* val,
+                             const double* y, const double* cost, double* rc) {
+    /* simplex.cpp:1229-1232 */
+    hno_csr_tmultiply(m, n, rp, ci, val, y, rc);
+    for (int64_t j = 0; j < n; ++j) rc[j] = cost[j] - rc[j];
+}
+
+void hno_price_devex_update(int64_t m, int64_t n, const int64_t* rp, const int64_t* ci, const double* val,
+                            const double* u, const int32_t* nonbasis, double* weights, double* alpha) {
+    /* simplex.cpp:1249-1270 */
+    for (int64_t j = 0; j < n; ++j) alpha[j] = 0.0;
+    for (int64_t i = 0; i < m; ++i) {
+        if (u[i] == 0.0) continue;
+        for (int64_t k = rp[i]; k < rp[i + 1]; ++k) alpha[ci[k]] += val[k] * u[i];
+    }
+    double s = 0.0;
+    for (int64_t j = 0; j < n; ++j) {
+        if (nonbasis[j] < 0) continue;
+        const double a = fabs(alpha[j]);
+        s = (s < a) ? a : s; /* std::max(s, a) */
+    }
+    if (s == 0.0) return;
+    for (int64_t j = 0; j < n; ++j) {
+        if (nonbasis[j] < 0) continue;
+        const double t = alpha[j] / s;
+        const double w = t * t;
+        if (w > weights[j]) weights[j] = w;
+    }
+}
+
+typedef struct {
+    int64_t j;
+    double score;
+} hno_ranked;
+
+static int hno_ranked_cmp(const void* pa, const void* pb) {
+    const hno_ranked* a = (const hno_ranked*)pa;
+    const hno_ranked* b = (const hno_ranked*)pb;
+    if (a->score != b->score) return a->score > b->score ? -1 : 1;
+    return a->j < b->j ? -1 : (a->j > b->j ? 1 : 0);
+}
+
+int64_t hno_price_ranked(int64_t n, const double* rc, const double* w, const int32_t* nonbasis,
+                         const uint8_t* artificial, int phase1, int maximize, double tol, int64_t cap,
+                         int64_t* out) {
+    /* simplex.cpp:1283-1308: filter, score |rc|/sqrt(w) with w guarded, sort by
+     * (score desc, index asc) -- a total order, so qsort gives stable_sort's result */
+    hno_ranked* r = (hno_ranked*)malloc(sizeof(hno_ranked) * (size_t)(n > 0 ? n : 1));
+    int64_t cnt = 0;
+    for (int64_t j = 0; j < n; ++j) {
+        if (nonbasis[j] < 0) continue;
+        if (!phase1 && artificial && artificial[j]) continue;
+        double c = rc[j];
+        if (maximize) c = -c;
+        if (c >= -tol) continue;
+        double wj = w ? w[j] : 1.0;
+        if (!(wj > 0.0) || !isfinite(wj)) wj = 1.0;
+        r[cnt].j = j;
+        r[cnt].score = fabs(c) / sqrt(wj);
+        ++cnt;
+    }
+    qsort(r, (size_t)cnt, sizeof(hno_ranked), hno_ranked_cmp);
+    for (int64_t k = 0; k < cap; ++k) out[k] = k < cnt ? r[k].j : -1;
+    free(r);
+    return cnt;
+}
+
+int64_t hno_price_bland(int64_t n, const double* rc, const int32_t* nonbasis, const uint8_t* artificial,
+                        int phase1, int maximize, double tol) {
+    /* simplex.cpp:1328-1338 */
+    for (int64_t j = 0; j < n; ++j) {
+        if (nonbasis[j] < 0) continue;
+        if (!phase1 && artificial && artificial[j]) continue;
+        double c = rc[j];
+        if (maximize) c = -c;
+        if (c < -tol) return j;
+    }
+    return -1;
+}
+
+void hno_extract_column(int64_t m, const int64_t* rp, const int64_t* ci, const double* val, int64_t j,
+                        double* col) {
+    /* simplex.cpp:25-35 */
+    for (int64_t i = 0; i < m; ++i) {
+        col[i] = 0.0;
+        for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+            if (ci[k] == j) {
+                col[i] = val[k];
+                break;
+            }
+        }
+    }
+}

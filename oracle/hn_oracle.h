@@ -72,6 +72,28 @@ int64_t hno_ada_pattern(int64_t m, int64_t n, const int64_t* rp, const int64_t* 
 void hno_merge_tiles(int64_t m, int64_t nnz, const int32_t* rp, int64_t items, int64_t ntiles,
                      int32_t* tile_row, int32_t* tile_nz);
 
+/* ---- revised-simplex pricing (core/lp/simplex.cpp) ---- */
+/* rc = cost - A^T y, A^T y by transpose_multiply's scatter
+ * (compute_reduced_costs, simplex.cpp:1225-1233). */
+void hno_price_reduced_costs(int64_t m, int64_t n, const int64_t* rp, const int64_t* ci, const double* val,
+                             const double* y, const double* cost, double* rc);
+/* update_devex_weights (simplex.cpp:1235-1271) with the BTRAN row u given;
+ * alpha (n) receives A^T u. */
+void hno_price_devex_update(int64_t m, int64_t n, const int64_t* rp, const int64_t* ci, const double* val,
+                            const double* u, const int32_t* nonbasis, double* weights, double* alpha);
+/* ranked_candidates (simplex.cpp:1283-1308): writes the first `cap` indices
+ * of the ranking into out, returns the number of candidates. */
+int64_t hno_price_ranked(int64_t n, const double* rc, const double* w, const int32_t* nonbasis,
+                         const uint8_t* artificial, int phase1, int maximize, double tol, int64_t cap,
+                         int64_t* out);
+/* The Bland branch of select_entering_variable (simplex.cpp:1328-1338). */
+int64_t hno_price_bland(int64_t n, const double* rc, const int32_t* nonbasis, const uint8_t* artificial,
+                        int phase1, int maximize, double tol);
+/* extract_column (simplex.cpp:25-35): col (m) = column j of A, the first
+ * entry with that column in each row. */
+void hno_extract_column(int64_t m, const int64_t* rp, const int64_t* ci, const double* val, int64_t j,
+                        double* col);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,6 +24,7 @@ _i64p = C.POINTER(C.c_int64)
 _u64p = C.POINTER(C.c_uint64)
 _f64p = C.POINTER(C.c_double)
 _i32p = C.POINTER(C.c_int32)
+_u8p = C.POINTER(C.c_uint8)
 
 _port = None
 _ref = None
@@ -62,6 +63,12 @@ def port():
                                             _i64p, _f64p, _f64p]),
             "hno_ada_pattern": (_i64, [_i64, _i64, _i64p, _i64p, _i64p, _i32p]),
             "hno_merge_tiles": (None, [_i64, _i64, _i32p, _i64, _i64, _i32p, _i32p]),
+            "hno_price_reduced_costs": (None, [_i64, _i64, _i64p, _i64p, _f64p, _f64p, _f64p, _f64p]),
+            "hno_price_devex_update": (None, [_i64, _i64, _i64p, _i64p, _f64p, _f64p, _i32p, _f64p, _f64p]),
+            "hno_price_ranked": (_i64, [_i64, _f64p, _f64p, _i32p, _u8p, C.c_int, C.c_int, C.c_double, _i64,
+                                        _i64p]),
+            "hno_price_bland": (_i64, [_i64, _f64p, _i32p, _u8p, C.c_int, C.c_int, C.c_double]),
+            "hno_extract_column": (None, [_i64, _i64p, _i64p, _f64p, _i64, _f64p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -99,6 +106,11 @@ def ref():
             "hnref_max_step": (C.c_double, [_i64, _f64p, _f64p]),
             "hnref_step_sample": (C.c_double, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, _f64p, _i64,
                                                C.c_int, C.c_int, _i64p, _i64p]),
+            "hnref_price_reduced_costs": (None, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, _f64p]),
+            "hnref_price_devex_update": (None, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _i32p, _f64p]),
+            "hnref_price_ranked": (_i64, [_i64, _f64p, _f64p, _i32p, _u8p, C.c_int, C.c_int, _i64, _i64p]),
+            "hnref_price_select": (_i64, [_i64, _f64p, _f64p, _i32p, _u8p, C.c_int, C.c_int, C.c_int]),
+            "hnref_price_edge_weight": (C.c_double, [_i64, _i64, _u64p, _u64p, _f64p, _i64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -335,3 +347,91 @@ def ref_step_sample(lp, x, lam, D, ncols_sample, threads, reps):
                                    _p(x, C.c_double), _p(lam, C.c_double), _p(D, C.c_double), int(ncols_sample),
                                    int(threads), int(reps), C.byref(trip), C.byref(nnzn))
     return secs, trip.value, nnzn.value
+
+
+# ---- revised-simplex pricing (core/lp/simplex.cpp) ----
+def price_reduced_costs(m, n, rp, ci, val, y, cost):
+    rp, ci = i64(rp), i64(ci)
+    rc = np.empty(n)
+    port().hno_price_reduced_costs(m, n, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(f64(val), C.c_double),
+                                   _p(f64(y), C.c_double), _p(f64(cost), C.c_double), _p(rc, C.c_double))
+    return rc
+
+
+def price_devex_update(m, n, rp, ci, val, u, nonbasis, weights):
+    """Returns (new weights, alpha = A^T u)."""
+    rp, ci = i64(rp), i64(ci)
+    w = np.array(weights, dtype=np.float64)
+    alpha = np.empty(n)
+    nb = np.ascontiguousarray(nonbasis, dtype=np.int32)
+    port().hno_price_devex_update(m, n, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(f64(val), C.c_double),
+                                  _p(f64(u), C.c_double), _p(nb, C.c_int32), _p(w, C.c_double),
+                                  _p(alpha, C.c_double))
+    return w, alpha
+
+
+def price_ranked(rc, w, nonbasis, artificial, phase1=False, maximize=False, tol=1e-9, cap=None):
+    n = len(rc)
+    cap = n if cap is None else cap
+    out = np.empty(max(cap, 1), dtype=np.int64)
+    nb = np.ascontiguousarray(nonbasis, dtype=np.int32)
+    art = np.ascontiguousarray(artificial, dtype=np.uint8)
+    cnt = port().hno_price_ranked(n, _p(f64(rc), C.c_double), _p(f64(w), C.c_double), _p(nb, C.c_int32),
+                                  _p(art, C.c_uint8), int(phase1), int(maximize), tol, cap,
+                                  _p(out, C.c_int64))
+    return cnt, out[:cap]
+
+
+def price_bland(rc, nonbasis, artificial, phase1=False, maximize=False, tol=1e-9):
+    nb = np.ascontiguousarray(nonbasis, dtype=np.int32)
+    art = np.ascontiguousarray(artificial, dtype=np.uint8)
+    return port().hno_price_bland(len(rc), _p(f64(rc), C.c_double), _p(nb, C.c_int32), _p(art, C.c_uint8),
+                                  int(phase1), int(maximize), tol)
+
+
+def extract_column(m, rp, ci, val, j):
+    rp, ci = i64(rp), i64(ci)
+    col = np.empty(m)
+    port().hno_extract_column(m, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(f64(val), C.c_double), j,
+                              _p(col, C.c_double))
+    return col
+
+
+def ref_price_reduced_costs(m, n, rp, ci, val, y, cost):
+    rc = np.empty(n)
+    ref().hnref_price_reduced_costs(m, n, _p(u64(rp), C.c_uint64), _p(u64(ci), C.c_uint64),
+                                    _p(f64(val), C.c_double), _p(f64(y), C.c_double), _p(f64(cost), C.c_double),
+                                    _p(rc, C.c_double))
+    return rc
+
+
+def ref_price_devex_update(m, n, rp, ci, val, u, nonbasis, weights):
+    w = np.array(weights, dtype=np.float64)
+    nb = np.ascontiguousarray(nonbasis, dtype=np.int32)
+    ref().hnref_price_devex_update(m, n, _p(u64(rp), C.c_uint64), _p(u64(ci), C.c_uint64),
+                                   _p(f64(val), C.c_double), _p(f64(u), C.c_double), _p(nb, C.c_int32),
+                                   _p(w, C.c_double))
+    return w
+
+
+def ref_price_ranked(rc, w, nonbasis, artificial, phase1=False, maximize=False, cap=None):
+    n = len(rc)
+    cap = n if cap is None else cap
+    out = np.empty(max(cap, 1), dtype=np.int64)
+    nb = np.ascontiguousarray(nonbasis, dtype=np.int32)
+    art = np.ascontiguousarray(artificial, dtype=np.uint8)
+    cnt = ref().hnref_price_ranked(n, _p(f64(rc), C.c_double), _p(f64(w), C.c_double), _p(nb, C.c_int32),
+                                   _p(art, C.c_uint8), int(phase1), int(maximize), cap, _p(out, C.c_int64))
+    return cnt, out[: min(cap, cnt)]
+
+
+def ref_price_select(rc, w, nonbasis, artificial, phase1=False, maximize=False, rule=1):
+    nb = np.ascontiguousarray(nonbasis, dtype=np.int32)
+    art = np.ascontiguousarray(artificial, dtype=np.uint8)
+    return ref().hnref_price_select(len(rc), _p(f64(rc), C.c_double), _p(f64(w), C.c_double), _p(nb, C.c_int32),
+                                    _p(art, C.c_uint8), int(phase1), int(maximize), rule)
+
+
+def ref_price_edge_weight(m, n, rp, ci, val, var):
+    return ref().hnref_price_edge_weight(m, n, _p(u64(rp), C.c_uint64), _p(u64(ci), C.c_uint64),
+                                         _p(f64(val), C.c_double), var)
