@@ -252,6 +252,8 @@ def run_ours(args, rank, world, local):
         }
         if not args.no_ipm:
             result["plain_ipm"] = plain_ipm()
+        if not args.no_batch:
+            result["batched_ipm"] = batched_ipm(args.batch_k)
         if not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(lp, vec, threads=os.cpu_count() or 1, reps=1)
     return result
@@ -278,6 +280,60 @@ def plain_ipm():
                             "ms": round(ref["time_ms"], 1), "rel_obj_diff": abs(r["objective"] - ref["objective"]) /
                             (1.0 + abs(ref["objective"]))}
     return out
+
+
+def batched_ipm(K: int, sample_per_stratum: int = 4):
+    """The 4096-LP batch (m log-uniform in [50, 2000], n = round(2.5 m),
+    6 nonzeros per column, seeds 20000+i) through the batched GPU IPM, and the
+    plain one-at-a-time GPU IPM on a seeded stratified sample of the same
+    instances (8 log-size strata), extrapolated to the batch. Wall-clock
+    times with the device synchronised on both sides; both include the
+    host->device copies of the LPs and the device->host copies of the
+    solutions."""
+    import torch
+
+    import hnb200 as hn
+    import lpgen
+
+    sizes = lpgen.batch_sizes(K, seed=2000)
+    lps = [lpgen.lp_uniform(int(m), int(round(2.5 * m)), 6, 20000 + i) for i, m in enumerate(sizes)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = hn.lp_solve_batch(lps)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    st = r["status"]
+    # stratified plain sample
+    edges = np.exp(np.linspace(np.log(50), np.log(2000) + 1e-9, 9))
+    rng = np.random.default_rng(7)
+    est, matched, sampled, plain_iters = 0.0, 0, 0, []
+    for a, b in zip(edges[:-1], edges[1:]):
+        idx = np.nonzero((sizes >= a) & (sizes < b))[0]
+        if idx.size == 0:
+            continue
+        pick = rng.choice(idx, size=min(sample_per_stratum, idx.size), replace=False)
+        times = []
+        for i in pick:
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            p = hn.lp_solve(lps[i])
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t1)
+            plain_iters.append(p["iterations"])
+            sampled += 1
+            rel = abs(p["objective"] - r["objective"][i]) / (1.0 + abs(p["objective"]))
+            matched += int(p["status"] == st[i] == 1 and rel <= 1e-8)
+        est += float(np.mean(times)) * idx.size
+    return {"workload": f"{K} LPs, m log-uniform [50,2000], n=2.5m, 6 nnz/col (seeds 20000+i)",
+            "rows": int(sizes.sum()), "batched_s": round(wall, 3), "batched_solves_per_s": round(K / wall, 1),
+            "optimal": int((st == 1).sum()), "iterations_max": int(r["stats"]["iterations"]),
+            "iterations_mean": round(float(r["iterations"].mean()), 2),
+            "factor_ms": round(r["stats"]["factor_ms"], 1), "solve_ms": round(r["stats"]["solve_ms"], 1),
+            "plain_gpu_s_extrapolated": round(est, 2), "plain_gpu_solves_per_s_extrapolated": round(K / est, 2),
+            "speedup_vs_plain_gpu": round(est / wall, 2),
+            "plain_sample": {"instances": sampled, "per_stratum": sample_per_stratum,
+                             "matching_status_and_objective_1e-8": matched,
+                             "iterations_mean": round(float(np.mean(plain_iters)), 2)}}
 
 
 def run_only(args, local):
@@ -381,6 +437,8 @@ def main():
                     help="time one kernel group alone (for profiling); 'step' is the measured workload")
     ap.add_argument("--no-ipm", action="store_true", help="skip the plain GPU IPM solve on the m=2000 LP")
     ap.add_argument("--scale", type=int, default=1, help="--only modes: shrink the LP by this factor (profiling)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-IPM key")
+    ap.add_argument("--batch-k", type=int, default=4096, help="instances in the batched-IPM key")
     args = ap.parse_args()
     rank, world, local = dist_setup()
     if args.impl == "reference":

@@ -38,7 +38,7 @@ constexpr int kT = 256;
 constexpr int64_t kMaxBitmapWords = 12500;  // row reach <= 400,000 columns: four W-word arrays in 200 KB of shared memory
 constexpr uint32_t kMulti = 0x80000000u;
 constexpr int64_t kDiagFlag = int64_t(1) << 62;
-constexpr int kSlotsPerThread = 8;  // slots per thread per trip of the numeric kernel
+constexpr int kSlotsPerThread = 4;  // slots per thread per trip of the numeric kernel
 
 __device__ __forceinline__ uint32_t bit_of(int k) { return 1u << (k & 31); }
 
@@ -271,36 +271,86 @@ __device__ __forceinline__ double term(uint2 pe, const double2* __restrict__ vd,
     return (q.y <= 0.0) ? 0.0 : (q.x * __ldg(valT + pe.x)) * q.y;  // columns with D_j <= 0 skipped
 }
 
-__global__ void __launch_bounds__(kT) ada_slot_kernel(int64_t nnz, const uint2* __restrict__ gmap,
-                                                      const double2* __restrict__ vd,
-                                                      const double* __restrict__ valT, double* __restrict__ nval) {
+// Numeric phase, two kernels per call:
+//   ada_combine_kernel sums every multi slot's terms in column order (the
+//     order from_triplets' stable sort leaves them in) into the compact mval;
+//   ada_slot_kernel then writes every slot of N once, in slot order: a single
+//     term (A value x A^T value) x d, or the multi slot's mval entry.
+// In the slot kernel each thread handles kSlotsPerThread slots per trip; all
+// gathers of a trip are issued before any use (a multi slot reads mval and
+// gathers entry 0, which always exists), and the next trip's map entries are
+// loaded before this trip's gathers, so the map stream from HBM overlaps the
+// gathers from L2.
+__global__ void __launch_bounds__(kT, 4) ada_slot_kernel(int64_t nnz, const uint2* __restrict__ gmap,
+                                                         const double2* __restrict__ vd,
+                                                         const double* __restrict__ valT,
+                                                         const double* __restrict__ mval, double* __restrict__ nval) {
     const int64_t stride = (int64_t)gridDim.x * kT * kSlotsPerThread;
-    for (int64_t t0 = blockIdx.x * (int64_t)kT * kSlotsPerThread + threadIdx.x; t0 < nnz; t0 += stride) {
-        uint2 g[kSlotsPerThread];
+    int64_t t0 = blockIdx.x * (int64_t)kT * kSlotsPerThread + threadIdx.x;
+    uint2 g[kSlotsPerThread];
+#pragma unroll
+    for (int u = 0; u < kSlotsPerThread; ++u) {
+        const int64_t t = t0 + (int64_t)u * kT;
+        g[u] = t < nnz ? __ldcs(gmap + t) : make_uint2(kMulti, 0u);
+    }
+    for (; t0 < nnz; t0 += stride) {
+        uint2 gn[kSlotsPerThread];
 #pragma unroll
         for (int u = 0; u < kSlotsPerThread; ++u) {
+            const int64_t t = t0 + stride + (int64_t)u * kT;
+            gn[u] = t < nnz ? __ldcs(gmap + t) : make_uint2(kMulti, 0u);
+        }
+        double2 q[kSlotsPerThread];
+        double b[kSlotsPerThread];
+#pragma unroll
+        for (int u = 0; u < kSlotsPerThread; ++u) {
+            const bool multi = g[u].x & kMulti;
             const int64_t t = t0 + (int64_t)u * kT;
-            g[u] = t < nnz ? __ldcs(gmap + t) : make_uint2(kMulti, 0u);
+            q[u] = __ldg(vd + (multi ? 0u : g[u].y));
+            b[u] = (multi && t < nnz) ? __ldcs(mval + (g[u].x & ~kMulti)) : __ldg(valT + (multi ? 0u : g[u].x));
         }
 #pragma unroll
         for (int u = 0; u < kSlotsPerThread; ++u) {
             const int64_t t = t0 + (int64_t)u * kT;
-            if (!(g[u].x & kMulti)) __stcs(nval + t, term(g[u], vd, valT));
+            if (t >= nnz) continue;
+            const double v = (g[u].x & kMulti) ? b[u]
+                             : (q[u].y <= 0.0) ? 0.0  // columns with D_j <= 0 skipped
+                                               : (q[u].x * b[u]) * q[u].y;
+            __stcs(nval + t, v);
         }
+#pragma unroll
+        for (int u = 0; u < kSlotsPerThread; ++u) g[u] = gn[u];
     }
 }
 
+// The first kBatch terms of a slot are gathered together; longer lists
+// continue one term at a time.
+constexpr int kBatch = 4;
 __global__ void ada_combine_kernel(int64_t nms, const int64_t* __restrict__ mpos, const int32_t* __restrict__ mbeg,
                                    const uint2* __restrict__ mlist, const double2* __restrict__ vd,
-                                   const double* __restrict__ valT, double* __restrict__ nval,
+                                   const double* __restrict__ valT, double* __restrict__ mval,
                                    unsigned long long* maxdiag) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= nms) return;
+    const int32_t u0 = mbeg[t], u1 = mbeg[t + 1];
+    uint2 pe[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) pe[k] = (u0 + k < u1) ? __ldg(mlist + u0 + k) : make_uint2(0u, 0u);
+    double2 q[kBatch];
+    double b[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+        q[k] = __ldg(vd + pe[k].y);
+        b[k] = __ldg(valT + pe[k].x);
+    }
     double s = 0.0;
-    for (int32_t u = mbeg[t]; u < mbeg[t + 1]; ++u) s += term(mlist[u], vd, valT);
-    const int64_t mp = mpos[t];
-    nval[mp & ~kDiagFlag] = s;
-    if ((mp & kDiagFlag) && s > 0.0) atomicMax(maxdiag, static_cast<unsigned long long>(__double_as_longlong(s)));
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k)
+        if (u0 + k < u1) s += (q[k].y <= 0.0) ? 0.0 : (q[k].x * b[k]) * q[k].y;
+    for (int32_t u = u0 + kBatch; u < u1; ++u) s += term(mlist[u], vd, valT);
+    mval[t] = s;
+    if ((mpos[t] & kDiagFlag) && s > 0.0)
+        atomicMax(maxdiag, static_cast<unsigned long long>(__double_as_longlong(s)));
 }
 
 __global__ void ada_reg_kernel(int m, const int64_t* __restrict__ diag_pos, double reg,
@@ -317,7 +367,7 @@ __global__ void ada_reg_kernel(int m, const int64_t* __restrict__ diag_pos, doub
 void free_pattern(hn_pattern* P) {
     if (!P) return;
     for (void* p : {(void*)P->rp, (void*)P->ci, (void*)P->diag_pos, (void*)P->maxdiag, (void*)P->gmap,
-                    (void*)P->mpos, (void*)P->mbeg, (void*)P->mlist, (void*)P->vd})
+                    (void*)P->mpos, (void*)P->mbeg, (void*)P->mlist, (void*)P->vd, (void*)P->mval})
         dfree(p);
     delete P;
 }
@@ -331,22 +381,22 @@ int64_t d2h_i64(const int64_t* p, cudaStream_t s) {
 
 void launch_numeric(const hn_pattern* P, const double* d, double* nval, cudaStream_t s) {
     const hn_csr* A = P->A;
-    const int64_t per_block = (int64_t)kT * kSlotsPerThread;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P->nnz + per_block - 1) / per_block,
-                                                                 (int64_t)ctx().sm_count * 16));
     if (A->nnz > 0) {
         const int gv = (int)std::min<int64_t>((A->nnz + kT - 1) / kT, (int64_t)ctx().sm_count * 16);
         ada_vd_kernel<<<gv, kT, 0, s>>>(A->nnz, A->val, A->ci, d, P->vd);
         launched("ada_vd_kernel");
     }
-    ada_slot_kernel<<<grid, kT, 0, s>>>(P->nnz, P->gmap, P->vd, A->valT, nval);
-    launched("ada_slot_kernel");
     check_cuda(cudaMemsetAsync(P->maxdiag, 0, sizeof(unsigned long long), s), "memset maxdiag");
     if (P->nms > 0) {
         ada_combine_kernel<<<(unsigned)((P->nms + 255) / 256), 256, 0, s>>>(P->nms, P->mpos, P->mbeg, P->mlist,
-                                                                            P->vd, A->valT, nval, P->maxdiag);
+                                                                            P->vd, A->valT, P->mval, P->maxdiag);
         launched("ada_combine_kernel");
     }
+    const int64_t per_block = (int64_t)kT * kSlotsPerThread;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P->nnz + per_block - 1) / per_block,
+                                                                 (int64_t)ctx().sm_count * 4));
+    ada_slot_kernel<<<grid, kT, 0, s>>>(P->nnz, P->gmap, P->vd, A->valT, P->mval, nval);
+    launched("ada_slot_kernel");
 }
 
 }  // namespace
@@ -431,6 +481,7 @@ int hn_ada_symbolic(const hn_csr* A, hn_pattern** out) {
             P->ci = dmalloc<int32_t>(P->nnz);
             P->gmap = dmalloc<uint2>(P->nnz);
             P->mpos = dmalloc<int64_t>(P->nms);
+            P->mval = dmalloc<double>(P->nms);
             P->mbeg = dmalloc<int32_t>(P->nms + 1);
             P->mlist = dmalloc<uint2>(P->nmq);
             mcnt = dmalloc<int32_t>(P->nms);

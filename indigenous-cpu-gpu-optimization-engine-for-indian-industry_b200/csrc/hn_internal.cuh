@@ -319,4 +319,5 @@ struct hn_pattern {
     int64_t nmq = 0;                 // terms into those slots
     uint2* mlist = nullptr;          // nmq
     double2* vd = nullptr;           // nnz(A): (A value, d of its column), per numeric call
+    double* mval = nullptr;          // nms: sums of the multi slots, per numeric call
 };
