@@ -153,6 +153,16 @@ int hn_nrm2(int64_t n, const double* v_dev, double* result_dev, void* stream);
  * (the span from its smallest to its largest k; block-diagonal batches are
  * limited by their largest block only), and nnz(N) < 2^31. */
 int hn_ada_symbolic(const hn_csr* A, hn_pattern** out);
+/* The numeric phase has two layouts with bit-identical results. Gather
+ * mode (the default) keeps an 8-byte source pair per slot of N and is the
+ * faster one. Row mode, asked for with HN_ADA_COMPACT and used when every row
+ * of N has <= 65,534 slots and every row of A <= 256 entries, keeps a 2-byte
+ * slot offset per term (about a quarter of the memory) and assembles each
+ * row of N in shared-memory windows. */
+#define HN_ADA_COMPACT 1u
+int hn_ada_symbolic_ex(const hn_csr* A, unsigned flags, hn_pattern** out);
+/* row_mode: 1 for row mode, 0 for gather mode; max_row: longest row of N. */
+int hn_pattern_mode(const hn_pattern* P, int* row_mode, int64_t* max_row);
 int hn_pattern_info(const hn_pattern* P, int64_t* m, int64_t* nnz);
 /* Host copy of the pattern: rp m+1, ci nnz (reference layout). */
 int hn_pattern_export(const hn_pattern* P, uint64_t* rp_host, uint64_t* ci_host);

@@ -39,6 +39,11 @@ constexpr int64_t kMaxBitmapWords = 12500;  // row reach <= 400,000 columns: fou
 constexpr uint32_t kMulti = 0x80000000u;
 constexpr int64_t kDiagFlag = int64_t(1) << 62;
 constexpr int kSlotsPerThread = 4;  // slots per thread per trip of the numeric kernel
+constexpr uint16_t kSlotMulti = 0xFFFFu;
+constexpr int kRowThreads = 256;     // row-mode numeric kernel
+constexpr int kRowWindow = 4096;     // row mode: slots of a row of N assembled per pass (32 KB)
+constexpr int kRowMaxSlots = 65534;  // row mode: slot offsets fit 16 bits
+constexpr int kRowMaxEntries = 256;  // row mode: entries of a row of A staged in shared memory
 
 __device__ __forceinline__ uint32_t bit_of(int k) { return 1u << (k & 31); }
 
@@ -107,7 +112,8 @@ __global__ void __launch_bounds__(kT) ada_count_kernel(int m, const int32_t* __r
                                                        const int32_t* __restrict__ wbase,
                                                        const int32_t* __restrict__ wcount,
                                                        int64_t* __restrict__ len, int64_t* __restrict__ nq,
-                                                       int64_t* __restrict__ nms, int64_t* __restrict__ nmq) {
+                                                       int64_t* __restrict__ nms, int64_t* __restrict__ nmq,
+                                                       unsigned* __restrict__ maxes) {
     extern __shared__ uint32_t smem[];
     uint32_t* b1 = smem;
     uint32_t* b2 = smem + Wmax;
@@ -137,6 +143,8 @@ __global__ void __launch_bounds__(kT) ada_count_kernel(int m, const int32_t* __r
             nq[i] = q;
             nms[i] = MS;
             nmq[i] = q - D1;
+            atomicMax(maxes + 1, (unsigned)L);
+            atomicMax(maxes + 2, (unsigned)(rp[i + 1] - rp[i]));
         }
         __syncthreads();
     }
@@ -152,7 +160,7 @@ __global__ void __launch_bounds__(kT) ada_fill_kernel(
     const int32_t* __restrict__ wcount, const int64_t* __restrict__ rpN, const int64_t* __restrict__ msrow,
     const int64_t* __restrict__ mqrow, int32_t* __restrict__ ciN, int64_t* __restrict__ diag_pos,
     int64_t* __restrict__ mpos, int32_t* mcnt, int32_t* __restrict__ mbeg, uint2* __restrict__ gmap,
-    uint2* __restrict__ mlist) {
+    uint2* __restrict__ mlist, const int64_t* __restrict__ tq, uint16_t* __restrict__ smap) {
     extern __shared__ uint32_t smem[];
     uint32_t* b1 = smem;
     uint32_t* b2 = smem + Wmax;
@@ -196,7 +204,7 @@ __global__ void __launch_bounds__(kT) ada_fill_kernel(
                 if ((bits2 >> b) & 1u) {
                     mpos[ms0 + o2] = pos | (k == i ? kDiagFlag : 0);
                     mcnt[ms0 + o2] = 0;
-                    gmap[pos] = make_uint2(kMulti | static_cast<uint32_t>(ms0 + o2), 0u);
+                    if (gmap) gmap[pos] = make_uint2(kMulti | static_cast<uint32_t>(ms0 + o2), 0u);
                     ++o2;
                 }
                 ++o1;
@@ -234,8 +242,9 @@ __global__ void __launch_bounds__(kT) ada_fill_kernel(
             }
         }
         __syncthreads();
-        // gather map; entries e go one after the other so the terms of each
-        // multi slot are listed in column order
+        // gather map (or slot map); entries e go one after the other so the
+        // terms of each multi slot are listed in column order
+        int64_t tloc = smap ? tq[i] : 0;
         for (int e = rp[i]; e < rp[i + 1]; ++e) {
             if (val[e] == 0.0) continue;
             const int j = ci[e];
@@ -243,14 +252,17 @@ __global__ void __launch_bounds__(kT) ada_fill_kernel(
             for (int p = cs + threadIdx.x; p < ce; p += kT) {
                 const int k = ciT[p];
                 const uint2 pe = make_uint2(static_cast<uint32_t>(p), static_cast<uint32_t>(e));
-                if (b2[(k >> 5) - wb] & bit_of(k)) {
+                const bool multi = b2[(k >> 5) - wb] & bit_of(k);
+                if (multi) {
                     const int64_t ms = ms0 + rank_of(b2, pre2, k, wb);
                     const int ord = atomicAdd(&mcnt[ms], 1);
                     mlist[mbeg[ms] + ord] = pe;
-                } else {
+                } else if (gmap) {
                     gmap[row0 + rank_of(b1, pre1, k, wb)] = pe;
                 }
+                if (smap) smap[tloc + (p - cs)] = multi ? kSlotMulti : static_cast<uint16_t>(rank_of(b1, pre1, k, wb));
             }
+            tloc += ce - cs;
             __syncthreads();
         }
         __syncthreads();
@@ -353,6 +365,97 @@ __global__ void ada_combine_kernel(int64_t nms, const int64_t* __restrict__ mpos
         atomicMax(maxdiag, static_cast<unsigned long long>(__double_as_longlong(s)));
 }
 
+// Row mode: one CTA per row of N at a time, in windows of kRowWindow slots.
+// The row's A entries (value, d, A^T row start, term offset) are staged in
+// shared memory; the row's terms (e, p) are cut into chunks of 8 -- one
+// 16-byte load of the slot map (each row's terms start on a 16-byte
+// boundary) -- and each thread walks its chunk, moving to the next entry as
+// the term offsets pass. A single-slot term in the current window writes
+// (A value x A^T value) x d into the shared window at its slot offset, the
+// window's multi slots take their combined sums from mval, and the window
+// leaves in one coalesced streaming store; a row longer than the window
+// walks its terms once per window. The arithmetic of each slot is the slot
+// kernel's, so both modes give the same bits.
+__global__ void __launch_bounds__(kRowThreads) ada_row_kernel(
+    int m, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double2* __restrict__ vd,
+    const int32_t* __restrict__ rpT, const double* __restrict__ valT, const int64_t* __restrict__ tq,
+    const uint16_t* __restrict__ smap, const int64_t* __restrict__ rpN, const int64_t* __restrict__ msrow,
+    const int64_t* __restrict__ mpos, const double* __restrict__ mval, double* __restrict__ nval) {
+    __shared__ double srow[kRowWindow];
+    __shared__ double2 s_vd[kRowMaxEntries];
+    __shared__ int32_t s_cs[kRowMaxEntries];
+    __shared__ int32_t s_to[kRowMaxEntries + 1];
+    __shared__ int64_t sh[32];
+    const int tid = threadIdx.x;
+    for (int i = blockIdx.x; i < m; i += gridDim.x) {
+        const int e0 = rp[i], ne = rp[i + 1] - e0;
+        // term counts per entry (0 for an explicit zero of A), exclusive scan
+        int64_t cnt = 0;
+        if (tid < ne) {
+            const double2 q = vd[e0 + tid];
+            const int j = ci[e0 + tid];
+            const int cs = rpT[j];
+            s_vd[tid] = q;
+            s_cs[tid] = cs;
+            cnt = (q.x == 0.0) ? 0 : rpT[j + 1] - cs;
+        }
+        int64_t tot;
+        const int64_t ex = block_exclusive_scan_i64<kRowThreads>(cnt, sh, &tot);
+        if (tid < ne) s_to[tid] = static_cast<int32_t>(ex);
+        if (tid == 0) s_to[ne] = static_cast<int32_t>(tot);
+        __syncthreads();
+        const int T = static_cast<int>(tot);
+        const uint4* sm = reinterpret_cast<const uint4*>(smap + tq[i]);
+        const int nch = (T + 7) >> 3;
+        const int64_t r0 = rpN[i];
+        const int L = static_cast<int>(rpN[i + 1] - r0);
+        const int64_t ms0 = msrow[i], ms1 = msrow[i + 1];
+        for (int w0 = 0; w0 < L; w0 += kRowWindow) {
+            const int w1 = min(L, w0 + kRowWindow);
+            for (int c = tid; c < nch; c += kRowThreads) {
+                const uint4 raw = __ldcs(sm + c);
+                const uint32_t w[4] = {raw.x, raw.y, raw.z, raw.w};
+                const int t0 = c << 3;
+                int lo = 0, hi = ne - 1;  // entry of term t0: last e with s_to[e] <= t0
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_to[mid] <= t0)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                int e = lo, next = s_to[lo + 1];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int t = t0 + u;
+                    if (t < T) {
+                        while (t >= next) next = s_to[++e + 1];
+                        const int slot = static_cast<int>((w[u >> 1] >> ((u & 1) * 16)) & 0xFFFFu);
+                        if (slot != kSlotMulti && slot >= w0 && slot < w1) {
+                            const double2 q = s_vd[e];
+                            const double b = __ldg(valT + s_cs[e] + (t - s_to[e]));
+                            srow[slot - w0] = (q.y <= 0.0) ? 0.0 : (q.x * b) * q.y;  // columns with D_j <= 0 skipped
+                        }
+                    }
+                }
+            }
+            for (int64_t ms = ms0 + tid; ms < ms1; ms += kRowThreads) {
+                const int64_t k = (mpos[ms] & ~kDiagFlag) - r0;
+                if (k >= w0 && k < w1) srow[k - w0] = __ldcs(mval + ms);
+            }
+            __syncthreads();
+            for (int k = w0 + tid; k < w1; k += kRowThreads) __stcs(nval + r0 + k, srow[k - w0]);
+            __syncthreads();
+        }
+    }
+}
+
+// term counts of a row rounded up to whole 16-byte chunks of the slot map
+__global__ void pad8_kernel(int64_t m, const int64_t* __restrict__ nq, int64_t* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < m) out[i] = (nq[i] + 7) & ~int64_t(7);
+}
+
 __global__ void ada_reg_kernel(int m, const int64_t* __restrict__ diag_pos, double reg,
                                const unsigned long long* __restrict__ maxdiag, double* __restrict__ nval,
                                double* dyn_out) {
@@ -367,7 +470,8 @@ __global__ void ada_reg_kernel(int m, const int64_t* __restrict__ diag_pos, doub
 void free_pattern(hn_pattern* P) {
     if (!P) return;
     for (void* p : {(void*)P->rp, (void*)P->ci, (void*)P->diag_pos, (void*)P->maxdiag, (void*)P->gmap,
-                    (void*)P->mpos, (void*)P->mbeg, (void*)P->mlist, (void*)P->vd, (void*)P->mval})
+                    (void*)P->mpos, (void*)P->mbeg, (void*)P->mlist, (void*)P->vd, (void*)P->mval, (void*)P->tq,
+                    (void*)P->smap, (void*)P->msrow})
         dfree(p);
     delete P;
 }
@@ -392,6 +496,13 @@ void launch_numeric(const hn_pattern* P, const double* d, double* nval, cudaStre
                                                                             P->vd, A->valT, P->mval, P->maxdiag);
         launched("ada_combine_kernel");
     }
+    if (P->row_mode) {
+        const int grid = (int)std::min<int64_t>(P->m, (int64_t)ctx().sm_count * 5);
+        ada_row_kernel<<<grid, kRowThreads, 0, s>>>((int)P->m, A->rp, A->ci, P->vd, A->rpT, A->valT, P->tq,
+                                                       P->smap, P->rp, P->msrow, P->mpos, P->mval, nval);
+        launched("ada_row_kernel");
+        return;
+    }
     const int64_t per_block = (int64_t)kT * kSlotsPerThread;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P->nnz + per_block - 1) / per_block,
                                                                  (int64_t)ctx().sm_count * 4));
@@ -412,7 +523,17 @@ using namespace hn;
 
 extern "C" {
 
-int hn_ada_symbolic(const hn_csr* A, hn_pattern** out) {
+int hn_ada_symbolic(const hn_csr* A, hn_pattern** out) { return hn_ada_symbolic_ex(A, 0u, out); }
+
+int hn_pattern_mode(const hn_pattern* P, int* row_mode, int64_t* max_row) {
+    return guard("hn_pattern_mode", [&] {
+        if (!P) fail(HN_ERR_INVALID_ARG, "null pattern");
+        if (row_mode) *row_mode = P->row_mode ? 1 : 0;
+        if (max_row) *max_row = P->max_row;
+    });
+}
+
+int hn_ada_symbolic_ex(const hn_csr* A, unsigned flags, hn_pattern** out) {
     return guard("hn_ada_symbolic", [&] {
         require_init();
         if (!A || !out) fail(HN_ERR_INVALID_ARG, "bad arguments");
@@ -421,15 +542,15 @@ int hn_ada_symbolic(const hn_csr* A, hn_pattern** out) {
         const int64_t m = A->m;
         hn_pattern* P = new hn_pattern();
         cudaStream_t s = nullptr;
-        int64_t *nq = nullptr, *nms = nullptr, *nmq = nullptr;
+        int64_t *nq = nullptr, *nms = nullptr, *nmq = nullptr, *tqa = nullptr;
         int32_t *mcnt = nullptr, *wbase = nullptr, *wcount = nullptr;
         unsigned* wmax_d = nullptr;
         try {
             // row reaches -> bitmap width
             wbase = dmalloc<int32_t>(m);
             wcount = dmalloc<int32_t>(m);
-            wmax_d = dmalloc<unsigned>(1);
-            check_cuda(cudaMemsetAsync(wmax_d, 0, sizeof(unsigned), s), "memset");
+            wmax_d = dmalloc<unsigned>(3);  // widest bitmap, longest row of N, longest row of A
+            check_cuda(cudaMemsetAsync(wmax_d, 0, 3 * sizeof(unsigned), s), "memset");
             if (m > 0) {
                 ada_window_kernel<<<(unsigned)((m * 32 + 255) / 256), 256, 0, s>>>((int)m, A->rp, A->ci, A->val,
                                                                                   A->rpT, A->ciT, wbase, wcount,
@@ -465,9 +586,16 @@ int hn_ada_symbolic(const hn_csr* A, hn_pattern** out) {
             const int grid = (int)std::min<int64_t>(std::max<int64_t>(m, 1), (int64_t)ctx().sm_count * 8);
             if (m > 0) {
                 ada_count_kernel<<<grid, kT, smem_count, s>>>((int)m, A->rp, A->ci, A->val, A->rpT, A->ciT, (int)W,
-                                                              wbase, wcount, P->rp, nq, nms, nmq);
+                                                              wbase, wcount, P->rp, nq, nms, nmq, wmax_d);
                 launched("ada_count_kernel");
             }
+            tqa = dmalloc<int64_t>(m + 1);
+            check_cuda(cudaMemsetAsync(tqa, 0, sizeof(int64_t) * (m + 1), s), "memset");
+            if (m > 0) {
+                pad8_kernel<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(m, nq, tqa);
+                launched("pad8_kernel");
+            }
+            scan_exclusive_i64(tqa, tqa, m + 1, s);
             scan_exclusive_i64(P->rp, P->rp, m + 1, s);
             scan_exclusive_i64(nq, nq, m + 1, s);
             scan_exclusive_i64(nms, nms, m + 1, s);
@@ -478,8 +606,22 @@ int hn_ada_symbolic(const hn_csr* A, hn_pattern** out) {
             P->nmq = d2h_i64(nmq + m, s);
             if (P->nnz >= (int64_t(1) << 31) || P->nmq >= (int64_t(1) << 31))
                 fail(HN_ERR_UNSUPPORTED, "nnz(N) = " + std::to_string(P->nnz) + " exceeds the 2^31 slot limit");
+            unsigned maxes[3] = {0, 0, 0};
+            check_cuda(cudaMemcpyAsync(maxes, wmax_d, sizeof(maxes), cudaMemcpyDeviceToHost, s), "D2H");
+            check_cuda(cudaStreamSynchronize(s), "count sync");
+            P->max_row = static_cast<int32_t>(maxes[1]);
+            P->row_mode = (flags & HN_ADA_COMPACT) && m > 0 && maxes[1] <= (unsigned)kRowMaxSlots &&
+                          maxes[1] < kSlotMulti &&
+                          maxes[2] <= (unsigned)kRowMaxEntries && P->nq < (int64_t(1) << 31);
             P->ci = dmalloc<int32_t>(P->nnz);
-            P->gmap = dmalloc<uint2>(P->nnz);
+            if (P->row_mode) {
+                P->smap = dmalloc<uint16_t>(d2h_i64(tqa + m, s));
+                P->tq = tqa;
+                P->msrow = nms;
+                tqa = nms = nullptr;  // owned by the pattern now
+            } else {
+                P->gmap = dmalloc<uint2>(P->nnz);
+            }
             P->mpos = dmalloc<int64_t>(P->nms);
             P->mval = dmalloc<double>(P->nms);
             P->mbeg = dmalloc<int32_t>(P->nms + 1);
@@ -489,19 +631,21 @@ int hn_ada_symbolic(const hn_csr* A, hn_pattern** out) {
             check_cuda(cudaMemcpyAsync(P->mbeg + P->nms, &last, sizeof(last), cudaMemcpyHostToDevice, s), "H2D");
             if (m > 0) {
                 ada_fill_kernel<<<grid, kT, smem_fill, s>>>((int)m, A->rp, A->ci, A->val, A->rpT, A->ciT, (int)W,
-                                                            wbase, wcount, P->rp, nms, nmq, P->ci, P->diag_pos,
-                                                            P->mpos, mcnt, P->mbeg, P->gmap, P->mlist);
+                                                            wbase, wcount, P->rp, P->row_mode ? P->msrow : nms, nmq,
+                                                            P->ci, P->diag_pos, P->mpos, mcnt, P->mbeg, P->gmap,
+                                                            P->mlist, P->tq, P->smap);
                 launched("ada_fill_kernel");
             }
             check_cuda(cudaStreamSynchronize(s), "symbolic sync");
         } catch (...) {
             for (void* p : {(void*)nq, (void*)nms, (void*)nmq, (void*)mcnt, (void*)wbase, (void*)wcount,
-                            (void*)wmax_d})
+                            (void*)wmax_d, (void*)tqa})
                 dfree(p);
             free_pattern(P);
             throw;
         }
-        for (void* p : {(void*)nq, (void*)nms, (void*)nmq, (void*)mcnt, (void*)wbase, (void*)wcount, (void*)wmax_d})
+        for (void* p : {(void*)nq, (void*)nms, (void*)nmq, (void*)mcnt, (void*)wbase, (void*)wcount, (void*)wmax_d,
+                        (void*)tqa})
             dfree(p);
         *out = P;
     });

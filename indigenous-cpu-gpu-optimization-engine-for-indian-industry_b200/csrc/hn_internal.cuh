@@ -320,4 +320,13 @@ struct hn_pattern {
     uint2* mlist = nullptr;          // nmq
     double2* vd = nullptr;           // nnz(A): (A value, d of its column), per numeric call
     double* mval = nullptr;          // nms: sums of the multi slots, per numeric call
+    // row mode (every row of N fits in shared memory): instead of gmap, the
+    // terms of row i in enumeration order (A entries e of row i with a
+    // nonzero value, then the entries p of A^T row ci[e]) carry their slot
+    // offset within the row, or kSlotMulti for a term of a multi slot
+    bool row_mode = false;
+    int32_t max_row = 0;             // longest row of N (slots)
+    int64_t* tq = nullptr;           // m+1: term offsets per row
+    uint16_t* smap = nullptr;        // nq
+    int64_t* msrow = nullptr;        // m+1: multi-slot offsets per row
 };

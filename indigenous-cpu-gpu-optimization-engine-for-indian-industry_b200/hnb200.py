@@ -74,6 +74,8 @@ SIGNATURES = {
     "hn_nrm_inf": [_i64, _vp, _vp, _vp],
     "hn_nrm2": [_i64, _vp, _vp, _vp],
     "hn_ada_symbolic": [_vp, C.POINTER(_vp)],
+    "hn_ada_symbolic_ex": [_vp, C.c_uint, C.POINTER(_vp)],
+    "hn_pattern_mode": [_vp, C.POINTER(C.c_int), _i64p],
     "hn_pattern_info": [_vp, _i64p, _i64p],
     "hn_pattern_export": [_vp, _u64p, _u64p],
     "hn_pattern_device": [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)],
@@ -247,14 +249,20 @@ class Csr:
 class Pattern:
     """Fixed pattern of A diag(d) A^T + reg I (hn_pattern)."""
 
-    def __init__(self, A: Csr):
+    def __init__(self, A: Csr, compact: bool = False):
         h = C.c_void_p()
-        check(load().hn_ada_symbolic(A.h, C.byref(h)))
+        check(load().hn_ada_symbolic_ex(A.h, 1 if compact else 0, C.byref(h)))
         self.h = h
         self.A = A
         m, nnz = C.c_int64(), C.c_int64()
         check(load().hn_pattern_info(h, C.byref(m), C.byref(nnz)))
         self.m, self.nnz = m.value, nnz.value
+
+    def mode(self):
+        """(row_mode, longest row of N)."""
+        rm, mr = C.c_int(), C.c_int64()
+        check(load().hn_pattern_mode(self.h, C.byref(rm), C.byref(mr)))
+        return bool(rm.value), mr.value
 
     def export(self):
         rp = np.empty(self.m + 1, dtype=np.uint64)

@@ -19,9 +19,9 @@ pytestmark = pytest.mark.gpu
 GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_golden.npz"))
 
 
-def assemble(hn, torch, lp, D, reg=1e-8):
+def assemble(hn, torch, lp, D, reg=1e-8, compact=False):
     A = hn.Csr(lp["m"], lp["n"], lp["rp"], lp["ci"], lp["val"])
-    P = hn.Pattern(A)
+    P = hn.Pattern(A, compact=compact)
     nval = torch.empty(P.nnz, dtype=torch.float64, device="cuda")
     dyn = torch.empty(1, dtype=torch.float64, device="cuda")
     Dd = torch.as_tensor(D, device="cuda")
@@ -128,3 +128,45 @@ def test_large_zipf_pattern_properties(hn, torch_cuda):
     row_cnt = torch.diff(rp)
     col_cnt = torch.bincount(ci, minlength=m)
     assert torch.equal(row_cnt, col_cnt)
+
+
+@pytest.mark.parametrize("shape", [(2000, 5000, 8, 0), (529, 1322, 6, 7)])
+def test_row_and_gather_modes_bit_identical(hn, torch_cuda, shape):
+    """The two numeric layouts give the same bits (gather mode is the
+    default; row mode is asked for)."""
+    m, n, k, seed = shape
+    lp = lpgen.scaled_problem(lpgen.lp_uniform(m, n, k, seed))
+    D = np.random.default_rng(seed).uniform(1e-3, 1e3, n)
+    D[::17] = 0.0  # inactive columns
+    A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
+    Dd = torch_cuda.as_tensor(D, device="cuda")
+    out = []
+    for compact in (True, False):
+        P = hn.Pattern(A, compact=compact)
+        assert P.mode()[0] == compact
+        nval = torch_cuda.empty(P.nnz, dtype=torch_cuda.float64, device="cuda")
+        dyn = torch_cuda.empty(1, dtype=torch_cuda.float64, device="cuda")
+        P.numeric(Dd, 1e-8, nval, dyn)
+        torch_cuda.cuda.synchronize()
+        out.append((P.export(), nval.cpu().numpy(), dyn.item()))
+    (p0, v0, d0), (p1, v1, d1) = out
+    assert np.array_equal(p0[0], p1[0]) and np.array_equal(p0[1], p1[1])
+    assert np.array_equal(v0, v1) and d0 == d1
+
+
+def test_long_row_of_a_selects_gather_mode(hn, torch_cuda):
+    """A row of A with more than 256 entries: gather mode even when row mode
+    is asked for, values still match build_normal_equations."""
+    m, n = 300, 1500
+    lp = lpgen.scaled_problem(lpgen.lp_uniform(m, n, 4, 21))
+    rows = [lp["ci"][lp["rp"][i]:lp["rp"][i + 1]] for i in range(m)]
+    vals = [lp["val"][lp["rp"][i]:lp["rp"][i + 1]] for i in range(m)]
+    dense = np.arange(0, n, 2)  # 750 entries in row 0
+    rows[0] = dense
+    vals[0] = np.random.default_rng(2).uniform(0.1, 1.0, dense.size)
+    rp = np.concatenate([[0], np.cumsum([r.size for r in rows])]).astype(np.int64)
+    lp2 = dict(lp, rp=rp, ci=np.concatenate(rows).astype(np.int64), val=np.concatenate(vals))
+    D = np.random.default_rng(5).uniform(0.1, 10, n)
+    A, P, rp_, ci_, vals_, dyn = assemble(hn, torch_cuda, lp2, D, compact=True)
+    assert P.mode()[0] is False
+    check_values(lp2, D, 1e-8, rp_, ci_, vals_, dyn)
