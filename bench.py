@@ -108,6 +108,21 @@ def make_inputs(seed: int, scale: int = 1):
     return lp, vec
 
 
+PROFILE_TRAFFIC = {"ada_numeric": "profiles/ada_numeric_c1-5m.md"}
+
+
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from its committed ncu summary (the
+    `traffic_per_launch_bytes:` line), or None."""
+    rel = PROFILE_TRAFFIC.get(kernel)
+    if not rel or not os.path.exists(os.path.join(ROOT, rel)):
+        return None, None
+    for line in open(os.path.join(ROOT, rel)):
+        if line.startswith("traffic_per_launch_bytes:"):
+            return int(line.split(":")[1]), rel
+    return None, None
+
+
 def step_bytes(m, n, nnz, nnz_t, nnz_n):
     """Algorithmic bytes per kernel (int32 indices for A / A^T, int64 row pointer for N)."""
     return {
@@ -234,6 +249,7 @@ def run_ours(args, rank, world, local):
         hbm, how = peaks()
         dom = max(kt, key=kt.get)
         achieved = nb[dom] / (kt[dom] * 1e-3) / 1e9
+        traffic, traffic_src = profiled_traffic(dom)
         result = {
             "metric": METRIC, "value": round(value, 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
@@ -247,7 +263,8 @@ def run_ours(args, rank, world, local):
             "kernels": {k: {"ms": round(kt[k], 4), "bytes": nb[k], "GB/s": round(nb[k] / (kt[k] * 1e-3) / 1e9, 1)}
                         for k in names},
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
-                         "peak_source": how, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None},
+                         "peak_source": how, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": traffic,
+                         "traffic_source": traffic_src, "bytes_per_launch": nb[dom]},
             "clocks": clk,
         }
         if not args.no_ipm:
