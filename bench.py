@@ -353,6 +353,55 @@ def batched_ipm(K: int, sample_per_stratum: int = 4):
                              "iterations_mean": round(float(np.mean(plain_iters)), 2)}}
 
 
+def bb_batch(K: int, chunk: int, sample: int = 2):
+    """Branch-and-bound style batch: one base LP (m=5000, n=12000, 8 nonzeros
+    per column, seed 3000) and K node relaxations (lpgen.bb_nodes, seed 3000),
+    each warm-started from the base LP's barrier solution (primal and dual
+    estimate), solved by the batched GPU IPM in chunks of `chunk` nodes (the
+    dense normal-matrix factors of a chunk share the device); the plain GPU
+    IPM on `sample` nodes, extrapolated."""
+    import torch
+
+    import hnb200 as hn
+    import lpgen
+
+    base = lpgen.lp_uniform(5000, 12000, 8, 3000)
+    nodes = lpgen.bb_nodes(base, K)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r0 = hn.lp_solve(base)
+    base_s = time.perf_counter() - t0
+    status, obj, iters, used = [], [], [], []
+    t0 = time.perf_counter()
+    for c0 in range(0, K, chunk):
+        part = nodes[c0:c0 + chunk]
+        r = hn.lp_solve_batch([base] * len(part), lbs=[a for a, _ in part], ubs=[b for _, b in part],
+                              x0s=[r0["x"]] * len(part), y0s=[r0["y"]] * len(part))
+        status.append(r["status"])
+        obj.append(r["objective"])
+        iters.append(r["iterations"])
+        used.append(r["warm_used"])
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    status, obj, iters, used = map(np.concatenate, (status, obj, iters, used))
+    pt, matched = [], 0
+    for i in range(sample):
+        t1 = time.perf_counter()
+        p = hn.lp_solve(base, lb=nodes[i][0], ub=nodes[i][1])
+        torch.cuda.synchronize()
+        pt.append(time.perf_counter() - t1)
+        matched += int(p["status"] == status[i] and abs(p["objective"] - obj[i]) / (1 + abs(p["objective"])) <= 1e-8)
+    est = float(np.mean(pt)) * K
+    return {"workload": f"B&B batch: base LP m=5000 n=12000 8 nnz/col (seed 3000), {K} node relaxations "
+                        f"(1-40 bound changes each), warm-started from the base solution, chunks of {chunk}",
+            "base_solve_s": round(base_s, 2), "base_iterations": r0["iterations"],
+            "batched_s": round(wall, 2), "batched_solves_per_s": round(K / wall, 2),
+            "status_counts": {int(k): int(v) for k, v in zip(*np.unique(status, return_counts=True))},
+            "warm_used": int(used.sum()), "iterations_mean": round(float(iters.mean()), 2),
+            "plain_gpu_s_extrapolated": round(est, 1), "plain_gpu_solves_per_s_extrapolated": round(K / est, 3),
+            "speedup_vs_plain_gpu": round(est / wall, 2), "plain_sample": {"instances": sample, "matching": matched}}
+
+
 def run_only(args, local):
     """Single kernel group on the same LP (profiling aid). spmv / spmv_t flush
     L2 between launches by writing a 256 MB buffer; ada streams 11.6 GB."""
@@ -364,6 +413,8 @@ def run_only(args, local):
     dev = torch.device("cuda", local)
     torch.zeros(1, device=dev)
     hn.init(local)
+    if args.only == "bb":
+        return bb_batch(args.bb_k, args.bb_chunk)
     lp, vec = make_inputs(1000, args.scale)
     m, n = lp["m"], lp["n"]
     A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
@@ -450,12 +501,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", default="step", choices=["step", "spmv", "spmv_t", "ada"],
+    ap.add_argument("--only", default="step", choices=["step", "spmv", "spmv_t", "ada", "bb"],
                     help="time one kernel group alone (for profiling); 'step' is the measured workload")
     ap.add_argument("--no-ipm", action="store_true", help="skip the plain GPU IPM solve on the m=2000 LP")
     ap.add_argument("--scale", type=int, default=1, help="--only modes: shrink the LP by this factor (profiling)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-IPM key")
     ap.add_argument("--batch-k", type=int, default=4096, help="instances in the batched-IPM key")
+    ap.add_argument("--bb-k", type=int, default=2048, help="--only bb: node relaxations")
+    ap.add_argument("--bb-chunk", type=int, default=256, help="--only bb: nodes per batched solve")
     args = ap.parse_args()
     rank, world, local = dist_setup()
     if args.impl == "reference":

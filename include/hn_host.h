@@ -28,6 +28,17 @@ typedef struct hn_ipm_options {
      * with status INTERRUPTED (interior_point.cpp:490-493). May be NULL. */
     int (*interrupt_cb)(void* user);
     void* interrupt_user;
+    /* Warm start (no counterpart in the reference, whose IPM always starts
+     * from interior_point.cpp:443-453): x (n), y (m), s (n) in the original
+     * space of the minimisation form, A^T y + s = c at a dual-feasible point;
+     * y or s may be NULL. Mapped to the scaled standard form, shifted to strict
+     * interiority (Mehrotra's heuristic) and used only when its relative KKT
+     * residual is below the default start's. All NULL = default start. For
+     * hn_lp_solve_batch the arrays are packed by the instances' col_off /
+     * row_off. */
+    const double* initial_x;
+    const double* initial_y;
+    const double* initial_s;
 } hn_ipm_options;
 
 /* InteriorPointResult (core/lp/interior_point.hpp:29-38) plus phase times;
@@ -41,14 +52,21 @@ typedef struct hn_ipm_result {
     double factor_ms;
     double solve_ms;
     int64_t nnz_normal;
+    int warm_start_used;  /* 1 when the warm start was taken */
+    double kkt_default;   /* relative KKT residual of the default start */
+    double kkt_warm;      /* ... of the shifted warm start (0 if none) */
 } hn_ipm_result;
 
 void hn_ipm_default_options(hn_ipm_options* opt);
 /* min/max c^T x + obj_offset s.t. row i of A (sense 0 LE, 1 GE, 2 EQ) vs b_i,
- * lb <= x <= ub; A as CSR in the reference layout. x_out (n) may be NULL. */
+ * lb <= x <= ub; A as CSR in the reference layout. x_out (n) may be NULL.
+ * y_out (m) and s_out (n), may be NULL: the barrier's dual estimate in the
+ * original space of the minimisation form (A^T y + s = c) -- an extension;
+ * the reference's barrier returns no duals without crossover. */
 int hn_lp_solve(int64_t m, int64_t n, const uint64_t* row_ptr, const uint64_t* col_idx, const double* val,
                 const double* c, const double* b, const int* sense, const double* lb, const double* ub,
-                int maximize, double obj_offset, const hn_ipm_options* opt, hn_ipm_result* res, double* x_out);
+                int maximize, double obj_offset, const hn_ipm_options* opt, hn_ipm_result* res, double* x_out,
+                double* y_out, double* s_out);
 const char* hn_host_last_error(void);
 
 /* K LPs solved in lockstep by the batched GPU IPM (hn::lp::BatchInteriorPointSolver).
@@ -56,7 +74,9 @@ const char* hn_host_last_error(void);
  * col_off[i]..col_off[i+1] of c/lb/ub/x_out, nonzeros nnz_off[i]..nnz_off[i+1]
  * of col_idx/val (column indices local to the instance), and row pointer
  * entries row_off[i]+i .. row_off[i+1]+i+1 of row_ptr (local, starting at 0).
- * Per-instance outputs: status (model::ProblemStatus), objective, iterations. */
+ * Per-instance outputs: status (model::ProblemStatus), objective, iterations;
+ * optional (NULL = not wanted): x_out / s_out packed by col_off, y_out by
+ * row_off, warm_used (K). */
 typedef struct hn_batch_stats {
     int64_t rows, cols, nnz, nnz_normal;
     int64_t iterations;
@@ -66,7 +86,8 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
                       const uint64_t* row_ptr, const uint64_t* col_idx, const double* val, const double* c,
                       const double* b, const int* sense, const double* lb, const double* ub, const int* maximize,
                       const double* obj_offset, const hn_ipm_options* opt, int* status, double* objective,
-                      int64_t* iterations, double* x_out, hn_batch_stats* stats);
+                      int64_t* iterations, double* x_out, hn_batch_stats* stats, int* warm_used, double* y_out,
+                      double* s_out);
 
 /* B200Backend through C: the matrix arrives as the reference's three vectors
  * each call; the backend keeps it resident between calls. */

@@ -345,23 +345,27 @@ INTERRUPT_CB = C.CFUNCTYPE(C.c_int, C.c_void_p)
 class IpmOptions(C.Structure):
     _fields_ = [("max_iterations", C.c_int), ("time_limit_seconds", C.c_double), ("convergence_tol", C.c_double),
                 ("complementarity_tol", C.c_double), ("regularization", C.c_double), ("device", C.c_int),
-                ("verbose", C.c_int), ("interrupt_cb", INTERRUPT_CB), ("interrupt_user", C.c_void_p)]
+                ("verbose", C.c_int), ("interrupt_cb", INTERRUPT_CB), ("interrupt_user", C.c_void_p),
+                ("initial_x", _f64p), ("initial_y", _f64p), ("initial_s", _f64p)]
 
 
 class IpmResult(C.Structure):
     _fields_ = [("status", C.c_int), ("iterations", C.c_int64), ("objective", C.c_double),
                 ("solve_time_ms", C.c_double), ("device_ms", C.c_double), ("factor_ms", C.c_double),
-                ("solve_ms", C.c_double), ("nnz_normal", C.c_int64)]
+                ("solve_ms", C.c_double), ("nnz_normal", C.c_int64), ("warm_start_used", C.c_int),
+                ("kkt_default", C.c_double), ("kkt_warm", C.c_double)]
 
 
 HOST_SIGNATURES = {
     "hn_ipm_default_options": (None, [C.POINTER(IpmOptions)]),
     "hn_lp_solve": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, C.POINTER(C.c_int), _f64p, _f64p,
-                              C.c_int, C.c_double, C.POINTER(IpmOptions), C.POINTER(IpmResult), _f64p]),
+                              C.c_int, C.c_double, C.POINTER(IpmOptions), C.POINTER(IpmResult), _f64p,
+                              _f64p, _f64p]),
     "hn_host_last_error": (C.c_char_p, []),
     "hn_lp_solve_batch": (C.c_int, [_i64, _i64p, _i64p, _i64p, _u64p, _u64p, _f64p, _f64p, _f64p,
                                     C.POINTER(C.c_int), _f64p, _f64p, C.POINTER(C.c_int), _f64p,
-                                    C.POINTER(IpmOptions), C.POINTER(C.c_int), _f64p, _i64p, _f64p, _vp]),
+                                    C.POINTER(IpmOptions), C.POINTER(C.c_int), _f64p, _i64p, _f64p, _vp,
+                                    C.POINTER(C.c_int), _f64p, _f64p]),
     "hn_be_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
     "hn_be_destroy": (C.c_int, [_vp]),
     "hn_be_spmv": (C.c_int, [_vp, _i64, _i64, _u64p, _u64p, _f64p, _i64, _f64p, _f64p]),
@@ -399,9 +403,20 @@ def host_check(status: int) -> None:
         raise HnError(status, host().hn_host_last_error().decode(errors="replace"))
 
 
+def _warm_arrays(opt, x0, y0, s0):
+    keep = []
+    for name, a in (("initial_x", x0), ("initial_y", y0), ("initial_s", s0)):
+        if a is not None:
+            a = f64(a)
+            keep.append(a)
+            setattr(opt, name, _p(a, C.c_double))
+    return keep
+
+
 def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=0.0, max_iter=100,
-             time_limit=0.0, device=0, interrupt=None, verbose=False):
-    """GPU IPM on an LP given as CSR (rows EQ and x >= 0 unless told otherwise)."""
+             time_limit=0.0, device=0, interrupt=None, verbose=False, x0=None, y0=None, s0=None):
+    """GPU IPM on an LP given as CSR (rows EQ and x >= 0 unless told otherwise);
+    x0/y0/s0: optional warm start in the original space."""
     m, n = int(lp["m"]), int(lp["n"])
     rp, ci, val = u64(lp["rp"]), u64(lp["ci"]), f64(lp["val"])
     c, b = f64(lp["c"]), f64(lp["b"])
@@ -416,17 +431,22 @@ def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=
     opt.verbose = int(verbose)
     cb = INTERRUPT_CB(lambda _u: int(bool(interrupt()))) if interrupt is not None else INTERRUPT_CB()
     opt.interrupt_cb = cb
+    keep = _warm_arrays(opt, x0, y0, s0)  # noqa: F841 (alive through the call)
     res = IpmResult()
     x = np.zeros(n)
+    y = np.full(m, np.nan)
+    s = np.full(n, np.nan)
     host_check(host().hn_lp_solve(m, n, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
                                   _p(c, C.c_double), _p(b, C.c_double), sense.ctypes.data_as(C.POINTER(C.c_int)),
                                   _p(lb, C.c_double), _p(ub, C.c_double), int(maximize), float(obj_offset),
-                                  C.byref(opt), C.byref(res), _p(x, C.c_double)))
+                                  C.byref(opt), C.byref(res), _p(x, C.c_double), _p(y, C.c_double),
+                                  _p(s, C.c_double)))
     err = host().hn_host_last_error().decode(errors="replace")
     return {"status": res.status, "status_name": STATUS[res.status], "objective": res.objective,
             "iterations": res.iterations, "time_ms": res.solve_time_ms, "device_ms": res.device_ms,
             "factor_ms": res.factor_ms, "solve_ms": res.solve_ms, "nnz_normal": res.nnz_normal, "x": x,
-            "error": err}
+            "y": y, "s": s, "warm_start_used": bool(res.warm_start_used), "kkt_default": res.kkt_default,
+            "kkt_warm": res.kkt_warm, "error": err}
 
 
 class BatchStats(C.Structure):
@@ -435,8 +455,10 @@ class BatchStats(C.Structure):
                 ("solve_ms", C.c_double)]
 
 
-def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs=None):
-    """Batched GPU IPM over a list of LP dicts (rows EQ, x >= 0 unless given)."""
+def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs=None, x0s=None, y0s=None,
+                   s0s=None):
+    """Batched GPU IPM over a list of LP dicts (rows EQ, x >= 0 unless given);
+    x0s/y0s/s0s: optional per-instance warm starts (lists of arrays)."""
     K = len(lps)
     row_off = np.zeros(K + 1, np.int64)
     col_off = np.zeros(K + 1, np.int64)
@@ -459,10 +481,15 @@ def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs
     host().hn_ipm_default_options(C.byref(opt))
     opt.max_iterations = max_iter
     opt.device = device
+    keep = _warm_arrays(opt, None if x0s is None else np.concatenate(x0s),  # noqa: F841
+                        None if y0s is None else np.concatenate(y0s), None if s0s is None else np.concatenate(s0s))
+    warm_used = np.zeros(K, np.int32)
     status = np.zeros(K, np.int32)
     obj = np.zeros(K)
     iters = np.zeros(K, np.int64)
     x = np.zeros(col_off[-1])
+    y = np.full(row_off[-1], np.nan)
+    s = np.full(col_off[-1], np.nan)
     st = BatchStats()
     P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
     host_check(host().hn_lp_solve_batch(K, P(row_off, C.c_int64), P(col_off, C.c_int64), P(nnz_off, C.c_int64),
@@ -470,8 +497,11 @@ def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs
                                         P(b, C.c_double), P(sense, C.c_int), P(lb, C.c_double), P(ub, C.c_double),
                                         P(maxi, C.c_int), P(off, C.c_double), C.byref(opt), P(status, C.c_int),
                                         P(obj, C.c_double), P(iters, C.c_int64), P(x, C.c_double),
-                                        C.cast(C.pointer(st), C.c_void_p)))
-    return {"status": status, "objective": obj, "iterations": iters, "x": x, "col_off": col_off,
+                                        C.cast(C.pointer(st), C.c_void_p), P(warm_used, C.c_int), P(y, C.c_double),
+                                        P(s, C.c_double)))
+    return {"status": status, "objective": obj, "iterations": iters, "x": x, "y": y, "s": s, "col_off": col_off,
+            "row_off": row_off,
+            "warm_used": warm_used.astype(bool),
             "stats": {k: getattr(st, k) for k, _ in BatchStats._fields_}}
 
 

@@ -43,7 +43,8 @@ using Clock = std::chrono::steady_clock;
 double ms_since(Clock::time_point t) { return std::chrono::duration<double, std::milli>(Clock::now() - t).count(); }
 }  // namespace
 
-std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vector<model::LpProblem>& problems) {
+std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vector<model::LpProblem>& problems,
+                                                                 const std::vector<WarmStart>* warm) {
     const auto start = Clock::now();
     const auto& O = options_;
     const std::size_t K = problems.size();
@@ -52,7 +53,7 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
     stats_ = BatchStats{};
     try {
         PackedForm pf;
-        build_forms(problems, O.feasibility_tol, pf);
+        build_forms(problems, O.feasibility_tol, pf, warm);
         const std::size_t m = pf.row_off.back(), n = pf.col_off.back();
         stats_.rows = m;
         stats_.cols = n;
@@ -77,7 +78,7 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
         void* st = nullptr;
         ck(hn_memcpy_h2d(x.p, pf.x0.data(), 8 * n, st), "H2D");
         ck(hn_memcpy_h2d(z.p, pf.z0.data(), 8 * n, st), "H2D");
-        ck(hn_memset(lam.p, 0, 8 * m, st), "memset");
+        ck(hn_memcpy_h2d(lam.p, pf.lam0.data(), 8 * m, st), "H2D");
         ck(hn_memcpy_h2d(b.p, pf.rhs.data(), 8 * m, st), "H2D");
         ck(hn_memcpy_h2d(c.p, pf.c.data(), 8 * n, st), "H2D");
         ck(hn_memset(status.p, 0, 4 * K, st), "memset");
@@ -134,7 +135,8 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
         ck(hn_batch_residuals(B, M, x.d(), lam.d(), z.d(), b.d(), c.d(), mx.d(), rp.d(), rd.d(), D.d(), Drd.d(),
                               scal.d(), st_copy.i(), iters.i(), iter, O.convergence_tol, O.complementarity_tol, st),
            "hn_batch_residuals");
-        std::vector<double> hscal(HN_IPM_NSCAL * K), hx(n);
+        std::vector<double> hscal(HN_IPM_NSCAL * K), hx(n), hl(m);
+        ck(hn_memcpy_d2h(hl.data(), lam.p, 8 * m, st), "D2H lam");
         ck(hn_memcpy_d2h(hscal.data(), scal.p, 8 * HN_IPM_NSCAL * K, st), "D2H scal");
         ck(hn_memcpy_d2h(hstatus.data(), status.p, 4 * K, st), "D2H status");
         ck(hn_memcpy_d2h(hiters.data(), iters.p, 4 * K, st), "D2H iters");
@@ -162,6 +164,10 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
             r.dual.assign(p.num_rows, 0.0);
             r.iterations = (std::size_t)hiters[i];
             r.nnz_normal = 0;
+            original_duals_packed(pf, i, p, hl.data() + pf.row_off[i], r.dual_estimate, r.reduced_cost_estimate);
+            r.warm_start_used = pf.warm_used[i] != 0;
+            r.kkt_default = pf.kkt_default[i];
+            r.kkt_warm = pf.kkt_warm[i];
             r.solve_time_ms = total_ms;
             const bool feasible_incumbent = s[HN_IPM_NRP] <= O.feasibility_tol;
             r.status = numerical_error ? model::ProblemStatus::NUMERICAL_ERROR

@@ -48,13 +48,17 @@ void hn_ipm_default_options(hn_ipm_options* o) {
     o->verbose = 0;
     o->interrupt_cb = nullptr;
     o->interrupt_user = nullptr;
+    o->initial_x = nullptr;
+    o->initial_y = nullptr;
+    o->initial_s = nullptr;
 }
 
 const char* hn_host_last_error(void) { return g_err.c_str(); }
 
 int hn_lp_solve(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, const double* val, const double* c,
                 const double* b, const int* sense, const double* lb, const double* ub, int maximize,
-                double obj_offset, const hn_ipm_options* opt, hn_ipm_result* res, double* x_out) {
+                double obj_offset, const hn_ipm_options* opt, hn_ipm_result* res, double* x_out, double* y_out,
+                double* s_out) {
     return wrap([&] {
         if (m < 0 || n < 0 || !rp || !res) throw std::invalid_argument("bad arguments");
         hn::model::LpProblem p;
@@ -87,6 +91,11 @@ int hn_lp_solve(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, co
                 void* user = opt->interrupt_user;
                 o.interrupt_callback = [cb, user]() { return cb(user) != 0; };
             }
+            if (opt->initial_x) {
+                o.initial_point.x = vec(opt->initial_x, n);
+                if (opt->initial_y) o.initial_point.y = vec(opt->initial_y, m);
+                if (opt->initial_s) o.initial_point.s = vec(opt->initial_s, n);
+            }
         }
         hn::lp::InteriorPointSolver solver(o);
         auto r = solver.solve(p);
@@ -98,7 +107,13 @@ int hn_lp_solve(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, co
         res->factor_ms = r.factor_ms;
         res->solve_ms = r.solve_ms;
         res->nnz_normal = (int64_t)r.nnz_normal;
+        res->warm_start_used = r.warm_start_used ? 1 : 0;
+        res->kkt_default = r.kkt_default;
+        res->kkt_warm = r.kkt_warm;
         if (x_out && r.primal.size() == (std::size_t)n) std::memcpy(x_out, r.primal.data(), 8 * n);
+        if (y_out && r.dual_estimate.size() == (std::size_t)m) std::memcpy(y_out, r.dual_estimate.data(), 8 * m);
+        if (s_out && r.reduced_cost_estimate.size() == (std::size_t)n)
+            std::memcpy(s_out, r.reduced_cost_estimate.data(), 8 * n);
         g_err = r.error;
     });
 }
@@ -107,7 +122,8 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
                       const uint64_t* rp, const uint64_t* ci, const double* val, const double* c, const double* b,
                       const int* sense, const double* lb, const double* ub, const int* maximize,
                       const double* obj_offset, const hn_ipm_options* opt, int* status, double* objective,
-                      int64_t* iterations, double* x_out, hn_batch_stats* stats) {
+                      int64_t* iterations, double* x_out, hn_batch_stats* stats, int* warm_used, double* y_out,
+                      double* s_out) {
     return wrap([&] {
         if (K < 0 || !row_off || !col_off || !nnz_off || !status || !objective || !iterations)
             throw std::invalid_argument("bad arguments");
@@ -143,13 +159,29 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
             o.regularization = opt->regularization;
             o.device = opt->device;
         }
+        std::vector<hn::lp::WarmStart> warm;
+        if (opt && opt->initial_x) {
+            warm.resize((std::size_t)K);
+            for (int64_t i = 0; i < K; ++i) {
+                auto& w = warm[(std::size_t)i];
+                w.x = vec(opt->initial_x + col_off[i], col_off[i + 1] - col_off[i]);
+                if (opt->initial_y) w.y = vec(opt->initial_y + row_off[i], row_off[i + 1] - row_off[i]);
+                if (opt->initial_s) w.s = vec(opt->initial_s + col_off[i], col_off[i + 1] - col_off[i]);
+            }
+        }
         hn::lp::BatchInteriorPointSolver solver(o);
-        auto res = solver.solve(probs);
+        auto res = solver.solve(probs, warm.empty() ? nullptr : &warm);
         for (int64_t i = 0; i < K; ++i) {
             const auto& r = res[(std::size_t)i];
             status[i] = static_cast<int>(r.status);
             objective[i] = r.objective_value;
             iterations[i] = (int64_t)r.iterations;
+            if (warm_used) warm_used[i] = r.warm_start_used ? 1 : 0;
+            const auto& pi = probs[(std::size_t)i];
+            if (y_out && r.dual_estimate.size() == pi.num_rows)
+                std::memcpy(y_out + row_off[i], r.dual_estimate.data(), 8 * pi.num_rows);
+            if (s_out && r.reduced_cost_estimate.size() == pi.num_cols)
+                std::memcpy(s_out + col_off[i], r.reduced_cost_estimate.data(), 8 * pi.num_cols);
             if (x_out && r.primal.size() == probs[(std::size_t)i].num_cols)
                 std::memcpy(x_out + col_off[i], r.primal.data(), 8 * r.primal.size());
         }

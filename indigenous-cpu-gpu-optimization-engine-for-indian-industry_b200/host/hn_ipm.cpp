@@ -35,6 +35,8 @@ struct StandardForm {
     std::vector<double> val, rhs, c, col_scale;
     double offset = 0.0;
     std::vector<VarInfo> var_info;
+    std::size_t nslots = 0;         // structural columns; the rest are slacks (one entry each)
+    std::vector<double> row_mult;   // original row i -> standard row i scaled by this (-gamma for GE)
 };
 
 }  // namespace detail
@@ -164,6 +166,7 @@ StandardForm build_standard_form(const model::LpProblem& p, double feas_tol) {
     for (std::size_t i = 0; i < norig; ++i)
         if (p.sense[i] == ConstraintSense::LE || p.sense[i] == ConstraintSense::GE) ++ntle;
     const std::size_t m_rows = norig + m_ub, ncols = nslots + ntle + m_ub;
+    f.nslots = nslots;
     f.m = m_rows;
     f.n = ncols;
     f.rhs.assign(m_rows, 0.0);
@@ -177,6 +180,8 @@ StandardForm build_standard_form(const model::LpProblem& p, double feas_tol) {
         for (std::size_t k = p.row_ptr[i]; k < p.row_ptr[i + 1]; ++k) rowmax = std::max(rowmax, std::abs(p.values[k]));
         if (rowmax > 0.0) gamma[i] = 1.0 / rowmax;
     }
+    f.row_mult.resize(norig);
+    for (std::size_t i = 0; i < norig; ++i) f.row_mult[i] = p.sense[i] == ConstraintSense::GE ? -gamma[i] : gamma[i];
     std::vector<Trip> trips;
     std::size_t next_slack = nslots;
     for (std::size_t i = 0; i < norig; ++i) {
@@ -224,6 +229,154 @@ StandardForm build_standard_form(const model::LpProblem& p, double feas_tol) {
     csr_from_triplets(m_rows, scaled, f.rp, f.ci, f.val);
     for (std::size_t j = 0; j < ncols; ++j) f.c[j] *= f.col_scale[j];
     return f;
+}
+
+// ---- start points ----
+
+// Mehrotra's default start on the scaled standard form (interior_point.cpp:439-453).
+void default_start(const StandardForm& f, std::vector<double>& x, std::vector<double>& z, std::vector<double>& lam) {
+    double b_norm = 1.0, c_norm = 1.0;
+    for (double v : f.rhs) b_norm = std::max(b_norm, std::abs(v));
+    for (double v : f.c) c_norm = std::max(c_norm, std::abs(v));
+    x.assign(f.n, b_norm + 1.0);
+    z.resize(f.n);
+    for (std::size_t j = 0; j < f.n; ++j) z[j] = std::max(c_norm + 1.0, std::abs(f.c[j]));
+    lam.assign(f.m, 0.0);
+}
+
+// Relative KKT residual of (x, z, lam) on the scaled form:
+// max(||Mx-b||inf/(1+||b||inf), ||M^T lam + z - c||inf/(1+||c||inf), |x^T z|/(1+|c^T x|)).
+double start_kkt(const StandardForm& f, const std::vector<double>& x, const std::vector<double>& z,
+                 const std::vector<double>& lam) {
+    double bn = 0.0, cn = 0.0, rp = 0.0, rd = 0.0, xz = 0.0, cx = 0.0;
+    std::vector<double> mtl(f.n, 0.0);
+    for (std::size_t i = 0; i < f.m; ++i) {
+        double s = 0.0;
+        for (std::size_t k = f.rp[i]; k < f.rp[i + 1]; ++k) {
+            s += f.val[k] * x[f.ci[k]];
+            mtl[f.ci[k]] += f.val[k] * lam[i];
+        }
+        rp = std::max(rp, std::abs(s - f.rhs[i]));
+        bn = std::max(bn, std::abs(f.rhs[i]));
+    }
+    for (std::size_t j = 0; j < f.n; ++j) {
+        rd = std::max(rd, std::abs(mtl[j] + z[j] - f.c[j]));
+        cn = std::max(cn, std::abs(f.c[j]));
+        xz += x[j] * z[j];
+        cx += f.c[j] * x[j];
+    }
+    return std::max({rp / (1.0 + bn), rd / (1.0 + cn), std::abs(xz) / (1.0 + std::abs(cx))});
+}
+
+// Maps an original-space (x, y, s) to the scaled standard form and shifts it
+// to strict interiority with Mehrotra's heuristic (S. Mehrotra, "On the
+// implementation of a primal-dual interior point method", SIAM J. Optim.
+// 2(4), 1992, section 7): dx = max(-1.5 min x, 0), dz likewise, then
+// x += 0.5 x'z / sum z, z += 0.5 x'z / sum x. Returns false when the point
+// cannot be made strictly interior.
+bool warm_point(const StandardForm& f, const WarmStart& w, std::vector<double>& x, std::vector<double>& z,
+                std::vector<double>& lam) {
+    const std::size_t norig = f.row_mult.size();
+    if (w.x.size() != f.var_info.size() || (!w.y.empty() && w.y.size() != norig) ||
+        (!w.s.empty() && w.s.size() != f.var_info.size()))
+        return false;
+    x.assign(f.n, 0.0);
+    for (std::size_t j = 0; j < f.var_info.size(); ++j) {
+        const VarInfo& v = f.var_info[j];
+        if (v.is_fixed) continue;
+        if (v.slots.size() == 1) {
+            const int g = v.slots[0];
+            x[g] = (w.x[j] - v.shifts[0]) / (v.signs[0] * f.col_scale[g]);
+        } else if (v.slots.size() == 2) {
+            x[v.slots[0]] = std::max(w.x[j], 0.0) / f.col_scale[v.slots[0]];
+            x[v.slots[1]] = std::max(-w.x[j], 0.0) / f.col_scale[v.slots[1]];
+        }
+    }
+    // slack columns from the rows' residuals (each slack has one entry)
+    std::vector<double> r(f.rhs);
+    std::vector<std::size_t> slack_row(f.n - f.nslots);
+    std::vector<double> slack_coef(f.n - f.nslots, 0.0);
+    for (std::size_t i = 0; i < f.m; ++i)
+        for (std::size_t k = f.rp[i]; k < f.rp[i + 1]; ++k) {
+            if (f.ci[k] < f.nslots) {
+                r[i] -= f.val[k] * x[f.ci[k]];
+            } else {
+                slack_row[f.ci[k] - f.nslots] = i;
+                slack_coef[f.ci[k] - f.nslots] = f.val[k];
+            }
+        }
+    for (std::size_t s = 0; s < slack_coef.size(); ++s)
+        if (slack_coef[s] != 0.0) x[f.nslots + s] = r[slack_row[s]] / slack_coef[s];
+    lam.assign(f.m, 0.0);
+    if (!w.y.empty())
+        for (std::size_t i = 0; i < norig; ++i) lam[i] = w.y[i] / f.row_mult[i];
+    // z = c - M^T lam, then the given reduced costs on the structural slots
+    z = f.c;
+    for (std::size_t i = 0; i < f.m; ++i)
+        if (lam[i] != 0.0)
+            for (std::size_t k = f.rp[i]; k < f.rp[i + 1]; ++k) z[f.ci[k]] -= f.val[k] * lam[i];
+    if (!w.s.empty())
+        for (std::size_t j = 0; j < f.var_info.size(); ++j) {
+            const VarInfo& v = f.var_info[j];
+            for (std::size_t q = 0; q < v.slots.size(); ++q)
+                z[v.slots[q]] = v.signs[q] * f.col_scale[v.slots[q]] * w.s[j];
+        }
+    for (std::size_t j = 0; j < f.n; ++j)
+        if (!std::isfinite(x[j]) || !std::isfinite(z[j])) return false;
+    double xmin = 0.0, zmin = 0.0;
+    for (std::size_t j = 0; j < f.n; ++j) {
+        xmin = std::min(xmin, x[j]);
+        zmin = std::min(zmin, z[j]);
+    }
+    const double dx = std::max(-1.5 * xmin, 0.0), dz = std::max(-1.5 * zmin, 0.0);
+    double xz = 0.0, sx = 0.0, sz = 0.0;
+    for (std::size_t j = 0; j < f.n; ++j) {
+        x[j] += dx;
+        z[j] += dz;
+        xz += x[j] * z[j];
+        sx += x[j];
+        sz += z[j];
+    }
+    if (!(xz > 0.0) || !(sx > 0.0) || !(sz > 0.0)) return false;
+    const double dx2 = 0.5 * xz / sz, dz2 = 0.5 * xz / sx;
+    for (std::size_t j = 0; j < f.n; ++j) {
+        x[j] += dx2;
+        z[j] += dz2;
+        if (!(x[j] > 0.0) || !(z[j] > 0.0) || !std::isfinite(x[j]) || !std::isfinite(z[j])) return false;
+    }
+    return true;
+}
+
+// The start the solve uses: the warm one when given, usable and better by
+// the KKT residual, else the default. Returns whether the warm one is used.
+bool choose_start(const StandardForm& f, const WarmStart* w, std::vector<double>& x, std::vector<double>& z,
+                  std::vector<double>& lam, double* kkt_default, double* kkt_warm) {
+    default_start(f, x, z, lam);
+    *kkt_default = start_kkt(f, x, z, lam);
+    *kkt_warm = 0.0;
+    if (!w || w->empty()) return false;
+    std::vector<double> wx, wz, wl;
+    if (!warm_point(f, *w, wx, wz, wl)) return false;
+    *kkt_warm = start_kkt(f, wx, wz, wl);
+    if (!(*kkt_warm < *kkt_default)) return false;
+    x.swap(wx);
+    z.swap(wz);
+    lam.swap(wl);
+    return true;
+}
+
+void original_duals(const StandardForm& f, const model::LpProblem& p, const double* lam, std::vector<double>& y,
+                    std::vector<double>& s) {
+    y.clear();
+    s.clear();
+    if (f.row_mult.size() != p.num_rows) return;
+    y.resize(p.num_rows);
+    for (std::size_t i = 0; i < p.num_rows; ++i) y[i] = f.row_mult[i] * lam[i];
+    const bool negate = p.obj_sense == model::ObjectiveSense::MAXIMIZE;
+    s.resize(p.num_cols);
+    for (std::size_t j = 0; j < p.num_cols; ++j) s[j] = negate ? -p.objective[j] : p.objective[j];
+    for (std::size_t i = 0; i < p.num_rows; ++i)
+        for (std::size_t k = p.row_ptr[i]; k < p.row_ptr[i + 1]; ++k) s[p.col_indices[k]] -= p.values[k] * y[i];
 }
 
 std::vector<double> to_original_primal(const StandardForm& f, const std::vector<double>& y) {
@@ -312,7 +465,8 @@ constexpr std::size_t kMaxDenseRows = 12000;
 
 }  // namespace
 
-void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol, PackedForm& out) {
+void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol, PackedForm& out,
+                 const std::vector<WarmStart>* warm) {
     const std::size_t K = problems.size();
     std::vector<std::shared_ptr<StandardForm>> forms(K);
     std::string err;
@@ -352,20 +506,34 @@ void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol,
         }
         out.rhs.insert(out.rhs.end(), f.rhs.begin(), f.rhs.end());
         out.c.insert(out.c.end(), f.c.begin(), f.c.end());
-        // start point per instance (:439-453)
-        double b_norm = 1.0, c_norm = 1.0;
-        for (double v : f.rhs) b_norm = std::max(b_norm, std::abs(v));
-        for (double v : f.c) c_norm = std::max(c_norm, std::abs(v));
-        for (std::size_t j = 0; j < f.n; ++j) {
-            out.x0.push_back(b_norm + 1.0);
-            out.z0.push_back(std::max(c_norm + 1.0, std::abs(f.c[j])));
-        }
+    }
+    // start points per instance (default :439-453, or the warm start)
+    out.x0.resize(out.col_off.back());
+    out.z0.resize(out.col_off.back());
+    out.lam0.resize(out.row_off.back());
+    out.warm_used.assign(K, 0);
+    out.kkt_default.assign(K, 0.0);
+    out.kkt_warm.assign(K, 0.0);
+#pragma omp parallel for schedule(dynamic, 8)
+    for (std::size_t i = 0; i < K; ++i) {
+        const StandardForm& f = *forms[i];
+        std::vector<double> x, z, lam;
+        const WarmStart* w = (warm && i < warm->size()) ? &(*warm)[i] : nullptr;
+        out.warm_used[i] = choose_start(f, w, x, z, lam, &out.kkt_default[i], &out.kkt_warm[i]);
+        std::copy(x.begin(), x.end(), out.x0.begin() + out.col_off[i]);
+        std::copy(z.begin(), z.end(), out.z0.begin() + out.col_off[i]);
+        std::copy(lam.begin(), lam.end(), out.lam0.begin() + out.row_off[i]);
     }
     out.forms = std::move(forms);
 }
 
 std::vector<double> to_original_primal_packed(const PackedForm& pf, std::size_t i, const std::vector<double>& y) {
     return to_original_primal(*pf.forms[i], y);
+}
+
+void original_duals_packed(const PackedForm& pf, std::size_t i, const model::LpProblem& p, const double* lam,
+                           std::vector<double>& y, std::vector<double>& s) {
+    original_duals(*pf.forms[i], p, lam, y, s);
 }
 
 InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) {
@@ -420,12 +588,10 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
         ck(hn_pattern_export(P, N.rp.data(), N.ci.data()), "hn_pattern_export");
         result.nnz_normal = (std::size_t)pnnz;
 
-        // start point (:439-453)
-        double b_norm = 1.0, c_norm = 1.0;
-        for (double v : f.rhs) b_norm = std::max(b_norm, std::abs(v));
-        for (double v : f.c) c_norm = std::max(c_norm, std::abs(v));
-        std::vector<double> hx(n, b_norm + 1.0), hz(n), hlam(m, 0.0);
-        for (std::size_t j = 0; j < n; ++j) hz[j] = std::max(c_norm + 1.0, std::abs(f.c[j]));
+        // start point (:439-453, or the warm start)
+        std::vector<double> hx, hz, hlam;
+        result.warm_start_used =
+            choose_start(f, &O.initial_point, hx, hz, hlam, &result.kkt_default, &result.kkt_warm);
 
         DevBuf x(8 * n), z(8 * n), lam(8 * m), b(8 * m), c(8 * n), mx(8 * m), rp(8 * m), rd(8 * n), D(8 * n),
             Drd(8 * n), rhs_pred(8 * m), rhs(8 * m), dlam(8 * m), dx(8 * n), dz(8 * n), zs(8 * n),
@@ -563,6 +729,11 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
         result.objective_value = obj_ok ? obj : 0.0;
         result.primal = primal;
         result.dual.assign(problem.num_rows, 0.0);
+        {
+            std::vector<double> hl(m);
+            ck(hn_memcpy_d2h(hl.data(), lam.p, 8 * m, st), "D2H lam");
+            original_duals(f, problem, hl.data(), result.dual_estimate, result.reduced_cost_estimate);
+        }
         const bool feasible_incumbent = last_nrp <= O.feasibility_tol;
         result.status = numerical_error ? ProblemStatus::NUMERICAL_ERROR
                         : interrupted   ? ProblemStatus::INTERRUPTED

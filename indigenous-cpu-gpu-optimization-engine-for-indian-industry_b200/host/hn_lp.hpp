@@ -55,6 +55,16 @@ struct LpProblem {
 
 namespace hn::lp {
 
+// A starting point in the original space of the minimisation form (the
+// objective negated for a maximisation): x (num_cols), y (num_rows) and s
+// (num_cols) with A^T y + s = c at a dual-feasible point. y or s may be empty
+// (y = 0; s = c - A^T y). No counterpart in the reference, whose IPM always
+// starts from Mehrotra's default point (interior_point.cpp:443-453).
+struct WarmStart {
+    std::vector<double> x, y, s;
+    bool empty() const { return x.empty(); }
+};
+
 struct InteriorPointOptions {
     int max_iterations = 100;
     double time_limit_seconds = 0.0;
@@ -68,6 +78,10 @@ struct InteriorPointOptions {
     std::function<bool()> interrupt_callback;
     int device = 0;
     bool verbose = false;
+    // Warm start: mapped to the scaled standard form, shifted to strict
+    // interiority (Mehrotra's heuristic) and used only when its KKT residual
+    // is below the default start's.
+    WarmStart initial_point;
 };
 
 struct InteriorPointResult {
@@ -82,6 +96,15 @@ struct InteriorPointResult {
     double factor_ms = 0.0;
     double solve_ms = 0.0;
     std::size_t nnz_normal = 0;
+    // start point: relative KKT residual of the default start and of the
+    // warm start (0 when none was given), and which one was used
+    bool warm_start_used = false;
+    double kkt_default = 0.0, kkt_warm = 0.0;
+    // the barrier's dual estimate in the original space of the minimisation
+    // form (A^T y + s = c): the reference's barrier leaves `dual` zero and
+    // fills it only through crossover, so `dual` stays zero here and the
+    // estimate is reported beside it (a WarmStart for a related LP)
+    std::vector<double> dual_estimate, reduced_cost_estimate;
     std::string error;
 };
 
@@ -108,11 +131,19 @@ struct StandardForm;
 struct PackedForm {
     std::vector<int64_t> row_off{0}, col_off{0};
     std::vector<uint64_t> rp{0}, ci;
-    std::vector<double> val, rhs, c, x0, z0;
+    std::vector<double> val, rhs, c, x0, z0, lam0;
     std::vector<std::shared_ptr<detail::StandardForm>> forms;
+    std::vector<char> warm_used;
+    std::vector<double> kkt_default, kkt_warm;
 };
-void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol, PackedForm& out);
+// warm: empty, or one (possibly empty) WarmStart per problem
+void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol, PackedForm& out,
+                 const std::vector<WarmStart>* warm = nullptr);
 std::vector<double> to_original_primal_packed(const PackedForm& pf, std::size_t i, const std::vector<double>& y);
+// y = the standard form's multipliers of the original rows mapped back, s = c - A^T y
+// (minimisation form); empty when the standard form dropped duplicate rows.
+void original_duals_packed(const PackedForm& pf, std::size_t i, const model::LpProblem& p, const double* lam,
+                           std::vector<double>& y, std::vector<double>& s);
 
 struct BatchStats {
     std::size_t rows = 0, cols = 0, nnz = 0, nnz_normal = 0;
@@ -128,7 +159,8 @@ class BatchInteriorPointSolver {
 public:
     explicit BatchInteriorPointSolver(const InteriorPointOptions& options = InteriorPointOptions())
         : options_(options) {}
-    std::vector<InteriorPointResult> solve(const std::vector<model::LpProblem>& problems);
+    std::vector<InteriorPointResult> solve(const std::vector<model::LpProblem>& problems,
+                                           const std::vector<WarmStart>* warm = nullptr);
     const BatchStats& stats() const { return stats_; }
 
 private:

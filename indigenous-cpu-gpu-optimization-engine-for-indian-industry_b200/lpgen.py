@@ -129,3 +129,24 @@ def scaled_problem(lp: dict) -> dict:
     v2 = v1 * cs[ci]
     return {"m": m, "n": n, "rp": rp, "ci": ci, "val": v2, "b": gamma * lp["b"], "c": lp["c"] * cs,
             "col_scale": cs, "row_scale": gamma}
+
+
+def bb_nodes(base: dict, count: int = 2048, kmax: int = 40, seed: int = 3000):
+    """Branch-and-bound style node relaxations of `base` (x >= 0 LP): each
+    node picks k ~ U{1..kmax} distinct variables, perturbs x0_j by
+    U(-0.5, 0.5) and sets ub = floor(.) or lb = ceil(.) (coin flip, clipped
+    to >= 0). Returns a list of (lb, ub) arrays."""
+    rng = np.random.default_rng(seed)
+    n = base["n"]
+    nodes = []
+    for _ in range(count):
+        k = int(rng.integers(1, kmax + 1))
+        js = rng.choice(n, size=k, replace=False)
+        v = base["x0"][js] + rng.uniform(-0.5, 0.5, size=k)
+        lb = np.zeros(n)
+        ub = np.full(n, np.inf)
+        up = rng.random(k) < 0.5
+        ub[js[up]] = np.maximum(np.floor(v[up]), 0.0)
+        lb[js[~up]] = np.maximum(np.ceil(v[~up]), 0.0)
+        nodes.append((lb, ub))
+    return nodes
