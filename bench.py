@@ -402,6 +402,97 @@ def bb_batch(K: int, chunk: int, sample: int = 2):
             "speedup_vs_plain_gpu": round(est / wall, 2), "plain_sample": {"instances": sample, "matching": matched}}
 
 
+def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: int, plain_sample: int = 8):
+    """GNN warm start: LPs of the m=2000 generator with m log-uniform in
+    [mlo, mhi] and n = round(2.5 m), 8 nonzeros per column. Training LPs
+    (seeds 4,000,000 + i) are labelled by the batched GPU IPM (its primal
+    and dual estimate), the network is trained on the GPU (gnn.py), and
+    fresh LPs (seeds 1,000,000 + i) are solved by the batched GPU IPM from
+    the default start and from the network's prediction (inference time
+    included), and a sample by the plain one-at-a-time GPU IPM."""
+    import torch
+
+    import gnn
+    import hnb200 as hn
+    import lpgen
+
+    def gen(count, seed0):
+        rng = np.random.default_rng(seed0)
+        sizes = np.round(np.exp(rng.uniform(np.log(mlo), np.log(mhi), count))).astype(int)
+        return [lpgen.lp_uniform(int(m), int(round(2.5 * m)), 8, seed0 + i) for i, m in enumerate(sizes)]
+
+    def batched(lps, warm=None):
+        out = {"status": [], "objective": [], "iterations": [], "warm_used": [], "x": [], "y": [], "s": []}
+        for c0 in range(0, len(lps), chunk):
+            part = lps[c0:c0 + chunk]
+            kw = {}
+            if warm is not None:
+                preds = gnn.predict(warm, gnn.Batch(part))
+                kw = {"x0s": [p[0] for p in preds], "y0s": [p[1] for p in preds], "s0s": [p[2] for p in preds]}
+            r = hn.lp_solve_batch(part, **kw)
+            for k in ("status", "objective", "iterations", "warm_used"):
+                out[k].append(r[k])
+            for k, lp in enumerate(part):
+                c0_, c1_ = r["col_off"][k], r["col_off"][k + 1]
+                r0_, r1_ = r["row_off"][k], r["row_off"][k + 1]
+                out["x"].append(r["x"][c0_:c1_])
+                out["y"].append(r["y"][r0_:r1_])
+                out["s"].append(r["s"][c0_:c1_])
+        for k in ("status", "objective", "iterations", "warm_used"):
+            out[k] = np.concatenate(out[k])
+        return out
+
+    train_lps = gen(n_train, 4_000_000)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lab = batched(train_lps)
+    label_s = time.perf_counter() - t0
+    keep = [i for i in range(n_train) if lab["status"][i] == 1]
+    batches = []
+    for j in range(0, len(keep), 8):
+        ids = keep[j:j + 8]
+        batches.append(gnn.Batch([train_lps[i] for i in ids], [(lab["x"][i], lab["y"][i], lab["s"][i]) for i in ids]))
+    model = gnn.Model(seed=0)
+    t0 = time.perf_counter()
+    losses = gnn.train(model, batches, epochs=epochs, lr=1e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    del batches
+
+    eval_lps = gen(n_eval, 1_000_000)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    cold = batched(eval_lps)
+    torch.cuda.synchronize()
+    cold_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    warm = batched(eval_lps, warm=model)
+    torch.cuda.synchronize()
+    warm_s = time.perf_counter() - t0
+    same = (cold["status"] == warm["status"]) & (np.abs(cold["objective"] - warm["objective"]) <=
+                                                  1e-8 * (1 + np.abs(cold["objective"])))
+    pt = []
+    for i in range(min(plain_sample, n_eval)):
+        t1 = time.perf_counter()
+        hn.lp_solve(eval_lps[i])
+        torch.cuda.synchronize()
+        pt.append(time.perf_counter() - t1)
+    plain_est = float(np.mean(pt)) * n_eval
+    return {"workload": f"m=2000-generator LPs, m log-uniform [{mlo},{mhi}], n=2.5m, 8 nnz/col; "
+                        f"train {n_train} (seeds 4e6+i), eval {n_eval} fresh (seeds 1e6+i)",
+            "label_s": round(label_s, 1), "train_s": round(train_s, 1), "epochs": epochs,
+            "loss_first_last": [round(losses[0], 4), round(losses[-1], 4)],
+            "cold_batched_s": round(cold_s, 2), "cold_batched_solves_per_s": round(n_eval / cold_s, 2),
+            "warm_batched_s": round(warm_s, 2), "warm_batched_solves_per_s": round(n_eval / warm_s, 2),
+            "iterations_mean_cold": round(float(cold["iterations"].mean()), 2),
+            "iterations_mean_warm": round(float(warm["iterations"].mean()), 2),
+            "warm_used": int(warm["warm_used"].sum()), "optimal_cold": int((cold["status"] == 1).sum()),
+            "optimal_warm": int((warm["status"] == 1).sum()),
+            "same_status_and_objective_1e-8": int(same.sum()),
+            "plain_gpu_solves_per_s_extrapolated": round(n_eval / plain_est, 3),
+            "warm_batched_vs_plain_gpu": round(plain_est / warm_s, 2)}
+
+
 def run_only(args, local):
     """Single kernel group on the same LP (profiling aid). spmv / spmv_t flush
     L2 between launches by writing a 256 MB buffer; ada streams 11.6 GB."""
@@ -415,6 +506,8 @@ def run_only(args, local):
     hn.init(local)
     if args.only == "bb":
         return bb_batch(args.bb_k, args.bb_chunk)
+    if args.only == "gnn":
+        return gnn_warm(args.gnn_train, args.gnn_eval, args.gnn_mlo, args.gnn_mhi, args.gnn_epochs, args.gnn_chunk)
     lp, vec = make_inputs(1000, args.scale)
     m, n = lp["m"], lp["n"]
     A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
@@ -501,7 +594,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", default="step", choices=["step", "spmv", "spmv_t", "ada", "bb"],
+    ap.add_argument("--only", default="step", choices=["step", "spmv", "spmv_t", "ada", "bb", "gnn"],
                     help="time one kernel group alone (for profiling); 'step' is the measured workload")
     ap.add_argument("--no-ipm", action="store_true", help="skip the plain GPU IPM solve on the m=2000 LP")
     ap.add_argument("--scale", type=int, default=1, help="--only modes: shrink the LP by this factor (profiling)")
@@ -509,6 +602,12 @@ def main():
     ap.add_argument("--batch-k", type=int, default=4096, help="instances in the batched-IPM key")
     ap.add_argument("--bb-k", type=int, default=2048, help="--only bb: node relaxations")
     ap.add_argument("--bb-chunk", type=int, default=256, help="--only bb: nodes per batched solve")
+    ap.add_argument("--gnn-train", type=int, default=1024, help="--only gnn: training LPs")
+    ap.add_argument("--gnn-eval", type=int, default=512, help="--only gnn: evaluation LPs")
+    ap.add_argument("--gnn-mlo", type=int, default=500, help="--only gnn: smallest m")
+    ap.add_argument("--gnn-mhi", type=int, default=5000, help="--only gnn: largest m")
+    ap.add_argument("--gnn-epochs", type=int, default=20, help="--only gnn: training epochs")
+    ap.add_argument("--gnn-chunk", type=int, default=256, help="--only gnn: LPs per batched solve")
     args = ap.parse_args()
     rank, world, local = dist_setup()
     if args.impl == "reference":

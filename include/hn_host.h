@@ -39,6 +39,9 @@ typedef struct hn_ipm_options {
     const double* initial_x;
     const double* initial_y;
     const double* initial_s;
+    /* the warm start's final shift is at least this times the default
+     * start's entries (0.01) */
+    double warm_start_floor;
 } hn_ipm_options;
 
 /* InteriorPointResult (core/lp/interior_point.hpp:29-38) plus phase times;

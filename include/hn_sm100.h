@@ -313,6 +313,38 @@ int hn_price_select(int64_t n, const double* rc_dev, const double* weights_dev, 
  * stream to report it). */
 int hn_price_columns(const hn_csr* A, int64_t k, const int64_t* cols_dev, double* out_dev, void* stream);
 
+/* ---- GNN warm start (no counterpart in the reference) ----
+ * Kernels of a bipartite variable-constraint network with hidden width 64
+ * whose prediction warm-starts the IPM. Activations are FP32 row-major
+ * (rows x 64); GEMM operands are rounded to BF16 (round to nearest even) and
+ * multiplied on the tensor cores with FP32 accumulation. Weights: FP32
+ * masters W (K x 64 row-major); hn_gnn_cast_weights makes the BF16 copies
+ * Wt (64 x K) used by hn_gnn_linear and Wb (K x 64) used by the backward. */
+/* out (rows x 64) = A H (trans 0; H n x 64) or A^T H (trans 1; H m x 64);
+ * A's values rounded to FP32; out += when accumulate != 0. */
+int hn_gnn_spmm(const hn_csr* A, int trans, const float* H_dev, float* out_dev, int accumulate, void* stream);
+int hn_gnn_cast_weights(int K, const float* W_dev, void* Wt_bf16_dev, void* Wb_bf16_dev, void* stream);
+/* Y (M x N) = act([X1 | X2] W + bias); K1, K2 multiples of 16, K1 + K2 <= 128
+ * (<= 64 when N = 128); N = 64 or 128; relu != 0 applies max(., 0); X2 and
+ * bias may be NULL (K2 = 0 / no bias). */
+int hn_gnn_linear(int64_t M, int K1, int K2, const float* X1_dev, const float* X2_dev, const void* Wt_bf16_dev,
+                  int N, const float* bias_dev, int relu, float* Y_dev, void* stream);
+/* Backward of hn_gnn_linear with N = 64: G = dY * relu'(Y); dX (M x K, may be
+ * NULL; K = 64 or 128) = G W^T; dW (K x 64) = [X1 | X2]^T G; db (64) = sum of
+ * G's rows. scratch: >= ceil(M / 64) * (64 K + 64) floats. Deterministic. */
+int hn_gnn_linear_bwd(int64_t M, int K1, int K2, const float* X1_dev, const float* X2_dev, const void* Wb_bf16_dev,
+                      const float* Y_dev, const float* dY_dev, int relu, float* G_dev, float* dX_dev, float* dW_dev,
+                      float* db_dev, float* scratch_dev, int64_t scratch_floats, void* stream);
+/* dH (M x 64) += dX[:, :64]; dAgg (M x 64) = dX[:, 64:] (dX M x 128). */
+int hn_gnn_split_grad(int64_t M, const float* dX_dev, float* dH_dev, float* dAgg_dev, void* stream);
+/* dO (M x 64) = scale * 2 (O - T) in the first nt columns (T: M x 2), 0 in the
+ * others; loss_part (nparts floats): per-block sums of the squared errors. */
+int hn_gnn_head_grad(int64_t M, const float* O_dev, const float* T_dev, int nt, float scale, float* dO_dev,
+                     float* loss_part_dev, int64_t nparts, void* stream);
+/* Adam (bias-corrected, step >= 1) on FP32 weights. */
+int hn_gnn_adam(int64_t len, float* w_dev, const float* g_dev, float* m1_dev, float* m2_dev, float lr, float beta1,
+                float beta2, float eps, int64_t step, void* stream);
+
 /* ---- SpMV for callers that cannot allocate device memory ----
  * No counterpart in the reference. y = A x with A given as device CSR arrays
  * (int32 row_ptr m+1, int32 col_idx and double values nnz, row_ptr[m] == nnz,

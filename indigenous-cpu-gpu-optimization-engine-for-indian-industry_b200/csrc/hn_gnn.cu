@@ -1,0 +1,395 @@
+// Kernels of the bipartite variable-constraint GNN that predicts an IPM warm
+// start (no counterpart in the reference). Hidden width 64 throughout.
+//
+//   hn_gnn_spmm          out = A H or A^T H, H row-major rows x 64 (FP32),
+//                        A's FP64 values rounded to FP32; each output row is a
+//                        sequential sum over its row of A (deterministic)
+//   hn_gnn_linear        Y = act([X1 | X2] W + b): BF16 operands on the tensor
+//                        cores (mma.sync m16n8k16, FP32 accumulation)
+//   hn_gnn_linear_bwd    G = dY * relu'(Y); dX = G W^T (tensor cores);
+//                        dW = [X1 | X2]^T G and db = sum G per CTA partials,
+//                        then summed in a fixed order (deterministic)
+//   hn_gnn_adam          Adam step on FP32 master weights
+//
+// BF16 rounding is round-to-nearest-even of the FP32 operand
+// (__float2bfloat16_rn), applied when a tile is staged into shared memory.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "hn_internal.cuh"
+
+namespace hn {
+namespace {
+
+constexpr int kH = 64;          // hidden width
+constexpr int kGT = 128;        // threads of the GEMM kernels (4 warps)
+constexpr int kRowsPerCta = 64; // GEMM rows per CTA (16 per warp)
+constexpr int kMaxK = 128;      // [X1 | X2] width
+
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, const uint32_t* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// ---- SpMM: one warp per output row, each lane two of the 64 columns ----
+__global__ void gnn_spmm_kernel(int rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                const double* __restrict__ val, const float* __restrict__ H, int accumulate,
+                                float* __restrict__ out) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    float2 acc = make_float2(0.f, 0.f);
+    for (int e = rp[r]; e < rp[r + 1]; ++e) {
+        const float a = static_cast<float>(val[e]);
+        const float2 h = reinterpret_cast<const float2*>(H + (int64_t)ci[e] * kH)[lane];
+        acc.x += a * h.x;
+        acc.y += a * h.y;
+    }
+    float2* o = reinterpret_cast<float2*>(out + (int64_t)r * kH) + lane;
+    if (accumulate) {
+        const float2 p = *o;
+        acc.x = p.x + acc.x;
+        acc.y = p.y + acc.y;
+    }
+    *o = acc;
+}
+
+// dH += dX[:, :64]; dAgg = dX[:, 64:] (the two halves of a concatenated input)
+__global__ void gnn_split_grad_kernel(int64_t M, const float* __restrict__ dX, float* __restrict__ dH,
+                                      float* __restrict__ dAgg) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= M * kH) return;
+    const int64_t r = i / kH, c = i % kH;
+    dH[i] += dX[r * 2 * kH + c];
+    dAgg[i] = dX[r * 2 * kH + kH + c];
+}
+
+// Squared-error head: dO[:, c] = scale * 2 (O[:, c] - T[:, c]) for c < nt, 0
+// for the other columns; per-block partial sums of the squared errors.
+__global__ void gnn_head_grad_kernel(int64_t M, const float* __restrict__ O, const float* __restrict__ T, int nt,
+                                     float scale, float* __restrict__ dO, float* __restrict__ loss_part) {
+    __shared__ double sh[32];
+    double l = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M * kH; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / kH;
+        const int c = (int)(i % kH);
+        float g = 0.f;
+        if (c < nt) {
+            const float e = O[i] - T[r * 2 + c];
+            g = scale * 2.f * e;
+            l += (double)e * (double)e;
+        }
+        dO[i] = g;
+    }
+    l = block_sum<256>(l, sh);
+    if (threadIdx.x == 0) loss_part[blockIdx.x] = (float)l;
+}
+
+// ---- C[M x N] = act([X1 | X2] Bt^T + bias) ----
+// X1: M x K1, X2: M x K2 (row-major FP32, K1 + K2 = K <= 128, multiples of
+// 16); Bt: N x K row-major BF16 (the weight transposed, K contiguous);
+// N = 64 or 128; K <= KMAX. Each warp owns 16 rows and all N columns.
+template <int N, int KMAX>
+__global__ void __launch_bounds__(kGT) gnn_gemm_kernel(int64_t M, int K1, int K2, const float* __restrict__ X1,
+                                                       const float* __restrict__ X2,
+                                                       const __nv_bfloat16* __restrict__ Bt,
+                                                       const float* __restrict__ bias, int relu,
+                                                       float* __restrict__ C) {
+    constexpr int KP = KMAX + 8;  // padded rows: the fragment loads of a warp hit 32 banks
+    __shared__ __align__(16) __nv_bfloat16 sA[kRowsPerCta][KP];
+    __shared__ __align__(16) __nv_bfloat16 sB[N][KP];
+    const int K = K1 + K2;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    for (int idx = tid; idx < N * K; idx += kGT) {
+        const int n = idx / K, k = idx % K;
+        sB[n][k] = Bt[(int64_t)n * K + k];
+    }
+    const int64_t row0 = blockIdx.x * (int64_t)kRowsPerCta;
+    for (int idx = tid; idx < kRowsPerCta * K; idx += kGT) {
+        const int r = idx / K, k = idx % K;
+        const int64_t gr = row0 + r;
+        float v = 0.f;
+        if (gr < M) v = k < K1 ? X1[gr * K1 + k] : X2[gr * K2 + (k - K1)];
+        sA[r][k] = __float2bfloat16_rn(v);
+    }
+    __syncthreads();
+    float acc[N / 8][4];
+#pragma unroll
+    for (int j = 0; j < N / 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+    const int rb = warp * 16;
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        uint32_t a[4];
+        a[0] = *reinterpret_cast<const uint32_t*>(&sA[rb + g][k0 + 2 * t]);
+        a[1] = *reinterpret_cast<const uint32_t*>(&sA[rb + g + 8][k0 + 2 * t]);
+        a[2] = *reinterpret_cast<const uint32_t*>(&sA[rb + g][k0 + 2 * t + 8]);
+        a[3] = *reinterpret_cast<const uint32_t*>(&sA[rb + g + 8][k0 + 2 * t + 8]);
+#pragma unroll
+        for (int j = 0; j < N / 8; ++j) {
+            uint32_t b[2];
+            b[0] = *reinterpret_cast<const uint32_t*>(&sB[j * 8 + g][k0 + 2 * t]);
+            b[1] = *reinterpret_cast<const uint32_t*>(&sB[j * 8 + g][k0 + 2 * t + 8]);
+            mma_bf16(acc[j], a, b);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < N / 8; ++j) {
+        const int c = j * 8 + 2 * t;
+        const float b0 = bias ? bias[c] : 0.f, b1 = bias ? bias[c + 1] : 0.f;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t gr = row0 + rb + g + 8 * h;
+            if (gr >= M) continue;
+            float v0 = acc[j][2 * h] + b0, v1 = acc[j][2 * h + 1] + b1;
+            if (relu) {
+                v0 = fmaxf(v0, 0.f);
+                v1 = fmaxf(v1, 0.f);
+            }
+            *reinterpret_cast<float2*>(C + gr * N + c) = make_float2(v0, v1);
+        }
+    }
+}
+
+// G = dY * (Y > 0) (or dY when relu == 0)
+__global__ void gnn_relu_bwd_kernel(int64_t len, const float* __restrict__ dY, const float* __restrict__ Y, int relu,
+                                    float* __restrict__ G) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+        G[i] = (!relu || Y[i] > 0.f) ? dY[i] : 0.f;
+}
+
+// Per-CTA partial dW (K x 64) = [X1 | X2]_chunk^T G_chunk over kWRows rows
+// and partial db (64). Tensor cores with A = G^T (rows = the 64 outputs,
+// reduction over the chunk's rows) and B = [X1 | X2] (columns = K).
+constexpr int kWRows = 64;
+__global__ void __launch_bounds__(kGT) gnn_wgrad_kernel(int64_t M, int K1, int K2, const float* __restrict__ X1,
+                                                        const float* __restrict__ X2, const float* __restrict__ G,
+                                                        float* __restrict__ part_w, float* __restrict__ part_b) {
+    constexpr int RP = kWRows + 8;
+    __shared__ __align__(16) __nv_bfloat16 sGt[kH][RP];     // [output o][row]
+    __shared__ __align__(16) __nv_bfloat16 sXt[kMaxK][RP];  // [input k][row]
+    const int K = K1 + K2;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int64_t row0 = blockIdx.x * (int64_t)kWRows;
+    for (int idx = tid; idx < kWRows * kH; idx += kGT) {
+        const int r = idx / kH, o = idx % kH;
+        const int64_t gr = row0 + r;
+        sGt[o][r] = __float2bfloat16_rn(gr < M ? G[gr * kH + o] : 0.f);
+    }
+    for (int idx = tid; idx < kWRows * K; idx += kGT) {
+        const int r = idx / K, k = idx % K;
+        const int64_t gr = row0 + r;
+        float v = 0.f;
+        if (gr < M) v = k < K1 ? X1[gr * K1 + k] : X2[gr * K2 + (k - K1)];
+        sXt[k][r] = __float2bfloat16_rn(v);
+    }
+    __syncthreads();
+    // bias partial: FP32 sum of G over the chunk, rows in order
+    if (tid < kH) {
+        float s = 0.f;
+        for (int r = 0; r < kWRows; ++r) {
+            const int64_t gr = row0 + r;
+            if (gr < M) s += G[gr * kH + tid];
+        }
+        part_b[(int64_t)blockIdx.x * kH + tid] = s;
+    }
+    // warp w: outputs o in [16w, 16w + 16), all K columns in 8-wide tiles
+    const int ob = warp * 16;
+    for (int n0 = 0; n0 < K; n0 += 8) {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int k0 = 0; k0 < kWRows; k0 += 16) {
+            uint32_t a[4], b[2];
+            a[0] = *reinterpret_cast<const uint32_t*>(&sGt[ob + g][k0 + 2 * t]);
+            a[1] = *reinterpret_cast<const uint32_t*>(&sGt[ob + g + 8][k0 + 2 * t]);
+            a[2] = *reinterpret_cast<const uint32_t*>(&sGt[ob + g][k0 + 2 * t + 8]);
+            a[3] = *reinterpret_cast<const uint32_t*>(&sGt[ob + g + 8][k0 + 2 * t + 8]);
+            b[0] = *reinterpret_cast<const uint32_t*>(&sXt[n0 + g][k0 + 2 * t]);
+            b[1] = *reinterpret_cast<const uint32_t*>(&sXt[n0 + g][k0 + 2 * t + 8]);
+            mma_bf16(acc, a, b);
+        }
+        // dW[k][o] (the weights' K x 64 layout)
+        float* pw = part_w + (int64_t)blockIdx.x * kH * K;
+        const int c = n0 + 2 * t;
+        pw[c * kH + ob + g] = acc[0];
+        pw[(c + 1) * kH + ob + g] = acc[1];
+        pw[c * kH + ob + g + 8] = acc[2];
+        pw[(c + 1) * kH + ob + g + 8] = acc[3];
+    }
+}
+
+// out[i] = sum over blocks b (in order) of part[b * len + i]
+__global__ void gnn_sum_parts_kernel(int64_t nb, int64_t len, const float* __restrict__ part, float* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= len) return;
+    float s = 0.f;
+    for (int64_t b = 0; b < nb; ++b) s += part[b * len + i];
+    out[i] = s;
+}
+
+// W (K x 64, FP32 master, row-major) -> Wt (64 x K, BF16) and Wb (K x 64, BF16)
+__global__ void gnn_cast_weights_kernel(int K, const float* __restrict__ W, __nv_bfloat16* __restrict__ Wt,
+                                        __nv_bfloat16* __restrict__ Wb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= K * kH) return;
+    const int k = i / kH, o = i % kH;
+    const __nv_bfloat16 v = __float2bfloat16_rn(W[i]);
+    Wt[o * K + k] = v;
+    Wb[i] = v;
+}
+
+__global__ void gnn_adam_kernel(int64_t len, float* __restrict__ w, const float* __restrict__ g,
+                                float* __restrict__ m1, float* __restrict__ m2, float lr, float b1, float b2,
+                                float eps, float c1, float c2) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= len) return;
+    const float gi = g[i];
+    const float a = b1 * m1[i] + (1.f - b1) * gi;
+    const float b = b2 * m2[i] + (1.f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = b;
+    w[i] -= lr * (a / c1) / (sqrtf(b / c2) + eps);
+}
+
+}  // namespace
+}  // namespace hn
+
+using namespace hn;
+
+extern "C" {
+
+int hn_gnn_spmm(const hn_csr* A, int trans, const float* H, float* out, int accumulate, void* stream) {
+    return guard("hn_gnn_spmm", [&] {
+        require_init();
+        if (!A || !H || !out) fail(HN_ERR_INVALID_ARG, "null argument");
+        if (trans && !A->has_t) fail(HN_ERR_INVALID_ARG, "matrix was created without its transpose");
+        const int rows = (int)(trans ? A->n : A->m);
+        if (rows == 0) return;
+        const int32_t* rp = trans ? A->rpT : A->rp;
+        const int32_t* ci = trans ? A->ciT : A->ci;
+        const double* val = trans ? A->valT : A->val;
+        gnn_spmm_kernel<<<(unsigned)((rows * 32LL + 255) / 256), 256, 0, as_stream(stream)>>>(rows, rp, ci, val, H,
+                                                                                            accumulate, out);
+        launched("gnn_spmm_kernel");
+    });
+}
+
+int hn_gnn_cast_weights(int K, const float* W, void* Wt_bf16, void* Wb_bf16, void* stream) {
+    return guard("hn_gnn_cast_weights", [&] {
+        require_init();
+        if (K <= 0 || K > kMaxK || !W || !Wt_bf16 || !Wb_bf16) fail(HN_ERR_INVALID_ARG, "bad arguments");
+        gnn_cast_weights_kernel<<<(K * kH + 255) / 256, 256, 0, as_stream(stream)>>>(
+            K, W, static_cast<__nv_bfloat16*>(Wt_bf16), static_cast<__nv_bfloat16*>(Wb_bf16));
+        launched("gnn_cast_weights_kernel");
+    });
+}
+
+int hn_gnn_linear(int64_t M, int K1, int K2, const float* X1, const float* X2, const void* Wt_bf16, int N,
+                  const float* bias, int relu, float* Y, void* stream) {
+    return guard("hn_gnn_linear", [&] {
+        require_init();
+        const int K = K1 + K2;
+        if (M < 0 || K1 <= 0 || K2 < 0 || K > kMaxK || K1 % 16 || K2 % 16 || !X1 || (K2 && !X2) || !Wt_bf16 ||
+            !Y || (N != 64 && N != 128))
+            fail(HN_ERR_INVALID_ARG, "bad arguments (K1, K2 multiples of 16, K1 + K2 <= 128, N 64 or 128)");
+        if (M == 0) return;
+        const unsigned grid = (unsigned)((M + kRowsPerCta - 1) / kRowsPerCta);
+        const auto* B = static_cast<const __nv_bfloat16*>(Wt_bf16);
+        if (N == 64) {
+            gnn_gemm_kernel<64, kMaxK><<<grid, kGT, 0, as_stream(stream)>>>(M, K1, K2, X1, X2, B, bias, relu, Y);
+        } else {
+            if (K > 64) fail(HN_ERR_INVALID_ARG, "N = 128 takes K1 + K2 <= 64");
+            gnn_gemm_kernel<128, 64><<<grid, kGT, 0, as_stream(stream)>>>(M, K1, K2, X1, X2, B, bias, relu, Y);
+        }
+        launched("gnn_gemm_kernel");
+    });
+}
+
+int hn_gnn_linear_bwd(int64_t M, int K1, int K2, const float* X1, const float* X2, const void* Wb_bf16,
+                      const float* Y, const float* dY, int relu, float* G, float* dX, float* dW, float* db,
+                      float* scratch, int64_t scratch_floats, void* stream) {
+    return guard("hn_gnn_linear_bwd", [&] {
+        require_init();
+        const int K = K1 + K2;
+        if (M < 0 || K1 <= 0 || K2 < 0 || K > kMaxK || K1 % 16 || K2 % 16 || !X1 || (K2 && !X2) || !Y || !dY ||
+            !G || !dW || !db || !scratch)
+            fail(HN_ERR_INVALID_ARG, "bad arguments");
+        cudaStream_t s = as_stream(stream);
+        const int64_t nb = std::max<int64_t>(1, (M + kWRows - 1) / kWRows);
+        if (scratch_floats < nb * (int64_t)(kH * K + kH)) fail(HN_ERR_INVALID_ARG, "scratch too small");
+        const int64_t len = M * kH;
+        if (len > 0) {
+            gnn_relu_bwd_kernel<<<(unsigned)std::min<int64_t>((len + 255) / 256, 148 * 16), 256, 0, s>>>(len, dY, Y,
+                                                                                                     relu, G);
+            launched("gnn_relu_bwd_kernel");
+        }
+        // dX = G W^T: N = K columns, B^T = W (K x 64 row-major BF16)
+        if (dX && M > 0) {
+            if (K != 64 && K != 128) fail(HN_ERR_INVALID_ARG, "dX needs K1 + K2 of 64 or 128");
+            const unsigned grid = (unsigned)((M + kRowsPerCta - 1) / kRowsPerCta);
+            const auto* B = static_cast<const __nv_bfloat16*>(Wb_bf16);
+            if (K == 64) {
+                gnn_gemm_kernel<64, 64><<<grid, kGT, 0, s>>>(M, kH, 0, G, nullptr, B, nullptr, 0, dX);
+            } else {
+                gnn_gemm_kernel<128, 64><<<grid, kGT, 0, s>>>(M, kH, 0, G, nullptr, B, nullptr, 0, dX);
+            }
+            launched("gnn_gemm_kernel");
+        }
+        float* pw = scratch;
+        float* pb = scratch + nb * kH * K;
+        if (M > 0) {
+            gnn_wgrad_kernel<<<(unsigned)nb, kGT, 0, s>>>(M, K1, K2, X1, X2, G, pw, pb);
+            launched("gnn_wgrad_kernel");
+        } else {
+            check_cuda(cudaMemsetAsync(scratch, 0, sizeof(float) * (kH * K + kH), s), "memset");
+        }
+        gnn_sum_parts_kernel<<<(unsigned)((kH * K + 255) / 256), 256, 0, s>>>(nb, (int64_t)kH * K, pw, dW);
+        launched("gnn_sum_parts_kernel");
+        gnn_sum_parts_kernel<<<1, kH, 0, s>>>(nb, kH, pb, db);
+        launched("gnn_sum_parts_kernel");
+    });
+}
+
+int hn_gnn_split_grad(int64_t M, const float* dX, float* dH, float* dAgg, void* stream) {
+    return guard("hn_gnn_split_grad", [&] {
+        require_init();
+        if (M < 0 || (M && (!dX || !dH || !dAgg))) fail(HN_ERR_INVALID_ARG, "bad arguments");
+        if (M == 0) return;
+        gnn_split_grad_kernel<<<(unsigned)((M * kH + 255) / 256), 256, 0, as_stream(stream)>>>(M, dX, dH, dAgg);
+        launched("gnn_split_grad_kernel");
+    });
+}
+
+int hn_gnn_head_grad(int64_t M, const float* O, const float* T, int nt, float scale, float* dO, float* loss_part,
+                     int64_t nparts, void* stream) {
+    return guard("hn_gnn_head_grad", [&] {
+        require_init();
+        if (M < 0 || nt < 1 || nt > 2 || nparts < 1 || (M && (!O || !T || !dO)) || !loss_part)
+            fail(HN_ERR_INVALID_ARG, "bad arguments");
+        const int grid = (int)std::min<int64_t>(nparts, std::max<int64_t>(1, (M * kH + 255) / 256));
+        gnn_head_grad_kernel<<<grid, 256, 0, as_stream(stream)>>>(M, O, T, nt, scale, dO, loss_part);
+        launched("gnn_head_grad_kernel");
+        if (grid < nparts)
+            check_cuda(cudaMemsetAsync(loss_part + grid, 0, sizeof(float) * (nparts - grid), as_stream(stream)),
+                       "memset");
+    });
+}
+
+int hn_gnn_adam(int64_t len, float* w, const float* g, float* m1, float* m2, float lr, float beta1, float beta2,
+                float eps, int64_t step, void* stream) {
+    return guard("hn_gnn_adam", [&] {
+        require_init();
+        if (len < 0 || step < 1 || (len && (!w || !g || !m1 || !m2))) fail(HN_ERR_INVALID_ARG, "bad arguments");
+        if (len == 0) return;
+        const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+        gnn_adam_kernel<<<(unsigned)((len + 255) / 256), 256, 0, as_stream(stream)>>>(len, w, g, m1, m2, lr, beta1,
+                                                                                      beta2, eps, c1, c2);
+        launched("gnn_adam_kernel");
+    });
+}
+
+}  // extern "C"

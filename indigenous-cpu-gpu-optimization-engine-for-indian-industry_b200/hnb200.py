@@ -93,6 +93,14 @@ SIGNATURES = {
     "hn_price_devex_update": [_vp, _vp, _vp, _vp, _vp, _vp],
     "hn_price_select": [_i64, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_double, C.c_int, _i64, _vp, _vp],
     "hn_price_columns": [_vp, _i64, _vp, _vp, _vp],
+    "hn_gnn_spmm": [_vp, C.c_int, _vp, _vp, C.c_int, _vp],
+    "hn_gnn_cast_weights": [C.c_int, _vp, _vp, _vp, _vp],
+    "hn_gnn_linear": [_i64, C.c_int, C.c_int, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp],
+    "hn_gnn_linear_bwd": [_i64, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _i64,
+                          _vp],
+    "hn_gnn_split_grad": [_i64, _vp, _vp, _vp, _vp],
+    "hn_gnn_head_grad": [_i64, _vp, _vp, C.c_int, C.c_float, _vp, _vp, _i64, _vp],
+    "hn_gnn_adam": [_i64, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_float, C.c_float, _i64, _vp],
     "hn_batch_create": [_i64, _i64p, _i64p, _vp, C.POINTER(_vp)],
     "hn_batch_destroy": [_vp],
     "hn_batch_residuals": [_vp, _vp] + [_vp] * 13 + [C.c_int, C.c_double, C.c_double, _vp],
@@ -346,7 +354,7 @@ class IpmOptions(C.Structure):
     _fields_ = [("max_iterations", C.c_int), ("time_limit_seconds", C.c_double), ("convergence_tol", C.c_double),
                 ("complementarity_tol", C.c_double), ("regularization", C.c_double), ("device", C.c_int),
                 ("verbose", C.c_int), ("interrupt_cb", INTERRUPT_CB), ("interrupt_user", C.c_void_p),
-                ("initial_x", _f64p), ("initial_y", _f64p), ("initial_s", _f64p)]
+                ("initial_x", _f64p), ("initial_y", _f64p), ("initial_s", _f64p), ("warm_start_floor", C.c_double)]
 
 
 class IpmResult(C.Structure):
@@ -414,7 +422,7 @@ def _warm_arrays(opt, x0, y0, s0):
 
 
 def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=0.0, max_iter=100,
-             time_limit=0.0, device=0, interrupt=None, verbose=False, x0=None, y0=None, s0=None):
+             time_limit=0.0, device=0, interrupt=None, verbose=False, x0=None, y0=None, s0=None, warm_floor=None):
     """GPU IPM on an LP given as CSR (rows EQ and x >= 0 unless told otherwise);
     x0/y0/s0: optional warm start in the original space."""
     m, n = int(lp["m"]), int(lp["n"])
@@ -432,6 +440,8 @@ def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=
     cb = INTERRUPT_CB(lambda _u: int(bool(interrupt()))) if interrupt is not None else INTERRUPT_CB()
     opt.interrupt_cb = cb
     keep = _warm_arrays(opt, x0, y0, s0)  # noqa: F841 (alive through the call)
+    if warm_floor is not None:
+        opt.warm_start_floor = warm_floor
     res = IpmResult()
     x = np.zeros(n)
     y = np.full(m, np.nan)
@@ -456,7 +466,7 @@ class BatchStats(C.Structure):
 
 
 def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs=None, x0s=None, y0s=None,
-                   s0s=None):
+                   s0s=None, warm_floor=None):
     """Batched GPU IPM over a list of LP dicts (rows EQ, x >= 0 unless given);
     x0s/y0s/s0s: optional per-instance warm starts (lists of arrays)."""
     K = len(lps)
@@ -483,6 +493,8 @@ def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs
     opt.device = device
     keep = _warm_arrays(opt, None if x0s is None else np.concatenate(x0s),  # noqa: F841
                         None if y0s is None else np.concatenate(y0s), None if s0s is None else np.concatenate(s0s))
+    if warm_floor is not None:
+        opt.warm_start_floor = warm_floor
     warm_used = np.zeros(K, np.int32)
     status = np.zeros(K, np.int32)
     obj = np.zeros(K)

@@ -53,7 +53,7 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
     stats_ = BatchStats{};
     try {
         PackedForm pf;
-        build_forms(problems, O.feasibility_tol, pf, warm);
+        build_forms(problems, O.feasibility_tol, pf, warm, O.warm_start_floor);
         const std::size_t m = pf.row_off.back(), n = pf.col_off.back();
         stats_.rows = m;
         stats_.cols = n;

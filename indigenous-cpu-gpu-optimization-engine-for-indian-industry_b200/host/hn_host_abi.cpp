@@ -51,6 +51,7 @@ void hn_ipm_default_options(hn_ipm_options* o) {
     o->initial_x = nullptr;
     o->initial_y = nullptr;
     o->initial_s = nullptr;
+    o->warm_start_floor = 1e-2;
 }
 
 const char* hn_host_last_error(void) { return g_err.c_str(); }
@@ -91,6 +92,7 @@ int hn_lp_solve(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, co
                 void* user = opt->interrupt_user;
                 o.interrupt_callback = [cb, user]() { return cb(user) != 0; };
             }
+            o.warm_start_floor = opt->warm_start_floor;
             if (opt->initial_x) {
                 o.initial_point.x = vec(opt->initial_x, n);
                 if (opt->initial_y) o.initial_point.y = vec(opt->initial_y, m);
@@ -158,6 +160,7 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
             o.complementarity_tol = opt->complementarity_tol;
             o.regularization = opt->regularization;
             o.device = opt->device;
+            o.warm_start_floor = opt->warm_start_floor;
         }
         std::vector<hn::lp::WarmStart> warm;
         if (opt && opt->initial_x) {

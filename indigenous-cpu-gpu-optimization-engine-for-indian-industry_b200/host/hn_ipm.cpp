@@ -272,10 +272,12 @@ double start_kkt(const StandardForm& f, const std::vector<double>& x, const std:
 // to strict interiority with Mehrotra's heuristic (S. Mehrotra, "On the
 // implementation of a primal-dual interior point method", SIAM J. Optim.
 // 2(4), 1992, section 7): dx = max(-1.5 min x, 0), dz likewise, then
-// x += 0.5 x'z / sum z, z += 0.5 x'z / sum x. Returns false when the point
-// cannot be made strictly interior.
-bool warm_point(const StandardForm& f, const WarmStart& w, std::vector<double>& x, std::vector<double>& z,
-                std::vector<double>& lam) {
+// x += 0.5 x'z / sum z, z += 0.5 x'z / sum x, the second shifts at least
+// `floor` times the default start's x and z entries (a point on the boundary
+// would otherwise start with almost no centrality). Returns false when the
+// point cannot be made strictly interior.
+bool warm_point(const StandardForm& f, const WarmStart& w, double floor, std::vector<double>& x,
+                std::vector<double>& z, std::vector<double>& lam) {
     const std::size_t norig = f.row_mult.size();
     if (w.x.size() != f.var_info.size() || (!w.y.empty() && w.y.size() != norig) ||
         (!w.s.empty() && w.s.size() != f.var_info.size()))
@@ -338,7 +340,11 @@ bool warm_point(const StandardForm& f, const WarmStart& w, std::vector<double>& 
         sz += z[j];
     }
     if (!(xz > 0.0) || !(sx > 0.0) || !(sz > 0.0)) return false;
-    const double dx2 = 0.5 * xz / sz, dz2 = 0.5 * xz / sx;
+    double b_norm = 1.0, c_norm = 1.0;
+    for (double v : f.rhs) b_norm = std::max(b_norm, std::abs(v));
+    for (double v : f.c) c_norm = std::max(c_norm, std::abs(v));
+    const double dx2 = std::max(0.5 * xz / sz, floor * (b_norm + 1.0));
+    const double dz2 = std::max(0.5 * xz / sx, floor * (c_norm + 1.0));
     for (std::size_t j = 0; j < f.n; ++j) {
         x[j] += dx2;
         z[j] += dz2;
@@ -349,14 +355,14 @@ bool warm_point(const StandardForm& f, const WarmStart& w, std::vector<double>& 
 
 // The start the solve uses: the warm one when given, usable and better by
 // the KKT residual, else the default. Returns whether the warm one is used.
-bool choose_start(const StandardForm& f, const WarmStart* w, std::vector<double>& x, std::vector<double>& z,
-                  std::vector<double>& lam, double* kkt_default, double* kkt_warm) {
+bool choose_start(const StandardForm& f, const WarmStart* w, double floor, std::vector<double>& x,
+                  std::vector<double>& z, std::vector<double>& lam, double* kkt_default, double* kkt_warm) {
     default_start(f, x, z, lam);
     *kkt_default = start_kkt(f, x, z, lam);
     *kkt_warm = 0.0;
     if (!w || w->empty()) return false;
     std::vector<double> wx, wz, wl;
-    if (!warm_point(f, *w, wx, wz, wl)) return false;
+    if (!warm_point(f, *w, floor, wx, wz, wl)) return false;
     *kkt_warm = start_kkt(f, wx, wz, wl);
     if (!(*kkt_warm < *kkt_default)) return false;
     x.swap(wx);
@@ -466,7 +472,7 @@ constexpr std::size_t kMaxDenseRows = 12000;
 }  // namespace
 
 void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol, PackedForm& out,
-                 const std::vector<WarmStart>* warm) {
+                 const std::vector<WarmStart>* warm, double warm_floor) {
     const std::size_t K = problems.size();
     std::vector<std::shared_ptr<StandardForm>> forms(K);
     std::string err;
@@ -519,7 +525,7 @@ void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol,
         const StandardForm& f = *forms[i];
         std::vector<double> x, z, lam;
         const WarmStart* w = (warm && i < warm->size()) ? &(*warm)[i] : nullptr;
-        out.warm_used[i] = choose_start(f, w, x, z, lam, &out.kkt_default[i], &out.kkt_warm[i]);
+        out.warm_used[i] = choose_start(f, w, warm_floor, x, z, lam, &out.kkt_default[i], &out.kkt_warm[i]);
         std::copy(x.begin(), x.end(), out.x0.begin() + out.col_off[i]);
         std::copy(z.begin(), z.end(), out.z0.begin() + out.col_off[i]);
         std::copy(lam.begin(), lam.end(), out.lam0.begin() + out.row_off[i]);
@@ -591,7 +597,8 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
         // start point (:439-453, or the warm start)
         std::vector<double> hx, hz, hlam;
         result.warm_start_used =
-            choose_start(f, &O.initial_point, hx, hz, hlam, &result.kkt_default, &result.kkt_warm);
+            choose_start(f, &O.initial_point, O.warm_start_floor, hx, hz, hlam, &result.kkt_default,
+                         &result.kkt_warm);
 
         DevBuf x(8 * n), z(8 * n), lam(8 * m), b(8 * m), c(8 * n), mx(8 * m), rp(8 * m), rd(8 * n), D(8 * n),
             Drd(8 * n), rhs_pred(8 * m), rhs(8 * m), dlam(8 * m), dx(8 * n), dz(8 * n), zs(8 * n),

@@ -79,9 +79,11 @@ struct InteriorPointOptions {
     int device = 0;
     bool verbose = false;
     // Warm start: mapped to the scaled standard form, shifted to strict
-    // interiority (Mehrotra's heuristic) and used only when its KKT residual
-    // is below the default start's.
+    // interiority (Mehrotra's heuristic, with the final shift at least
+    // warm_start_floor times the default start's entries) and used only when
+    // its KKT residual is below the default start's.
     WarmStart initial_point;
+    double warm_start_floor = 1e-2;
 };
 
 struct InteriorPointResult {
@@ -138,7 +140,7 @@ struct PackedForm {
 };
 // warm: empty, or one (possibly empty) WarmStart per problem
 void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol, PackedForm& out,
-                 const std::vector<WarmStart>* warm = nullptr);
+                 const std::vector<WarmStart>* warm = nullptr, double warm_floor = 1e-2);
 std::vector<double> to_original_primal_packed(const PackedForm& pf, std::size_t i, const std::vector<double>& y);
 // y = the standard form's multipliers of the original rows mapped back, s = c - A^T y
 // (minimisation form); empty when the standard form dropped duplicate rows.

@@ -1,0 +1,95 @@
+"""GPU: the GNN warm-start kernels (hn_gnn_*) against the numpy oracle
+(oracle/gnn_oracle.py, same BF16 operand rounding, float64 accumulation),
+training on the GPU, and the trained network's prediction used as an IPM
+warm start (same status and objective as the cold solve, 1e-8)."""
+import numpy as np
+import pytest
+
+import gnn
+import gnn_oracle as GO
+import lpgen
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_norm(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+
+
+def batch_and_net(torch, lps, seed=0):
+    rng = np.random.default_rng(seed)
+    sols = [(rng.uniform(0, 2, lp["n"]), rng.standard_normal(lp["m"]), rng.uniform(0, 1, lp["n"])) for lp in lps]
+    B = gnn.Batch(lps, sols)
+    model = gnn.Model(seed=seed)
+    rp, ci, m_off, n_off = gnn.pack(lps)
+    vr, vc = zip(*(gnn.normalised_values(lp) for lp in lps))
+    Ar = GO.csr_dense(B.m, B.n, rp, ci, np.concatenate(vr))
+    Ac = GO.csr_dense(B.m, B.n, rp, ci, np.concatenate(vc))
+    net = GO.Net(gnn.layer_shapes(), model.params().astype(np.float64), Ar, Ac, B.Fv.cpu().numpy(),
+                 B.Fc.cpu().numpy(), bf16=True)
+    return B, model, net
+
+
+def test_forward_and_gradients_match_oracle(hn, torch_cuda):
+    lps = [lpgen.lp_uniform(60, 150, 6, 1), lpgen.lp_uniform(90, 225, 6, 2), lpgen.lp_uniform(35, 88, 6, 3)]
+    B, model, net = batch_and_net(torch_cuda, lps)
+    cache = gnn.forward(model, B)
+    ref = net.forward()
+    for k in ("ov", "oc"):
+        assert rel_norm(cache[k].cpu().numpy().astype(np.float64), ref[k]) <= 1e-2, k
+    for l in range(gnn.LAYERS + 1):
+        assert rel_norm(cache["hv"][l].cpu().numpy().astype(np.float64), ref["hv"][l]) <= 1e-2
+        assert rel_norm(cache["hc"][l].cpu().numpy().astype(np.float64), ref["hc"][l]) <= 1e-2
+    loss = gnn.backward(model, B, cache)
+    Tv, Tc = B.Tv.cpu().numpy().astype(np.float64), B.Tc.cpu().numpy().astype(np.float64)
+    assert abs(loss - net.loss(Tv, Tc)) <= 1e-3 * abs(net.loss(Tv, Tc))
+    g_ref = net.backward(Tv, Tc)
+    g = model.g.cpu().numpy().astype(np.float64)
+    offs, _ = gnn.param_offsets()
+    for name, (o, K) in offs.items():
+        w = slice(o, o + K * 64)
+        b = slice(o + K * 64, o + K * 64 + 64)
+        assert rel_norm(g[w], g_ref[w]) <= 3e-2, (name, rel_norm(g[w], g_ref[w]))
+        assert rel_norm(g[b], g_ref[b]) <= 3e-2, (name, rel_norm(g[b], g_ref[b]))
+
+
+def test_backward_is_deterministic(hn, torch_cuda):
+    lps = [lpgen.lp_uniform(200, 500, 6, 7)]
+    B, model, _ = batch_and_net(torch_cuda, lps)
+    out = []
+    for _ in range(2):
+        cache = gnn.forward(model, B)
+        gnn.backward(model, B, cache)
+        out.append(model.g.cpu().numpy().copy())
+    assert np.array_equal(out[0], out[1])
+
+
+def test_training_lowers_the_loss_and_warm_start_keeps_the_answer(hn, torch_cuda):
+    """Train on IPM solutions of small C0-generator LPs; the prediction for
+    held-out LPs warm-starts the IPM without changing status or objective."""
+    sizes = [int(v) for v in np.exp(np.random.default_rng(0).uniform(np.log(60), np.log(200), 40))]
+    lps = [lpgen.lp_uniform(m, int(round(2.5 * m)), 8, 50000 + i) for i, m in enumerate(sizes)]
+    r = hn.lp_solve_batch(lps)
+    assert np.all(r["status"] == 1)
+    sols = []
+    for k, lp in enumerate(lps):
+        c0, c1 = r["col_off"][k], r["col_off"][k + 1]
+        r0, r1 = r["row_off"][k], r["row_off"][k + 1]
+        sols.append((r["x"][c0:c1], r["y"][r0:r1], r["s"][c0:c1]))
+    train, held = list(range(32)), list(range(32, 40))
+    batches = [gnn.Batch([lps[i] for i in train[j:j + 8]], [sols[i] for i in train[j:j + 8]])
+               for j in range(0, 32, 8)]
+    model = gnn.Model(seed=1)
+    losses = gnn.train(model, batches, epochs=40, lr=2e-3)
+    assert losses[-1] < 0.5 * losses[0], losses[::10]
+    Bh = gnn.Batch([lps[i] for i in held])
+    preds = gnn.predict(model, Bh)
+    used = 0
+    for k, i in enumerate(held):
+        x, y, s = preds[k]
+        w = hn.lp_solve(lps[i], x0=x, y0=y, s0=s)
+        cold = hn.lp_solve(lps[i])
+        used += int(w["warm_start_used"])
+        assert w["status"] == cold["status"] == 1
+        assert abs(w["objective"] - cold["objective"]) <= 1e-8 * (1 + abs(cold["objective"]))
+    assert used >= 1
