@@ -46,6 +46,7 @@ extern "C" {
 
 /* ---- hn_csr_create flags ---- */
 #define HN_CSR_NO_TRANSPOSE 1u /* do not build the device A^T */
+#define HN_CSR_NO_AUTOTUNE 2u  /* keep the merge-path SpMV without timing the alternatives */
 
 typedef struct hn_csr hn_csr;         /* device-resident CSR matrix (+ its A^T) */
 typedef struct hn_pattern hn_pattern; /* fixed pattern of A diag(d) A^T + reg I */
@@ -114,6 +115,19 @@ int hn_csr_shape(const hn_csr* A, int64_t* m, int64_t* n, int64_t* nnz, int64_t*
 int hn_csr_export(const hn_csr* A, int trans, uint64_t* rp_host, uint64_t* ci_host,
                   double* val_host);
 /* Merge-path tile table (row binning) of A or A^T: ntiles+1 coordinates. */
+/* SpMV path of a direction (trans 0: A, 1: A^T). HN_SPMV_MERGE: merge-path
+ * tiles (the default, any row-length distribution). HN_SPMV_BINNED: rows
+ * grouped by length, a group of 2^k lanes per row sized for about t nonzeros
+ * per lane. hn_csr_create times both (t = 4, 8, 16) on matrices with >= 2^20
+ * nonzeros per direction and keeps the binned kernel when it is >= 5 % faster
+ * (unless HN_CSR_NO_AUTOTUNE). Both sum each row in a fixed order; they
+ * differ from each other by rounding only. This is the reference's row binning
+ * (one kernel per matrix chosen by mean row length, gpu_backend.cpp:413-415)
+ * made per matrix and measured. */
+#define HN_SPMV_MERGE 0
+#define HN_SPMV_BINNED 1
+int hn_csr_spmv_kind(const hn_csr* A, int trans, int* kind, int* t);
+int hn_csr_set_spmv_kind(hn_csr* A, int trans, int kind, int t);
 int hn_csr_tiles(const hn_csr* A, int trans, int64_t* ntiles, int64_t* items_per_tile);
 int hn_csr_export_tiles(const hn_csr* A, int trans, int32_t* tile_row_host,
                         int32_t* tile_nz_host);

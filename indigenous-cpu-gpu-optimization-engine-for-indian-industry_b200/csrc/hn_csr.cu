@@ -222,6 +222,8 @@ void free_transpose(hn_csr* A) {
         nullptr;
     A->valT = A->carry_val_t = A->head_val_t = nullptr;
     A->has_t = false;
+    dfree(A->perm[1]);
+    A->perm[1] = nullptr;
 }
 
 void build_transpose(hn_csr* A, cudaStream_t s) {
@@ -332,6 +334,7 @@ void build_transpose(hn_csr* A, cudaStream_t s) {
 void free_csr(hn_csr* A) {
     if (!A) return;
     free_transpose(A);
+    dfree(A->perm[0]);
     dfree(A->rp);
     dfree(A->ci);
     dfree(A->val);
@@ -346,6 +349,127 @@ void free_csr(hn_csr* A) {
 
 // Host-side validation + int32 conversion. Every index the kernels will use
 // is checked here, so no launch can read out of bounds.
+// ---- SpMV path choice ----
+
+// Bins of the vector kernel for a target of t nonzeros per lane: a row of
+// length L gets the smallest group G = 2^lg (lg <= 5) with G * t >= L.
+void make_bins(const std::vector<int32_t>& rp, int t, std::vector<int32_t>& perm, SpmvBins& b) {
+    const int64_t rows = static_cast<int64_t>(rp.size()) - 1;
+    std::vector<int8_t> lg(rows);
+    int64_t cnt[kSpmvMaxBins] = {};
+    for (int64_t i = 0; i < rows; ++i) {
+        const int64_t L = rp[i + 1] - rp[i], q = (L + t - 1) / t;
+        int g = 0;
+        while ((int64_t(1) << g) < q && g < kSpmvMaxBins - 1) ++g;
+        lg[i] = static_cast<int8_t>(g);
+        ++cnt[g];
+    }
+    perm.clear();
+    perm.reserve(rows);
+    b = SpmvBins{};
+    int64_t uo = 0, ro = 0;
+    int nb = 0;
+    for (int g = 0; g < kSpmvMaxBins; ++g) {
+        if (!cnt[g]) continue;
+        b.lg[nb] = g;
+        b.unit_off[nb] = static_cast<int>(uo);
+        b.row_off[nb] = static_cast<int>(ro);
+        for (int64_t i = 0; i < rows; ++i)
+            if (lg[i] == g) perm.push_back(static_cast<int32_t>(i));
+        const int64_t rpw = 32 >> g;
+        uo += (cnt[g] + rpw - 1) / rpw;
+        ro += cnt[g];
+        ++nb;
+    }
+    if (uo * 32 >= INT32_MAX) fail(HN_ERR_UNSUPPORTED, "too many rows for the vector SpMV");
+    b.nbins = nb;
+    b.unit_off[nb] = static_cast<int>(uo);
+    b.row_off[nb] = static_cast<int>(ro);
+}
+
+std::vector<int32_t> host_rows(const hn_csr* A, int d) {
+    const int64_t rows = d ? A->n : A->m;
+    std::vector<int32_t> rp(rows + 1);
+    check_cuda(cudaMemcpy(rp.data(), d ? A->rpT : A->rp, sizeof(int32_t) * (rows + 1), cudaMemcpyDeviceToHost),
+               "D2H rp");
+    return rp;
+}
+
+void set_spmv_path(hn_csr* A, int d, int kind, int t) {
+    dfree(A->perm[d]);
+    A->perm[d] = nullptr;
+    A->spmv_kind[d] = HN_SPMV_MERGE;
+    A->spmv_t[d] = 0;
+    if (kind != HN_SPMV_BINNED) return;
+    std::vector<int32_t> perm;
+    SpmvBins b;
+    make_bins(host_rows(A, d), t, perm, b);
+    A->perm[d] = dmalloc<int32_t>(perm.size());
+    if (!perm.empty())
+        check_cuda(cudaMemcpy(A->perm[d], perm.data(), sizeof(int32_t) * perm.size(), cudaMemcpyHostToDevice),
+                   "H2D perm");
+    A->bins[d] = b;
+    A->spmv_kind[d] = HN_SPMV_BINNED;
+    A->spmv_t[d] = t;
+}
+
+// The autotuner: for each direction, times the merge-path kernel and the
+// binned vector kernel at t = 4, 8, 16 nonzeros per lane (three launches
+// each after one warm-up, best of three, CUDA events) and keeps the binned
+// kernel only when it is at least 5 % faster, so close calls stay on the
+// merge path. Small matrices (< 2^20 nonzeros) keep the merge path untimed.
+constexpr int64_t kAutotuneMinNnz = int64_t(1) << 20;
+void autotune(hn_csr* A, cudaStream_t s) {
+    for (int d = 0; d < (A->has_t ? 2 : 1); ++d) {
+        const int64_t rows = d ? A->n : A->m, cols = d ? A->m : A->n;
+        if ((d ? A->nnz_t : A->nnz) < kAutotuneMinNnz) continue;
+        double* x = dmalloc<double>(cols);
+        double* y = dmalloc<double>(rows);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        try {
+            check_cuda(cudaMemsetAsync(x, 0, sizeof(double) * cols, s), "memset");
+            check_cuda(cudaEventCreate(&e0), "event");
+            check_cuda(cudaEventCreate(&e1), "event");
+            auto time_path = [&]() {
+                const SpmvMat M = spmv_mat(A, d);
+                spmv_launch(M, x, EpiAxpby{1.0, 0.0, y}, s);
+                float best = 1e30f;
+                for (int rep = 0; rep < 3; ++rep) {
+                    check_cuda(cudaEventRecord(e0, s), "event");
+                    spmv_launch(M, x, EpiAxpby{1.0, 0.0, y}, s);
+                    check_cuda(cudaEventRecord(e1, s), "event");
+                    check_cuda(cudaEventSynchronize(e1), "event sync");
+                    float ms = 0.f;
+                    check_cuda(cudaEventElapsedTime(&ms, e0, e1), "event time");
+                    best = std::min(best, ms);
+                }
+                return best;
+            };
+            float best = time_path();
+            int best_t = 0;
+            for (int t : {4, 8, 16}) {
+                set_spmv_path(A, d, HN_SPMV_BINNED, t);
+                const float ms = time_path();
+                if (ms < 0.95f * best) {
+                    best = ms;
+                    best_t = t;
+                }
+            }
+            set_spmv_path(A, d, best_t ? HN_SPMV_BINNED : HN_SPMV_MERGE, best_t);
+        } catch (...) {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            dfree(x);
+            dfree(y);
+            throw;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        dfree(x);
+        dfree(y);
+    }
+}
+
 void convert_csr(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci,
                  std::vector<int32_t>& rp32, std::vector<int32_t>& ci32) {
     if (m < 0 || n < 0) fail(HN_ERR_INVALID_ARG, "negative dimension");
@@ -414,6 +538,7 @@ int hn_csr_create(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, 
                         A->head_row, A->head_val, s);
             if (!(flags & HN_CSR_NO_TRANSPOSE)) build_transpose(A, s);
             check_cuda(cudaStreamSynchronize(s), "hn_csr_create sync");
+            if (!(flags & HN_CSR_NO_AUTOTUNE)) autotune(A, s);
         } catch (...) {
             free_csr(A);
             throw;
@@ -431,9 +556,11 @@ int hn_csr_set_values(hn_csr* A, const double* val) {
             check_cuda(cudaMemcpy(A->val, val, sizeof(double) * A->nnz, cudaMemcpyHostToDevice),
                        "H2D values");
         if (A->has_t) {
-            // exact-zero dropping depends on the values: rebuild A^T
+            // exact-zero dropping depends on the values: rebuild A^T (and its bins)
+            const int kind = A->spmv_kind[1], t = A->spmv_t[1];
             free_transpose(A);
             build_transpose(A, nullptr);
+            set_spmv_path(A, 1, kind, t);
         }
     });
 }
@@ -481,6 +608,28 @@ int hn_csr_export(const hn_csr* A, int trans, uint64_t* rp, uint64_t* ci, double
             for (int64_t i = 0; i <= rows; ++i) rp[i] = static_cast<uint64_t>(r[i]);
         if (ci)
             for (int64_t k = 0; k < nnz; ++k) ci[k] = static_cast<uint64_t>(c[k]);
+    });
+}
+
+int hn_csr_spmv_kind(const hn_csr* A, int trans, int* kind, int* t) {
+    return guard("hn_csr_spmv_kind", [&] {
+        if (!A) fail(HN_ERR_INVALID_ARG, "null handle");
+        if (trans && !A->has_t) fail(HN_ERR_INVALID_ARG, "handle was created without A^T");
+        const int d = trans ? 1 : 0;
+        if (kind) *kind = A->spmv_kind[d];
+        if (t) *t = A->spmv_t[d];
+    });
+}
+
+int hn_csr_set_spmv_kind(hn_csr* A, int trans, int kind, int t) {
+    return guard("hn_csr_set_spmv_kind", [&] {
+        require_init();
+        if (!A) fail(HN_ERR_INVALID_ARG, "null handle");
+        if (trans && !A->has_t) fail(HN_ERR_INVALID_ARG, "handle was created without A^T");
+        if (kind != HN_SPMV_MERGE && kind != HN_SPMV_BINNED) fail(HN_ERR_INVALID_ARG, "unknown SpMV kind");
+        if (kind == HN_SPMV_BINNED && (t < 1 || t > 64)) fail(HN_ERR_INVALID_ARG, "t must be in [1, 64]");
+        check_cuda(cudaDeviceSynchronize(), "sync before changing the SpMV path");
+        set_spmv_path(A, trans ? 1 : 0, kind, t);
     });
 }
 

@@ -269,6 +269,17 @@ int guard(const char* name, F&& body) {
 }  // namespace hn
 
 // ---------------------------------------------------------------- objects
+// Row-length bins of the vector SpMV: bin b holds rows whose group of
+// 2^lg[b] lanes takes about `t` nonzeros per lane; perm lists the rows bin by
+// bin (ascending within a bin); a warp handles 32 / 2^lg rows of one bin.
+constexpr int kSpmvMaxBins = 6;
+struct SpmvBins {
+    int nbins = 0;
+    int unit_off[kSpmvMaxBins + 1] = {};  // first warp of each bin
+    int row_off[kSpmvMaxBins + 1] = {};   // first perm entry of each bin
+    int lg[kSpmvMaxBins] = {};
+};
+
 struct hn_csr {
     int64_t m = 0, n = 0, nnz = 0;
     // A (int32 indices, padded by one slot so empty matrices have storage)
@@ -298,6 +309,12 @@ struct hn_csr {
     double* carry_val_t = nullptr;
     int32_t* head_row_t = nullptr;
     double* head_val_t = nullptr;
+    // SpMV path per direction (0: A, 1: A^T): HN_SPMV_MERGE or HN_SPMV_BINNED
+    // (with its target nonzeros per lane, row permutation and bins)
+    int spmv_kind[2] = {0, 0};
+    int spmv_t[2] = {0, 0};
+    int32_t* perm[2] = {nullptr, nullptr};
+    SpmvBins bins[2];
 };
 
 struct hn_pattern {

@@ -41,6 +41,9 @@ struct SpmvMat {
     int32_t* head_row;
     double* head_val;
     int64_t ntiles;
+    int kind = 0;  // 0: merge path; 1: binned vector CSR
+    const int32_t* perm = nullptr;
+    SpmvBins bins = {};
 };
 
 inline SpmvMat spmv_mat(const hn_csr* A, int trans) {
@@ -51,6 +54,12 @@ inline SpmvMat spmv_mat(const hn_csr* A, int trans) {
     } else {
         M = SpmvMat{(int)A->n, (int)A->nnz_t, A->rpT, A->ciT, A->valT, A->tile_row_t, A->tile_nz_t,
                     A->carry_row_t, A->carry_val_t, A->head_row_t, A->head_val_t, A->ntiles_t};
+    }
+    const int d = trans ? 1 : 0;
+    if (A->spmv_kind[d] == 1 && A->perm[d]) {
+        M.kind = 1;
+        M.perm = A->perm[d];
+        M.bins = A->bins[d];
     }
     return M;
 }
@@ -116,7 +125,7 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_tile_kernel(SpmvMat a, cons
 #pragma unroll
         for (int u = 0; u < kSpmvIpt; ++u) w[u] = (u < cnt) ? __ldg(a.val + k0 + nz + u) : 0.0;
 #pragma unroll
-        for (int u = 0; u < kSpmvIpt; ++u) v[u] = (u < cnt) ? w[u] * __ldg(x + c[u]) : 0.0;
+        for (int u = 0; u < kSpmvIpt; ++u) v[u] = (u < cnt) ? w[u] * __ldcg(x + c[u]) : 0.0;
     }
 
     double sum = 0.0;
@@ -189,9 +198,73 @@ __global__ void spmv_fixup_kernel(SpmvMat a, Epi epi) {
     epi(r, acc);
 }
 
-// Launches the two kernels of one product on `s`.
+// ---- binned vector CSR ----
+// A group of G lanes sums one row: lane l takes the row's nonzeros l, l + G,
+// ... in order (kVecUnroll loads in flight), then the group combines its
+// lanes by a fixed shuffle tree; every row's association order is fixed, so
+// results are deterministic. Rows are grouped by G (bins); one launch covers
+// all bins.
+constexpr int kVecUnroll = 4;
+
+template <int G, class Epi>
+__device__ __forceinline__ void vec_rows(const SpmvMat& a, int bin, int unit, const double* __restrict__ x,
+                                         const Epi& epi) {
+    const int lane = threadIdx.x & 31, sub = lane / G, l = lane % G;
+    const int idx = a.bins.row_off[bin] + unit * (32 / G) + sub;
+    const bool valid = idx < a.bins.row_off[bin + 1];
+    const int r = valid ? a.perm[idx] : 0;
+    const int k0 = valid ? __ldg(a.rp + r) : 0, k1 = valid ? __ldg(a.rp + r + 1) : 0;
+    double sum = 0.0;
+    for (int k = k0 + l; k < k1; k += kVecUnroll * G) {
+        int c[kVecUnroll];
+        double w[kVecUnroll];
+#pragma unroll
+        for (int u = 0; u < kVecUnroll; ++u) {
+            const int kk = k + u * G;
+            c[u] = kk < k1 ? __ldg(a.ci + kk) : 0;
+            w[u] = kk < k1 ? __ldg(a.val + kk) : 0.0;
+        }
+        double p[kVecUnroll];
+#pragma unroll
+        for (int u = 0; u < kVecUnroll; ++u) p[u] = (k + u * G < k1) ? w[u] * __ldcg(x + c[u]) : 0.0;
+#pragma unroll
+        for (int u = 0; u < kVecUnroll; ++u)
+            if (k + u * G < k1) sum += p[u];
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o, G);
+    if (valid && l == 0) epi(r, sum);
+}
+
+template <class Epi>
+__global__ void __launch_bounds__(kSpmvThreads) spmv_vec_kernel(SpmvMat a, const double* __restrict__ x, Epi epi) {
+    const int w = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    if (w >= a.bins.unit_off[a.bins.nbins]) return;  // whole warps leave together
+    int bin = 0;
+    while (w >= a.bins.unit_off[bin + 1]) ++bin;
+    const int unit = w - a.bins.unit_off[bin];
+    switch (a.bins.lg[bin]) {
+        case 0: vec_rows<1>(a, bin, unit, x, epi); break;
+        case 1: vec_rows<2>(a, bin, unit, x, epi); break;
+        case 2: vec_rows<4>(a, bin, unit, x, epi); break;
+        case 3: vec_rows<8>(a, bin, unit, x, epi); break;
+        case 4: vec_rows<16>(a, bin, unit, x, epi); break;
+        default: vec_rows<32>(a, bin, unit, x, epi); break;
+    }
+}
+
+// Launches one product on `s`: the binned vector kernel, or the merge-path
+// tile kernel and its fix-up.
 template <class Epi>
 void spmv_launch(const SpmvMat& M, const double* x, const Epi& epi, cudaStream_t s) {
+    if (M.kind == 1) {
+        const int64_t units = M.bins.unit_off[M.bins.nbins];
+        if (units == 0) return;
+        spmv_vec_kernel<Epi><<<(unsigned)((units * 32 + kSpmvThreads - 1) / kSpmvThreads), kSpmvThreads, 0, s>>>(
+            M, x, epi);
+        launched("spmv_vec_kernel");
+        return;
+    }
     if (M.ntiles == 0) return;
     spmv_tile_kernel<Epi><<<(unsigned)M.ntiles, kSpmvThreads, 0, s>>>(M, x, epi);
     launched("spmv_tile_kernel");

@@ -24,6 +24,8 @@ HN_ERR_NOT_INITIALIZED = 4
 HN_ERR_UNSUPPORTED = 5
 HN_ERR_NUMERICAL = 6
 HN_ERR_INJECTED = 7
+HN_CSR_NO_AUTOTUNE = 2
+SPMV_MERGE, SPMV_BINNED = 0, 1
 HN_CSR_NO_TRANSPOSE = 1
 
 _i64, _u64p, _f64p, _vp, _i32p = C.c_int64, C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_int32)
@@ -89,6 +91,8 @@ SIGNATURES = {
     "hn_ipm_update": [_i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "hn_max_step": [_i64, _vp, _vp, _vp, _vp],
     "hn_spmv_noalloc": [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp],
+    "hn_csr_spmv_kind": [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "hn_csr_set_spmv_kind": [_vp, C.c_int, C.c_int, C.c_int],
     "hn_price_reduced_costs": [_vp, _vp, _vp, _vp, _vp],
     "hn_price_devex_update": [_vp, _vp, _vp, _vp, _vp, _vp],
     "hn_price_select": [_i64, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_double, C.c_int, _i64, _vp, _vp],
@@ -184,17 +188,26 @@ def _ptr(t) -> int | None:
 class Csr:
     """Device-resident CSR matrix handle (hn_csr)."""
 
-    def __init__(self, m: int, n: int, rp, ci, val, transpose: bool = True):
+    def __init__(self, m: int, n: int, rp, ci, val, transpose: bool = True, autotune: bool = True):
         self.m, self.n = int(m), int(n)
         self._rp, self._ci, self._val = u64(rp), u64(ci), f64(val)
         h = C.c_void_p()
-        flags = 0 if transpose else HN_CSR_NO_TRANSPOSE
+        flags = (0 if transpose else HN_CSR_NO_TRANSPOSE) | (0 if autotune else HN_CSR_NO_AUTOTUNE)
         check(load().hn_csr_create(self.m, self.n, _p(self._rp, C.c_uint64), _p(self._ci, C.c_uint64),
                                    _p(self._val, C.c_double), flags, C.byref(h)))
         self.h = h
         m_, n_, nnz, nnzt = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
         check(load().hn_csr_shape(h, C.byref(m_), C.byref(n_), C.byref(nnz), C.byref(nnzt)))
         self.nnz, self.nnz_t = nnz.value, nnzt.value
+
+    def spmv_kind(self, trans: int = 0):
+        """(kind, t): 0 merge path, 1 binned vector kernel with t nonzeros per lane."""
+        k, t = C.c_int(), C.c_int()
+        check(load().hn_csr_spmv_kind(self.h, trans, C.byref(k), C.byref(t)))
+        return k.value, t.value
+
+    def set_spmv_kind(self, kind: int, t: int = 8, trans: int = 0) -> None:
+        check(load().hn_csr_set_spmv_kind(self.h, trans, kind, t))
 
     def set_values(self, val) -> None:
         self._val = f64(val)
