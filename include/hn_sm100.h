@@ -140,6 +140,10 @@ int hn_csr_export_tiles(const hn_csr* A, int trans, int32_t* tile_row_host,
  * (sparse_matrix.cpp:161-184, interior_point.cpp:61-69). */
 int hn_spmv(const hn_csr* A, int trans, double alpha, const double* x_dev, double beta,
             double* y_dev, void* stream);
+/* y = op(A) x - b in one pass (the IPM's primal residual rp = M x - b,
+ * interior_point.cpp:512); y may not alias b. */
+int hn_spmv_residual(const hn_csr* A, int trans, const double* x_dev, const double* b_dev, double* y_dev,
+                     void* stream);
 /* Same product with host vectors, synchronous: copies x in and y out through
  * pinned staging (IComputeBackend::spmv's calling convention). */
 int hn_spmv_host(const hn_csr* A, int trans, const double* x_host, double* y_host);

@@ -59,6 +59,10 @@ struct hn_batch {
     std::vector<int64_t> step_pairs_h;   // host, total pairs per step
     std::vector<int64_t> pair_off_h;     // host, nsteps+1 offsets into step_pairs
     int64_t* step_pairs = nullptr;       // device, cumulative pairs per (step, instance)
+    // panel rows below each instance's diagonal block, in chunks of kT rows
+    std::vector<int64_t> step_chunks_h;  // host, total chunks per step
+    std::vector<int64_t> chunk_off_h;    // host, nsteps+1 offsets into step_chunks
+    int64_t* step_chunks = nullptr;      // device, cumulative chunks per (step, instance)
 };
 
 namespace hn {
@@ -264,9 +268,10 @@ __global__ void batch_dense_kernel(int64_t m, const int64_t* __restrict__ row_of
 // Blocked right-looking LDL^T, level-synchronous over the batch, in blocks of
 // kFb columns: block step s runs two launches for every instance that still
 // has a block s --
-//   batch_ldlt_panel_kernel: one CTA per instance factorises the kFb x kFb
-//     diagonal block (pivot clamp of factorization.cpp:1299-1305) and solves
-//     the panel below it, one row per thread;
+//   batch_ldlt_diag_kernel: one CTA per instance factorises the kFb x kFb
+//     diagonal block (pivot clamp of factorization.cpp:1299-1305);
+//   batch_ldlt_panel_kernel: every instance's panel below its diagonal block,
+//     in chunks of kT rows spread over the GPU, one row per thread;
 //   batch_ldlt_update_kernel: all instances' trailing kFb x kFb tiles
 //     A_rc -= sum_q (L_rq D_q) L_cq, spread over every CTA of the GPU, each
 //     thread accumulating a 4 x 4 block of the tile in registers.
@@ -275,12 +280,12 @@ constexpr int kFbP = kFb + 1;  // padded smem row (conflict-free column walks)
 constexpr size_t kPanelSmem = sizeof(double) * (kFb * kFbP + kFb);
 constexpr size_t kUpdateSmem = sizeof(double) * 2 * kFb * kFbP;
 
-__global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, const int64_t* __restrict__ row_off,
-                                                              const int64_t* __restrict__ dn_off,
-                                                              const int32_t* __restrict__ order,
-                                                              const int32_t* __restrict__ status,
-                                                              double* __restrict__ dense, double* __restrict__ dD,
-                                                              double tol) {
+__global__ void __launch_bounds__(kT) batch_ldlt_diag_kernel(int s, const int64_t* __restrict__ row_off,
+                                                             const int64_t* __restrict__ dn_off,
+                                                             const int32_t* __restrict__ order,
+                                                             const int32_t* __restrict__ status,
+                                                             double* __restrict__ dense, double* __restrict__ dD,
+                                                             double tol) {
     extern __shared__ double smem[];
     double(*sA)[kFbP] = reinterpret_cast<double(*)[kFbP]>(smem);
     double* sD = smem + kFb * kFbP;
@@ -291,7 +296,7 @@ __global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, const int64
     const int m = static_cast<int>(row_off[inst + 1] - r0);
     const int k0 = s * kFb;
     if (k0 >= m) return;
-    const int nb = min(kFb, m - k0), k1 = k0 + nb;
+    const int nb = min(kFb, m - k0);
     double* A = dense + dn_off[inst];
     for (int idx = tid; idx < kFb * kFb; idx += kT) {
         const int r = idx / kFb, c = idx % kFb;
@@ -319,25 +324,61 @@ __global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, const int64
         if (c < r) A[(int64_t)(k0 + r) * m + k0 + c] = sA[r][c];
     }
     if (tid < nb) dD[r0 + k0 + tid] = sD[tid];
-    // panel below: L[r, k0:k1] = A[r, k0:k1] (L_blk D)^-T
-    for (int r = k1 + tid; r < m; r += kT) {
-        double lv[kFb];
-        double* Ar = A + (int64_t)r * m + k0;
-#pragma unroll
-        for (int c = 0; c < kFb; ++c) lv[c] = (c < nb) ? Ar[c] : 0.0;
-#pragma unroll
-        for (int c = 0; c < kFb; ++c) {
-            if (c < nb) {
-                double v = lv[c];
-#pragma unroll
-                for (int q = 0; q < c; ++q) v -= (lv[q] * sD[q]) * sA[c][q];
-                lv[c] = v / sD[c];
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < kFb; ++c)
-            if (c < nb) Ar[c] = lv[c];
+}
+
+// L[r, k0:k1] = A[r, k0:k1] (L_blk D)^-T for the kT rows of chunk `local`
+// of one instance's panel (the instance: first b with chunks[b] > chunk).
+__global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, int cnt, const int64_t* __restrict__ chunks,
+                                                              const int64_t* __restrict__ row_off,
+                                                              const int64_t* __restrict__ dn_off,
+                                                              const int32_t* __restrict__ order,
+                                                              const int32_t* __restrict__ status,
+                                                              double* __restrict__ dense,
+                                                              const double* __restrict__ dD) {
+    __shared__ double sL[kFb][kFbP];
+    __shared__ double sD[kFb];
+    const int tid = threadIdx.x;
+    const int64_t chunk = blockIdx.x;
+    int lo = 0, hi = cnt - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (chunks[mid] <= chunk)
+            lo = mid + 1;
+        else
+            hi = mid;
     }
+    const int inst = order[lo];
+    if (status[inst] != ST_RUN) return;
+    const int64_t local = chunk - (lo > 0 ? chunks[lo - 1] : 0);
+    const int64_t r0 = row_off[inst];
+    const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int k0 = s * kFb;
+    const int nb = min(kFb, m - k0), k1 = k0 + nb;
+    double* A = dense + dn_off[inst];
+    for (int idx = tid; idx < kFb * kFb; idx += kT) {
+        const int r = idx / kFb, c = idx % kFb;
+        sL[r][c] = (r < nb && c < r) ? A[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
+    }
+    if (tid < kFb) sD[tid] = tid < nb ? dD[r0 + k0 + tid] : 1.0;
+    __syncthreads();
+    const int r = k1 + static_cast<int>(local) * kT + tid;
+    if (r >= m) return;
+    double lv[kFb];
+    double* Ar = A + (int64_t)r * m + k0;
+#pragma unroll
+    for (int c = 0; c < kFb; ++c) lv[c] = (c < nb) ? Ar[c] : 0.0;
+#pragma unroll
+    for (int c = 0; c < kFb; ++c) {
+        if (c < nb) {
+            double v = lv[c];
+#pragma unroll
+            for (int q = 0; q < c; ++q) v -= (lv[q] * sD[q]) * sL[c][q];
+            lv[c] = v / sD[c];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kFb; ++c)
+        if (c < nb) Ar[c] = lv[c];
 }
 
 __global__ void __launch_bounds__(kT) batch_ldlt_update_kernel(int s, int cnt, int64_t npairs,
@@ -579,7 +620,7 @@ void free_batch(hn_batch* B) {
     for (void* p : {(void*)B->row_off, (void*)B->col_off, (void*)B->row_inst, (void*)B->dn_off, (void*)B->order,
                     (void*)B->dense, (void*)B->dD, (void*)B->ticket, (void*)B->refine, (void*)B->nref, (void*)B->nrp,
                     (void*)B->tile_row, (void*)B->tile_nz, (void*)B->carry_row, (void*)B->head_row,
-                    (void*)B->carry_val, (void*)B->head_val, (void*)B->r, (void*)B->ax, (void*)B->step_pairs})
+                    (void*)B->carry_val, (void*)B->head_val, (void*)B->r, (void*)B->ax, (void*)B->step_pairs, (void*)B->step_chunks})
         dfree(p);
     delete B;
 }
@@ -663,10 +704,11 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
             const int64_t mmax = row_off_host[order[0] + 1] - row_off_host[order[0]];
             B->nsteps = (mmax + kFb - 1) / kFb;
             B->pair_off_h.assign(1, 0);
-            std::vector<int64_t> flat;
+            B->chunk_off_h.assign(1, 0);
+            std::vector<int64_t> flat, cflat;
             for (int64_t st = 0; st < B->nsteps; ++st) {
                 int32_t cnt = 0;
-                int64_t acc = 0;
+                int64_t acc = 0, cacc = 0;
                 for (int64_t b = 0; b < K; ++b) {
                     const int64_t mi = row_off_host[order[b] + 1] - row_off_host[order[b]];
                     if (mi <= st * kFb) break;
@@ -674,13 +716,21 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
                     const int64_t T = (rest + kFb - 1) / kFb;
                     acc += T * (T + 1) / 2;
                     flat.push_back(acc);
+                    cacc += (rest + kT - 1) / kT;
+                    cflat.push_back(cacc);
                     ++cnt;
                 }
                 B->step_cnt.push_back(cnt);
                 B->step_pairs_h.push_back(acc);
                 B->pair_off_h.push_back((int64_t)flat.size());
+                B->step_chunks_h.push_back(cacc);
+                B->chunk_off_h.push_back((int64_t)cflat.size());
             }
             B->step_pairs = dmalloc<int64_t>(flat.size());
+            B->step_chunks = dmalloc<int64_t>(cflat.size());
+            check_cuda(cudaMemcpy(B->step_chunks, cflat.data(), sizeof(int64_t) * cflat.size(),
+                                  cudaMemcpyHostToDevice),
+                       "H2D chunks");
             check_cuda(cudaFuncSetAttribute(batch_ldlt_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)kUpdateSmem),
                        "update kernel smem");
@@ -734,9 +784,16 @@ int hn_batch_factor(hn_batch* B, const double* D, double reg, double singular_to
         launched("batch_dense_kernel");
         for (int64_t st = 0; st < B->nsteps; ++st) {
             const int cnt = B->step_cnt[st];
-            batch_ldlt_panel_kernel<<<cnt, kT, kPanelSmem, s>>>((int)st, B->row_off, B->dn_off, B->order, status, B->dense,
-                                                       B->dD, singular_tol);
-            launched("batch_ldlt_panel_kernel");
+            batch_ldlt_diag_kernel<<<cnt, kT, kPanelSmem, s>>>((int)st, B->row_off, B->dn_off, B->order, status,
+                                                               B->dense, B->dD, singular_tol);
+            launched("batch_ldlt_diag_kernel");
+            const int64_t nc = B->step_chunks_h[st];
+            if (nc > 0) {
+                batch_ldlt_panel_kernel<<<(unsigned)nc, kT, 0, s>>>((int)st, cnt, B->step_chunks + B->chunk_off_h[st],
+                                                                    B->row_off, B->dn_off, B->order, status,
+                                                                    B->dense, B->dD);
+                launched("batch_ldlt_panel_kernel");
+            }
             const int64_t np = B->step_pairs_h[st];
             if (np > 0) {
                 const int grid = (int)std::min<int64_t>(np, (int64_t)ctx().sm_count * 8);

@@ -74,6 +74,18 @@ int hn_spmv(const hn_csr* A, int trans, double alpha, const double* x, double be
     });
 }
 
+int hn_spmv_residual(const hn_csr* A, int trans, const double* x, const double* b, double* y, void* stream) {
+    return guard("hn_spmv_residual", [&] {
+        require_init();
+        check_handle(A, trans);
+        const SpmvMat M = spmv_mat(A, trans);
+        const int64_t cols = trans ? A->m : A->n;
+        if (M.m > 0 && (!y || !b)) fail(HN_ERR_INVALID_ARG, "null b or y");
+        if (cols > 0 && M.nnz > 0 && !x) fail(HN_ERR_INVALID_ARG, "null x");
+        spmv_launch(M, x, EpiSub{b, y}, as_stream(stream));
+    });
+}
+
 int hn_spmv_host(const hn_csr* A, int trans, const double* x, double* y) {
     return guard("hn_spmv_host", [&] {
         require_init();

@@ -283,6 +283,13 @@ struct EpiAxpby {
     }
 };
 
+// y = s - b (a residual op(A) x - b in one pass)
+struct EpiSub {
+    const double* b;
+    double* y;
+    __device__ __forceinline__ void operator()(int r, double s) const { y[r] = s - b[r]; }
+};
+
 // IPM epilogues (core/lp/interior_point.cpp line numbers in hn_ipm.cu)
 struct EpiResidual {
     const double* b;

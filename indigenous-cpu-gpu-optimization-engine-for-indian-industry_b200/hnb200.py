@@ -92,6 +92,7 @@ SIGNATURES = {
     "hn_max_step": [_i64, _vp, _vp, _vp, _vp],
     "hn_spmv_noalloc": [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp],
     "hn_csr_spmv_kind": [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "hn_spmv_residual": [_vp, C.c_int, _vp, _vp, _vp, _vp],
     "hn_csr_set_spmv_kind": [_vp, C.c_int, C.c_int, C.c_int],
     "hn_price_reduced_costs": [_vp, _vp, _vp, _vp, _vp],
     "hn_price_devex_update": [_vp, _vp, _vp, _vp, _vp, _vp],
@@ -231,6 +232,10 @@ class Csr:
 
     def spmv(self, x, y, trans: int = 0, alpha: float = 1.0, beta: float = 0.0, stream=None) -> None:
         check(load().hn_spmv(self.h, trans, alpha, _ptr(x), beta, _ptr(y), _ptr(stream)))
+
+    def residual(self, x, b, y, trans: int = 0, stream=None) -> None:
+        """y = op(A) x - b."""
+        check(load().hn_spmv_residual(self.h, trans, _ptr(x), _ptr(b), _ptr(y), _ptr(stream)))
 
     def spmv_host(self, x, trans: int = 0) -> np.ndarray:
         x = f64(x)

@@ -53,6 +53,12 @@ def test_paths_match_oracle_on_ragged_rows(hn, torch_cuda, kind, t):
     A.spmv(dev(torch_cuda, lam), t_, trans=1)
     rpT, ciT, valT = O.transposed(rp, ci, val, n)
     assert normwise_ok(t_.cpu().numpy(), O.tmultiply(rp, ci, val, lam, n), rpT, ciT, valT, lam)
+    # residual y = A x - b
+    bb = rng.standard_normal(m)
+    yr = torch_cuda.full((m,), float("nan"), dtype=torch_cuda.float64, device="cuda")
+    A.residual(dev(torch_cuda, x), dev(torch_cuda, bb), yr)
+    ref = O.multiply(rp, ci, val, x) - bb
+    assert np.all(np.abs(yr.cpu().numpy() - ref) <= 1e-12 * O.multiply(rp, ci, np.abs(val), np.abs(x)) + 1e-16 * np.abs(bb))
     # alpha/beta epilogue
     y0 = rng.standard_normal(m)
     yd = dev(torch_cuda, y0)
