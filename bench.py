@@ -243,6 +243,9 @@ def run_ours(args, rank, world, local):
     h2d = 8 * (3 * n + m)
     d2h = 8 * (m + n) + 64
 
+    # the batched IPM runs on every rank (sharded when there are several)
+    batch_result = None if args.no_batch else batched_ipm(args.batch_k, args.batch_sample, rank, world)
+
     result = None
     if rank == 0:
         hbm, how = peaks()
@@ -268,8 +271,8 @@ def run_ours(args, rank, world, local):
         }
         if not args.no_ipm:
             result["plain_ipm"] = plain_ipm()
-        if not args.no_batch:
-            result["batched_ipm"] = batched_ipm(args.batch_k, args.batch_sample)
+        if batch_result is not None:
+            result["batched_ipm"] = batch_result
         if not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(lp, vec, threads=os.cpu_count() or 1, reps=1)
     return result
@@ -298,21 +301,41 @@ def plain_ipm():
     return out
 
 
-def batched_ipm(K: int, sample_per_stratum: int = 4):
+def batched_ipm(K: int, sample_per_stratum: int = 4, rank: int = 0, world: int = 1):
     """The 4096-LP batch (m log-uniform in [50, 2000], n = round(2.5 m),
     6 nonzeros per column, seeds 20000+i) through the batched GPU IPM, and the
     plain one-at-a-time GPU IPM on a seeded stratified sample of the same
     instances (8 log-size strata), extrapolated to the batch. Wall-clock
     times with the device synchronised on both sides; both include the
     host->device copies of the LPs and the device->host copies of the
-    solutions."""
+    solutions. With several ranks the batch is sharded by LPT greedy over
+    the ranks (shard.py: no data-path collective, one gather of the results)
+    and timed as the max over ranks; the plain sample runs on rank 0."""
     import torch
 
     import hnb200 as hn
     import lpgen
+    import shard
 
     sizes = lpgen.batch_sizes(K, seed=2000)
     lps = [lpgen.lp_uniform(int(m), int(round(2.5 * m)), 6, 20000 + i) for i, m in enumerate(sizes)]
+    if world > 1:
+        torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = shard.solve_sharded(lps, hn.lp_solve_batch, rank, world)
+        torch.cuda.synchronize()
+        wall_t = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(wall_t, op=torch.distributed.ReduceOp.MAX)
+        if rank != 0:
+            return None
+        wall = float(wall_t.item())
+        st = r["status"]
+        return {"workload": f"{K} LPs, m log-uniform [50,2000], n=2.5m, 6 nnz/col (seeds 20000+i)",
+                "ranks": world, "sharding": "LPT greedy on m^3/3 + nnz, one gather of the results",
+                "instances_per_rank": [int(p.size) for p in r["parts"]], "batched_s": round(wall, 3),
+                "batched_solves_per_s": round(K / wall, 1), "optimal": int((st == 1).sum()),
+                "iterations_mean": round(float(np.mean(r["iterations"])), 2)}
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     r = hn.lp_solve_batch(lps)
