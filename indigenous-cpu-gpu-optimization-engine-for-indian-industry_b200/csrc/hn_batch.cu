@@ -15,14 +15,14 @@
 //   - the normal-equation factorisation: each instance's N block is scattered
 //     into a dense lower triangle and factorised by a blocked LDL^T on the GPU
 //     with the reference's pivot clamp (factorization.cpp:1299-1305), level-
-//     synchronously: per 32-column block step one launch factorises every
-//     instance's diagonal block and panel, one launch spreads all instances'
-//     trailing tiles over the GPU. This is a deliberate deviation from keeping
-//     factorisations on the host: thousands of factorisations per iteration
-//     do not fit in host time;
-//   - the two triangular solves and iterative refinement
-//     (refinement.cpp:7-37: up to 5 sweeps, stop at 1e-10 relative) per
-//     instance, with N x as one merge-path SpMV over the packed N.
+//     synchronously in 64-column blocks: per block one launch factorises every
+//     instance's diagonal block, one spreads all instances' panel rows and one
+//     all instances' trailing tiles over the GPU. This is a deliberate
+//     deviation from keeping factorisations on the host: thousands of
+//     factorisations per iteration do not fit in host time;
+//   - the two triangular solves, level-synchronous in the same blocks, and
+//     iterative refinement (refinement.cpp:7-37: up to 5 sweeps, stop at
+//     1e-10 relative) per instance, with N x as one SpMV over the packed N.
 #include <algorithm>
 #include <cmath>
 #include <numeric>
@@ -40,7 +40,6 @@ struct hn_batch {
     int32_t* order = nullptr;    // instances by decreasing size
     double* dense = nullptr;     // sum m_i^2
     double* dD = nullptr;        // LDL^T pivots, m
-    unsigned* ticket = nullptr;  // queue counters
     int32_t* refine = nullptr;   // per-instance refinement flag (1 = keep sweeping)
     int32_t* nref = nullptr;     // number of instances still refining
     // N as an SpMV operand (int32 row pointer copy + merge-path tables)
@@ -63,13 +62,13 @@ struct hn_batch {
     std::vector<int64_t> step_chunks_h;  // host, total chunks per step
     std::vector<int64_t> chunk_off_h;    // host, nsteps+1 offsets into step_chunks
     int64_t* step_chunks = nullptr;      // device, cumulative chunks per (step, instance)
+    double* solve_part = nullptr;        // backward-solve partial dot products, 64 per chunk
 };
 
 namespace hn {
 namespace {
 
 constexpr int kT = 256;
-constexpr int kNb = 32;
 constexpr int S_NRP = HN_IPM_NRP, S_NRD = HN_IPM_NRD, S_MU = HN_IPM_MU, S_AP = HN_IPM_AP, S_AD = HN_IPM_AD,
               S_MUAFF = HN_IPM_MUAFF, S_SIGMA = HN_IPM_SIGMA;
 constexpr int ST_RUN = 0, ST_OPTIMAL = 1, ST_NUMERICAL = 7;
@@ -458,93 +457,199 @@ __global__ void __launch_bounds__(kT) batch_ldlt_update_kernel(int s, int cnt, i
     }
 }
 
-// Solve N_i x = b in place for every instance flagged in `mask` (status
-// running and, when refine != nullptr, refine[i] != 0): L y = b, y /= D,
-// L^T x = y, blocked by 32 with warp-sequential diagonal blocks.
-__global__ void __launch_bounds__(kT) batch_solve_kernel(int64_t K, const int64_t* __restrict__ row_off,
-                                                         const int64_t* __restrict__ dn_off,
-                                                         const int32_t* __restrict__ order,
-                                                         const int32_t* __restrict__ status,
-                                                         const int32_t* __restrict__ refine,
-                                                         const double* __restrict__ dense,
-                                                         const double* __restrict__ dD, double* __restrict__ xv,
-                                                         unsigned* ticket) {
-    __shared__ double sx[kNb];
-    __shared__ double sacc[kT / 32][kNb];
-    __shared__ double sB[kNb][kNb + 1];
-    __shared__ unsigned s_item;
+// ---- batched triangular solves: N_i x = b in place, N_i = L_i D_i L_i^T ----
+// Level-synchronous in the factorisation's 64-row blocks and its schedule
+// (instances in decreasing size, panel rows in chunks of kT): per block,
+// forward: one launch solves every instance's unit-lower diagonal block,
+// one launch subtracts the block's contribution from the rows below (chunks
+// spread over the GPU, one warp per row, coalesced loads); then x /= D;
+// backward: one launch forms, per chunk, the column-block dot products of
+// L^T x over the rows below, one launch sums them in chunk order per
+// instance and solves the diagonal block. Every sum has a fixed order.
+// An instance takes part when it is iterating and, with a refine mask, still
+// refining.
+__device__ __forceinline__ bool solving(const int32_t* status, const int32_t* refine, int inst) {
+    return status[inst] == ST_RUN && (!refine || refine[inst]);
+}
+
+__device__ __forceinline__ int chunk_instance(const int64_t* chunks, int cnt, int64_t chunk) {
+    int lo = 0, hi = cnt - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (chunks[mid] <= chunk)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kFb) batch_fwd_diag_kernel(int s, const int64_t* __restrict__ row_off,
+                                                            const int64_t* __restrict__ dn_off,
+                                                            const int32_t* __restrict__ order,
+                                                            const int32_t* __restrict__ status,
+                                                            const int32_t* __restrict__ refine,
+                                                            const double* __restrict__ dense, double* __restrict__ xv) {
+    __shared__ double sL[kFb][kFbP];
+    __shared__ double sy[kFb];
+    const int inst = order[blockIdx.x];
+    if (!solving(status, refine, inst)) return;
+    const int64_t r0 = row_off[inst];
+    const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int k0 = s * kFb;
+    if (k0 >= m) return;
+    const int nb = min(kFb, m - k0);
+    const double* L = dense + dn_off[inst];
+    double* x = xv + r0;
+    const int i = threadIdx.x;
+    for (int idx = i; idx < kFb * kFb; idx += kFb) {
+        const int r = idx / kFb, c = idx % kFb;
+        sL[r][c] = (r < nb && c < r) ? L[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
+    }
+    double v = i < nb ? x[k0 + i] : 0.0;
+    __syncthreads();
+    for (int j = 0; j < nb; ++j) {
+        if (i == j) sy[j] = v;
+        __syncthreads();
+        if (i > j && i < nb) v -= sL[i][j] * sy[j];
+    }
+    if (i < nb) x[k0 + i] = v;
+}
+
+__global__ void __launch_bounds__(kT) batch_fwd_gemv_kernel(int s, int cnt, const int64_t* __restrict__ chunks,
+                                                           const int64_t* __restrict__ row_off,
+                                                           const int64_t* __restrict__ dn_off,
+                                                           const int32_t* __restrict__ order,
+                                                           const int32_t* __restrict__ status,
+                                                           const int32_t* __restrict__ refine,
+                                                           const double* __restrict__ dense, double* __restrict__ xv) {
+    __shared__ double sx[kFb];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (;;) {
-        __syncthreads();
-        if (tid == 0) s_item = atomicAdd(ticket, 1u);
-        __syncthreads();
-        const unsigned item = s_item;
-        if (item >= K) break;
-        const int inst = order[item];
-        if (status[inst] != ST_RUN || (refine && !refine[inst])) continue;
-        const int64_t r0 = row_off[inst];
-        const int m = static_cast<int>(row_off[inst + 1] - r0);
-        const double* L = dense + dn_off[inst];
-        const double* Dv = dD + r0;
-        double* x = xv + r0;
-        // forward: L y = b (unit lower)
-        for (int k0 = 0; k0 < m; k0 += kNb) {
-            const int nb = min(kNb, m - k0), k1 = k0 + nb;
-            for (int idx = tid; idx < nb * nb; idx += kT) {
-                const int r = idx / nb, c = idx % nb;
-                sB[r][c] = L[(int64_t)(k0 + r) * m + k0 + c];
-            }
-            __syncthreads();
-            if (warp == 0) {
-                double v = lane < nb ? x[k0 + lane] : 0.0;
-                for (int j = 0; j < nb; ++j) {
-                    const double yj = __shfl_sync(0xffffffffu, v, j);
-                    if (lane > j && lane < nb) v -= sB[lane][j] * yj;
-                }
-                if (lane < nb) {
-                    x[k0 + lane] = v;
-                    sx[lane] = v;
-                }
-            }
-            __syncthreads();
-            for (int r = k1 + tid; r < m; r += kT) {
+    const int b = chunk_instance(chunks, cnt, blockIdx.x);
+    const int inst = order[b];
+    if (!solving(status, refine, inst)) return;
+    const int64_t local = blockIdx.x - (b > 0 ? chunks[b - 1] : 0);
+    const int64_t r0 = row_off[inst];
+    const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int k0 = s * kFb;
+    const int nb = min(kFb, m - k0), k1 = k0 + nb;
+    const double* L = dense + dn_off[inst];
+    double* x = xv + r0;
+    if (tid < kFb) sx[tid] = tid < nb ? x[k0 + tid] : 0.0;
+    __syncthreads();
+    const int rb = k1 + static_cast<int>(local) * kT, re = min(m, rb + kT);
+    for (int rw = rb + warp * 4; rw < re; rw += (kT / 32) * 4) {
+        double p[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int r = rw + u;
+            double a = 0.0;
+            if (r < re) {
                 const double* Lr = L + (int64_t)r * m + k0;
-                double s = 0.0;
-                for (int q = 0; q < nb; ++q) s += Lr[q] * sx[q];
-                x[r] -= s;
+                const double p0 = lane < nb ? Lr[lane] * sx[lane] : 0.0;
+                const double p1 = lane + 32 < nb ? Lr[lane + 32] * sx[lane + 32] : 0.0;
+                a = p0 + p1;
             }
-            __syncthreads();
+            p[u] = a;
         }
-        for (int r = tid; r < m; r += kT) x[r] /= Dv[r];
-        __syncthreads();
-        // backward: L^T x = y
-        for (int k1 = m; k1 > 0; k1 -= kNb) {
-            const int k0 = max(0, k1 - kNb), nb = k1 - k0;
-            double acc = 0.0;
-            if (lane < nb)
-                for (int c = k1 + warp; c < m; c += kT / 32) acc += L[(int64_t)c * m + k0 + lane] * x[c];
-            sacc[warp][lane] = acc;
-            for (int idx = tid; idx < nb * nb; idx += kT) {
-                const int r = idx / nb, c = idx % nb;
-                sB[r][c] = L[(int64_t)(k0 + r) * m + k0 + c];
-            }
-            __syncthreads();
-            if (warp == 0) {
-                double v = 0.0;
-                if (lane < nb) {
-                    double t = 0.0;
-                    for (int w = 0; w < kT / 32; ++w) t += sacc[w][lane];
-                    v = x[k0 + lane] - t;
-                }
-                for (int j = nb - 1; j >= 0; --j) {
-                    const double xj = __shfl_sync(0xffffffffu, v, j);
-                    if (lane < j) v -= sB[j][lane] * xj;
-                }
-                if (lane < nb) x[k0 + lane] = v;
-            }
-            __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) p[u] += __shfl_xor_sync(0xffffffffu, p[u], o);
+        }
+        if (lane < 4 && rw + lane < re) {
+            const double t = lane == 0 ? p[0] : lane == 1 ? p[1] : lane == 2 ? p[2] : p[3];
+            x[rw + lane] -= t;
         }
     }
+}
+
+__global__ void batch_scale_kernel(int64_t m, const int32_t* __restrict__ row_inst,
+                                   const int32_t* __restrict__ status, const int32_t* __restrict__ refine,
+                                   const double* __restrict__ dD, double* __restrict__ x) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    if (solving(status, refine, row_inst[k])) x[k] /= dD[k];
+}
+
+// part[chunk][q] = sum over the chunk's rows c (in order, per warp, then the
+// warps in order) of L[c][k0 + q] x[c]
+__global__ void __launch_bounds__(kT) batch_bwd_gemv_kernel(int s, int cnt, const int64_t* __restrict__ chunks,
+                                                           const int64_t* __restrict__ row_off,
+                                                           const int64_t* __restrict__ dn_off,
+                                                           const int32_t* __restrict__ order,
+                                                           const int32_t* __restrict__ status,
+                                                           const int32_t* __restrict__ refine,
+                                                           const double* __restrict__ dense,
+                                                           const double* __restrict__ xv, double* __restrict__ part) {
+    __shared__ double sacc[kT / 32][kFb];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int b = chunk_instance(chunks, cnt, blockIdx.x);
+    const int inst = order[b];
+    if (!solving(status, refine, inst)) return;
+    const int64_t local = blockIdx.x - (b > 0 ? chunks[b - 1] : 0);
+    const int64_t r0 = row_off[inst];
+    const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int k0 = s * kFb;
+    const int nb = min(kFb, m - k0), k1 = k0 + nb;
+    const double* L = dense + dn_off[inst];
+    const double* x = xv + r0;
+    const int rb = k1 + static_cast<int>(local) * kT, re = min(m, rb + kT);
+    double a0 = 0.0, a1 = 0.0;
+    for (int c = rb + warp; c < re; c += kT / 32) {
+        const double* Lc = L + (int64_t)c * m + k0;
+        const double xc = x[c];
+        if (lane < nb) a0 += Lc[lane] * xc;
+        if (lane + 32 < nb) a1 += Lc[lane + 32] * xc;
+    }
+    sacc[warp][lane] = a0;
+    sacc[warp][lane + 32] = a1;
+    __syncthreads();
+    if (tid < kFb) {
+        double t = 0.0;
+        for (int w = 0; w < kT / 32; ++w) t += sacc[w][tid];
+        part[blockIdx.x * (int64_t)kFb + tid] = t;
+    }
+}
+
+__global__ void __launch_bounds__(kFb) batch_bwd_diag_kernel(int s, const int64_t* __restrict__ chunks,
+                                                            const int64_t* __restrict__ row_off,
+                                                            const int64_t* __restrict__ dn_off,
+                                                            const int32_t* __restrict__ order,
+                                                            const int32_t* __restrict__ status,
+                                                            const int32_t* __restrict__ refine,
+                                                            const double* __restrict__ dense,
+                                                            const double* __restrict__ part,
+                                                            double* __restrict__ xv) {
+    __shared__ double sL[kFb][kFbP];
+    __shared__ double sxj[kFb];
+    const int b = blockIdx.x;
+    const int inst = order[b];
+    if (!solving(status, refine, inst)) return;
+    const int64_t r0 = row_off[inst];
+    const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int k0 = s * kFb;
+    if (k0 >= m) return;
+    const int nb = min(kFb, m - k0);
+    const double* L = dense + dn_off[inst];
+    double* x = xv + r0;
+    const int q = threadIdx.x;
+    for (int idx = q; idx < kFb * kFb; idx += kFb) {
+        const int r = idx / kFb, c = idx % kFb;
+        sL[r][c] = (r < nb && c < r) ? L[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
+    }
+    const int64_t c0 = b > 0 ? chunks[b - 1] : 0, c1 = chunks[b];
+    double t = 0.0;
+    if (q < nb)
+        for (int64_t ch = c0; ch < c1; ++ch) t += part[ch * kFb + q];
+    double v = q < nb ? x[k0 + q] - t : 0.0;
+    __syncthreads();
+    for (int j = nb - 1; j >= 0; --j) {
+        if (q == j) sxj[j] = v;
+        __syncthreads();
+        if (q < j) v -= sL[j][q] * sxj[j];
+    }
+    if (q < nb) x[k0 + q] = v;
 }
 
 // Refinement bookkeeping per instance (refinement.cpp:15-30): with r = rhs - N x,
@@ -618,9 +723,10 @@ __global__ void narrow_rp_kernel(int64_t n, const int64_t* __restrict__ in, int3
 void free_batch(hn_batch* B) {
     if (!B) return;
     for (void* p : {(void*)B->row_off, (void*)B->col_off, (void*)B->row_inst, (void*)B->dn_off, (void*)B->order,
-                    (void*)B->dense, (void*)B->dD, (void*)B->ticket, (void*)B->refine, (void*)B->nref, (void*)B->nrp,
+                    (void*)B->dense, (void*)B->dD, (void*)B->refine, (void*)B->nref, (void*)B->nrp,
                     (void*)B->tile_row, (void*)B->tile_nz, (void*)B->carry_row, (void*)B->head_row,
-                    (void*)B->carry_val, (void*)B->head_val, (void*)B->r, (void*)B->ax, (void*)B->step_pairs, (void*)B->step_chunks})
+                    (void*)B->carry_val, (void*)B->head_val, (void*)B->r, (void*)B->ax, (void*)B->step_pairs, (void*)B->step_chunks,
+                    (void*)B->solve_part})
         dfree(p);
     delete B;
 }
@@ -630,16 +736,34 @@ SpmvMat n_mat(const hn_batch* B, const double* nval) {
                    B->carry_val, B->head_row, B->head_val, B->ntiles};
 }
 
-void reset_ticket(hn_batch* B, cudaStream_t s) {
-    check_cuda(cudaMemsetAsync(B->ticket, 0, sizeof(unsigned), s), "memset ticket");
-}
-
 void solve_all(hn_batch* B, const int32_t* status, const int32_t* refine, double* x, cudaStream_t s) {
-    reset_ticket(B, s);
-    const int grid = (int)std::min<int64_t>(B->K, (int64_t)ctx().sm_count * 4);
-    batch_solve_kernel<<<grid, kT, 0, s>>>(B->K, B->row_off, B->dn_off, B->order, status, refine, B->dense, B->dD, x,
-                                           B->ticket);
-    launched("batch_solve_kernel");
+    for (int64_t st = 0; st < B->nsteps; ++st) {
+        const int cnt = B->step_cnt[st];
+        batch_fwd_diag_kernel<<<cnt, kFb, 0, s>>>((int)st, B->row_off, B->dn_off, B->order, status, refine, B->dense, x);
+        launched("batch_fwd_diag_kernel");
+        const int64_t nc = B->step_chunks_h[st];
+        if (nc > 0) {
+            batch_fwd_gemv_kernel<<<(unsigned)nc, kT, 0, s>>>((int)st, cnt, B->step_chunks + B->chunk_off_h[st],
+                                                              B->row_off, B->dn_off, B->order, status, refine,
+                                                              B->dense, x);
+            launched("batch_fwd_gemv_kernel");
+        }
+    }
+    batch_scale_kernel<<<(unsigned)((B->m + 255) / 256), 256, 0, s>>>(B->m, B->row_inst, status, refine, B->dD, x);
+    launched("batch_scale_kernel");
+    for (int64_t st = B->nsteps - 1; st >= 0; --st) {
+        const int cnt = B->step_cnt[st];
+        const int64_t nc = B->step_chunks_h[st];
+        const int64_t* ch = B->step_chunks + B->chunk_off_h[st];
+        if (nc > 0) {
+            batch_bwd_gemv_kernel<<<(unsigned)nc, kT, 0, s>>>((int)st, cnt, ch, B->row_off, B->dn_off, B->order,
+                                                              status, refine, B->dense, x, B->solve_part);
+            launched("batch_bwd_gemv_kernel");
+        }
+        batch_bwd_diag_kernel<<<cnt, kFb, 0, s>>>((int)st, ch, B->row_off, B->dn_off, B->order, status, refine,
+                                                  B->dense, B->solve_part, x);
+        launched("batch_bwd_diag_kernel");
+    }
 }
 
 }  // namespace
@@ -683,7 +807,6 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
             B->row_inst = dmalloc<int32_t>(m);
             B->dense = dmalloc<double>(dn[K]);
             B->dD = dmalloc<double>(m);
-            B->ticket = dmalloc<unsigned>(1);
             B->refine = dmalloc<int32_t>(K);
             B->nref = dmalloc<int32_t>(1);
             B->r = dmalloc<double>(m);
@@ -728,6 +851,9 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
             }
             B->step_pairs = dmalloc<int64_t>(flat.size());
             B->step_chunks = dmalloc<int64_t>(cflat.size());
+            int64_t maxc = 1;
+            for (int64_t c : B->step_chunks_h) maxc = std::max(maxc, c);
+            B->solve_part = dmalloc<double>(maxc * kFb);
             check_cuda(cudaMemcpy(B->step_chunks, cflat.data(), sizeof(int64_t) * cflat.size(),
                                   cudaMemcpyHostToDevice),
                        "H2D chunks");
