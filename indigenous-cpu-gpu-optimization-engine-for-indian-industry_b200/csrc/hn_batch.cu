@@ -272,12 +272,19 @@ __global__ void batch_dense_kernel(int64_t m, const int64_t* __restrict__ row_of
 //   batch_ldlt_panel_kernel: every instance's panel below its diagonal block,
 //     in chunks of kT rows spread over the GPU, one row per thread;
 //   batch_ldlt_update_kernel: all instances' trailing kFb x kFb tiles
-//     A_rc -= sum_q (L_rq D_q) L_cq, spread over every CTA of the GPU, each
-//     thread accumulating a 4 x 4 block of the tile in registers.
+//     A_rc -= sum_q (L_rq D_q) L_cq, spread over every CTA of the GPU, on the
+//     FP64 tensor cores (mma.sync m8n8k4, FP64 in and out).
 constexpr int kFb = 64;
+
+// D(8x8) += A(8x4) B(4x8) in FP64 on the tensor cores. Fragments: lane l
+// holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4)], D[l/4][2(l%4)+1].
+__device__ __forceinline__ void dmma_m8n8k4(double* d, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
 constexpr int kFbP = kFb + 1;  // padded smem row (conflict-free column walks)
 constexpr size_t kPanelSmem = sizeof(double) * (kFb * kFbP + kFb);
-constexpr size_t kUpdateSmem = sizeof(double) * 2 * kFb * kFbP;
 
 __global__ void __launch_bounds__(kT) batch_ldlt_diag_kernel(int s, const int64_t* __restrict__ row_off,
                                                              const int64_t* __restrict__ dn_off,
@@ -380,7 +387,7 @@ __global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, int cnt, co
         if (c < nb) Ar[c] = lv[c];
 }
 
-__global__ void __launch_bounds__(kT) batch_ldlt_update_kernel(int s, int cnt, int64_t npairs,
+__global__ void __launch_bounds__(kT, 4) batch_ldlt_update_kernel(int s, int cnt, int64_t npairs,
                                                                const int64_t* __restrict__ pairs,
                                                                const int64_t* __restrict__ row_off,
                                                                const int64_t* __restrict__ dn_off,
@@ -388,11 +395,13 @@ __global__ void __launch_bounds__(kT) batch_ldlt_update_kernel(int s, int cnt, i
                                                                const int32_t* __restrict__ status,
                                                                double* __restrict__ dense,
                                                                const double* __restrict__ dD) {
-    extern __shared__ double smem[];
-    // k-major copies of the two panel slices: sW[q][r] = L[rb+r, k0+q] D_q,
-    // sL[q][c] = L[cb+c, k0+q]
-    double(*sW)[kFbP] = reinterpret_cast<double(*)[kFbP]>(smem);
-    double(*sL)[kFbP] = reinterpret_cast<double(*)[kFbP]>(smem + kFb * kFbP);
+    // k-major copies of the two panel slices, kFb / 2 columns at a time:
+    // sW[q][r] = L[rb+r, k0+kh+q] D_(kh+q), sL[q][c] = L[cb+c, k0+kh+q]
+    // row stride 68 doubles: a half-warp's fragment loads (k = l%4, column
+    // l/4) fall in 16 distinct banks
+    constexpr int kUP = kFb + 4;
+    __shared__ double sW[kFb / 2][kUP];
+    __shared__ double sL[kFb / 2][kUP];
     const int tid = threadIdx.x;
     const int ty = tid >> 4, tx = tid & 15;
     const int k0 = s * kFb;
@@ -419,39 +428,50 @@ __global__ void __launch_bounds__(kT) batch_ldlt_update_kernel(int s, int cnt, i
         const int rb = k1 + ti * kFb, cb = k1 + tj * kFb;
         double* A = dense + dn_off[inst];
         const double* Dv = dD + r0 + k0;
-        __syncthreads();
-        for (int idx = tid; idx < kFb * kFb; idx += kT) {
-            const int rr = idx / kFb, q = idx % kFb;
-            const bool okr = rb + rr < m && q < nb, okc = cb + rr < m && q < nb;
-            sW[q][rr] = okr ? A[(int64_t)(rb + rr) * m + k0 + q] * Dv[q] : 0.0;
-            sL[q][rr] = okc ? A[(int64_t)(cb + rr) * m + k0 + q] : 0.0;
+        // warp w: rows 16 (w >> 1) .. + 16 (two 8-row tiles), columns
+        // 32 (w & 1) .. + 32 (four 8-column tiles) of the 64 x 64 output
+        const int lane = tid & 31, warp = tid >> 5;
+        const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
+        const int fr = lane >> 2, fk = lane & 3;
+        double acc[2][4][2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int kh = 0; kh < kFb; kh += kFb / 2) {
+            __syncthreads();
+            for (int idx = tid; idx < kFb * (kFb / 2); idx += kT) {
+                const int rr = idx / (kFb / 2), q = idx % (kFb / 2);
+                const bool okr = rb + rr < m && kh + q < nb, okc = cb + rr < m && kh + q < nb;
+                sW[q][rr] = okr ? A[(int64_t)(rb + rr) * m + k0 + kh + q] * Dv[kh + q] : 0.0;
+                sL[q][rr] = okc ? A[(int64_t)(cb + rr) * m + k0 + kh + q] : 0.0;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kq = 0; kq < kFb / 2; kq += 4) {
+                double a[2], b[4];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) a[i] = sW[kq + fk][wr + 8 * i + fr];  // A(8x4)[fr][fk]
+#pragma unroll
+                for (int j = 0; j < 4; ++j) b[j] = sL[kq + fk][wc + 8 * j + fr];  // B(4x8)[fk][fr]
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) dmma_m8n8k4(acc[i][j], a[i], b[j]);
+            }
         }
-        __syncthreads();
-        double acc[4][4];
+        // D(8x8)[fr][2 fk + t]
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-#pragma unroll 4
-        for (int q = 0; q < kFb; ++q) {
-            double a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = sW[q][ty + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = sL[q][tx + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int gr = rb + ty + 16 * i;
+        for (int i = 0; i < 2; ++i) {
+            const int gr = rb + wr + 8 * i + fr;
             if (gr >= m) continue;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const int gc = cb + tx + 16 * j;
-                if (gc <= gr) A[(int64_t)gr * m + gc] -= acc[i][j];
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                    const int gc = cb + wc + 8 * j + 2 * fk + t;
+                    if (gc <= gr) A[(int64_t)gr * m + gc] -= acc[i][j][t];
+                }
             }
         }
     }
@@ -857,9 +877,6 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
             check_cuda(cudaMemcpy(B->step_chunks, cflat.data(), sizeof(int64_t) * cflat.size(),
                                   cudaMemcpyHostToDevice),
                        "H2D chunks");
-            check_cuda(cudaFuncSetAttribute(batch_ldlt_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)kUpdateSmem),
-                       "update kernel smem");
             check_cuda(cudaMemcpy(B->step_pairs, flat.data(), sizeof(int64_t) * flat.size(), cudaMemcpyHostToDevice),
                        "H2D schedule");
             check_cuda(cudaStreamSynchronize(s), "batch create sync");
@@ -923,7 +940,7 @@ int hn_batch_factor(hn_batch* B, const double* D, double reg, double singular_to
             const int64_t np = B->step_pairs_h[st];
             if (np > 0) {
                 const int grid = (int)std::min<int64_t>(np, (int64_t)ctx().sm_count * 8);
-                batch_ldlt_update_kernel<<<grid, kT, kUpdateSmem, s>>>((int)st, cnt, np, B->step_pairs + B->pair_off_h[st],
+                batch_ldlt_update_kernel<<<grid, kT, 0, s>>>((int)st, cnt, np, B->step_pairs + B->pair_off_h[st],
                                                              B->row_off, B->dn_off, B->order, status, B->dense,
                                                              B->dD);
                 launched("batch_ldlt_update_kernel");
