@@ -454,7 +454,8 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
             kw = {}
             if warm is not None:
                 preds = gnn.predict(warm, gnn.Batch(part))
-                kw = {"x0s": [p[0] for p in preds], "y0s": [p[1] for p in preds], "s0s": [p[2] for p in preds]}
+                kw = {"x0s": [p[0] for p in preds], "y0s": [p[1] for p in preds], "s0s": [p[2] for p in preds],
+                      "warm_floor": gnn.WARM_FLOOR}
             r = hn.lp_solve_batch(part, **kw)
             for k in ("status", "objective", "iterations", "warm_used"):
                 out[k].append(r[k])

@@ -66,7 +66,9 @@ def test_backward_is_deterministic(hn, torch_cuda):
 
 def test_training_lowers_the_loss_and_warm_start_keeps_the_answer(hn, torch_cuda):
     """Train on IPM solutions of small C0-generator LPs; the prediction for
-    held-out LPs warm-starts the IPM without changing status or objective."""
+    held-out LPs warm-starts the IPM without changing status or objective,
+    and saves iterations: the held-out mean drops by at least one (measured
+    16.6 -> 12.8; everything here is seeded and the kernels deterministic)."""
     sizes = [int(v) for v in np.exp(np.random.default_rng(0).uniform(np.log(60), np.log(200), 40))]
     lps = [lpgen.lp_uniform(m, int(round(2.5 * m)), 8, 50000 + i) for i, m in enumerate(sizes)]
     r = hn.lp_solve_batch(lps)
@@ -84,12 +86,15 @@ def test_training_lowers_the_loss_and_warm_start_keeps_the_answer(hn, torch_cuda
     assert losses[-1] < 0.5 * losses[0], losses[::10]
     Bh = gnn.Batch([lps[i] for i in held])
     preds = gnn.predict(model, Bh)
-    used = 0
+    used, it_warm, it_cold = 0, [], []
     for k, i in enumerate(held):
         x, y, s = preds[k]
-        w = hn.lp_solve(lps[i], x0=x, y0=y, s0=s)
+        w = hn.lp_solve(lps[i], x0=x, y0=y, s0=s, warm_floor=gnn.WARM_FLOOR)
         cold = hn.lp_solve(lps[i])
         used += int(w["warm_start_used"])
+        it_warm.append(w["iterations"])
+        it_cold.append(cold["iterations"])
         assert w["status"] == cold["status"] == 1
         assert abs(w["objective"] - cold["objective"]) <= 1e-8 * (1 + abs(cold["objective"]))
-    assert used >= 1
+    assert used == len(held)
+    assert np.mean(it_warm) <= np.mean(it_cold) - 1.0, (it_warm, it_cold)
