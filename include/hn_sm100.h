@@ -347,6 +347,13 @@ int hn_gnn_cast_weights(int K, const float* W_dev, void* Wt_bf16_dev, void* Wb_b
  * bias may be NULL (K2 = 0 / no bias). */
 int hn_gnn_linear(int64_t M, int K1, int K2, const float* X1_dev, const float* X2_dev, const void* Wt_bf16_dev,
                   int N, const float* bias_dev, int relu, float* Y_dev, void* stream);
+/* hn_gnn_linear with N = 64 on the 5th-generation tensor cores: tcgen05.mma
+ * (kind::f16, BF16 operands from shared memory, FP32 accumulator in tensor
+ * memory), 128 rows per CTA. Same operand rounding as hn_gnn_linear; results
+ * differ from it only by accumulation order. Synchronises the stream (it
+ * reports a timed-out completion wait as HN_ERR_CUDA). */
+int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1_dev, const float* X2_dev, const void* Wt_bf16_dev,
+                       const float* bias_dev, int relu, float* Y_dev, void* stream);
 /* Backward of hn_gnn_linear with N = 64: G = dY * relu'(Y); dX (M x K, may be
  * NULL; K = 64 or 128) = G W^T; dW (K x 64) = [X1 | X2]^T G; db (64) = sum of
  * G's rows. scratch: >= ceil(M / 64) * (64 K + 64) floats. Deterministic. */

@@ -154,6 +154,152 @@ __global__ void __launch_bounds__(kGT) gnn_gemm_kernel(int64_t M, int K1, int K2
     }
 }
 
+// ---- the same layer on the 5th-generation tensor cores (tcgen05) ----
+// One CTA (4 warps) computes a 128-row x 64-column tile of Y with K <= 128:
+// both operands are staged in shared memory in the canonical K-major,
+// no-swizzle layout (core matrices of 8 rows x 16 bytes; the next 8-row
+// group 128 bytes on, the next 8-element K chunk LBO bytes on), one thread
+// issues K / 16 tcgen05.mma (kind::f16, BF16 in, FP32 accumulated in 64
+// TMEM columns), a commit signals an mbarrier, and each warp reads its 32
+// rows back with tcgen05.ld for the bias/ReLU epilogue. The mbarrier wait is
+// bounded: on a timeout the kernel records it in *err and still frees TMEM.
+constexpr int kUmmaM = 128;
+constexpr uint32_t kUmmaSbo = 128;
+constexpr uint32_t kUmmaLboA = (kUmmaM / 8) * 128;  // 2048
+constexpr uint32_t kUmmaLboB = (kH / 8) * 128;      // 1024
+constexpr uint32_t kUmmaSpin = 1u << 24;
+constexpr int kUmmaSmem = (kUmmaM + kH) * kMaxK * 2;  // 48 KB dynamic
+
+__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    // start address, leading and stride byte offsets (16-byte units), version 1, no swizzle
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+// kind::f16 instruction descriptor: F32 accumulator, BF16 A and B, both K-major
+constexpr uint32_t kUmmaIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kH >> 3) << 17) |
+                                ((uint32_t)(kUmmaM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__global__ void __launch_bounds__(128) gnn_umma_kernel(int64_t M, int K1, int K2, const float* __restrict__ X1,
+                                                      const float* __restrict__ X2,
+                                                      const __nv_bfloat16* __restrict__ Bt,
+                                                      const float* __restrict__ bias, int relu,
+                                                      float* __restrict__ Y, int* err) {
+    extern __shared__ __align__(1024) uint8_t umma_smem[];
+    uint8_t* sA = umma_smem;                        // 128 x K BF16, 32 KB at K = 128
+    uint8_t* sB = umma_smem + kUmmaM * kMaxK * 2;   // 64 x K BF16, 16 KB
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t s_tmem;
+    const int K = K1 + K2, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t row0 = blockIdx.x * (int64_t)kUmmaM;
+    // operands: 8 consecutive K elements (16 bytes) per store
+    for (int idx = tid; idx < kUmmaM * (K / 8); idx += 128) {
+        const int r = idx / (K / 8), kc = idx % (K / 8);
+        const int64_t gr = row0 + r;
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = 0.f;
+        if (gr < M) {
+            const int k = kc * 8;
+            const float* src = k < K1 ? X1 + gr * K1 + k : X2 + gr * K2 + (k - K1);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = src[u];
+        }
+        uint32_t w[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const __nv_bfloat16 lo = __float2bfloat16_rn(v[2 * u]), hi = __float2bfloat16_rn(v[2 * u + 1]);
+            w[u] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+        }
+        *reinterpret_cast<uint4*>(sA + kc * kUmmaLboA + (r >> 3) * kUmmaSbo + (r & 7) * 16) =
+            make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    for (int idx = tid; idx < kH * (K / 8); idx += 128) {
+        const int n = idx / (K / 8), kc = idx % (K / 8);
+        *reinterpret_cast<uint4*>(sB + kc * kUmmaLboB + (n >> 3) * kUmmaSbo + (n & 7) * 16) =
+            *reinterpret_cast<const uint4*>(Bt + (int64_t)n * K + kc * 8);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(kH));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // staged operands -> tensor core
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    if (tid == 0) {
+        const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+        for (int ks = 0; ks < K / 16; ++ks) {
+            const uint64_t da = umma_smem_desc(a0 + 2 * ks * kUmmaLboA, kUmmaLboA, kUmmaSbo);
+            const uint64_t db = umma_smem_desc(b0 + 2 * ks * kUmmaLboB, kUmmaLboB, kUmmaSbo);
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                "l"(da), "l"(db), "r"(kUmmaIdesc), "r"(ks > 0 ? 1 : 0));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&mbar))
+                     : "memory");
+    }
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < kUmmaSpin && !done; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_u32(&mbar)), "r"(0u)
+            : "memory");
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!done) {
+        if (lane == 0) atomicExch(err, 1);
+    } else {
+        uint32_t r[64];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,"
+            "%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63},"
+            " [%64];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+              "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+              "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+              "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]),
+              "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]),
+              "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]),
+              "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]),
+              "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+            : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int64_t gr = row0 + warp * 32 + lane;  // TMEM lane = row of the tile
+        if (gr < M) {
+            float4* out = reinterpret_cast<float4*>(Y + gr * kH);
+#pragma unroll
+            for (int c = 0; c < kH; c += 4) {
+                float v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    float t = __uint_as_float(r[c + u]) + (bias ? bias[c + u] : 0.f);
+                    v[u] = relu ? fmaxf(t, 0.f) : t;
+                }
+                out[c / 4] = make_float4(v[0], v[1], v[2], v[3]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kH));
+}
+
 // G = dY * (Y > 0) (or dY when relu == 0)
 __global__ void gnn_relu_bwd_kernel(int64_t len, const float* __restrict__ dY, const float* __restrict__ Y, int relu,
                                     float* __restrict__ G) {
@@ -306,6 +452,34 @@ int hn_gnn_linear(int64_t M, int K1, int K2, const float* X1, const float* X2, c
             gnn_gemm_kernel<128, 64><<<grid, kGT, 0, as_stream(stream)>>>(M, K1, K2, X1, X2, B, bias, relu, Y);
         }
         launched("gnn_gemm_kernel");
+    });
+}
+
+int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1, const float* X2, const void* Wt_bf16,
+                       const float* bias, int relu, float* Y, void* stream) {
+    return guard("hn_gnn_linear_umma", [&] {
+        require_init();
+        const int K = K1 + K2;
+        if (M < 0 || K1 <= 0 || K2 < 0 || K > kMaxK || K1 % 16 || K2 % 16 || !X1 || (K2 && !X2) || !Wt_bf16 || !Y)
+            fail(HN_ERR_INVALID_ARG, "bad arguments (K1, K2 multiples of 16, K1 + K2 <= 128)");
+        if (M == 0) return;
+        cudaStream_t s = as_stream(stream);
+        Workspace& w = workspace(s);
+        int* err = reinterpret_cast<int*>(w.select);  // pricing scratch word 0, free between calls
+        check_cuda(cudaMemsetAsync(err, 0, sizeof(int), s), "memset");
+        static int attr_device = -1;
+        if (attr_device != ctx().device) {
+            check_cuda(cudaFuncSetAttribute(gnn_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kUmmaSmem),
+                       "umma smem attribute");
+            attr_device = ctx().device;
+        }
+        gnn_umma_kernel<<<(unsigned)((M + kUmmaM - 1) / kUmmaM), 128, kUmmaSmem, s>>>(
+            M, K1, K2, X1, X2, static_cast<const __nv_bfloat16*>(Wt_bf16), bias, relu, Y, err);
+        launched("gnn_umma_kernel");
+        int h = 0;
+        check_cuda(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H flag");
+        check_cuda(cudaStreamSynchronize(s), "umma sync");
+        if (h) fail(HN_ERR_CUDA, "tensor-core layer: MMA completion wait timed out");
     });
 }
 

@@ -16,9 +16,9 @@ start (hnb200.lp_solve(..., x0, y0, s0)), which it shifts to strict interiority
 and keeps only when its KKT residual beats the default start.
 
 Every step runs on the sm_100a library (include/hn_sm100.h, hn_gnn_*):
-aggregations are its 64-wide SpMM over the device A and A^T, the 64-wide
-layers are BF16 tensor-core GEMMs with FP32 accumulation, forward and
-backward, and Adam updates FP32 master weights. PyTorch only holds the device
+aggregations are its 64-wide SpMM over the device A and A^T, the forward
+layers are BF16 tcgen05 MMAs with FP32 accumulation in tensor memory, the
+backward's GEMMs BF16 mma.sync tiles, and Adam updates FP32 master weights. PyTorch only holds the device
 buffers.
 """
 from __future__ import annotations
@@ -213,12 +213,13 @@ def forward(model: Model, B: Batch):
     lib = hn.load()
 
     def lin(X1, X2, name, relu, rows):
+        # the layers run on the tcgen05 tensor cores (hn_gnn_linear_umma)
         K1 = X1.shape[1]
         K2 = 0 if X2 is None else X2.shape[1]
         Y = _empty(torch, rows)
-        hn.check(lib.hn_gnn_linear(rows, K1, K2, X1.data_ptr(), None if X2 is None else X2.data_ptr(),
-                                   model.wt[name].data_ptr(), H, model.b(name).data_ptr(), relu, Y.data_ptr(),
-                                   None))
+        hn.check(lib.hn_gnn_linear_umma(rows, K1, K2, X1.data_ptr(), None if X2 is None else X2.data_ptr(),
+                                        model.wt[name].data_ptr(), model.b(name).data_ptr(), relu, Y.data_ptr(),
+                                        None))
         return Y
 
     hv = [lin(B.Fv, None, "ev", 1, B.n)]

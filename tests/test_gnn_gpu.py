@@ -98,3 +98,35 @@ def test_training_lowers_the_loss_and_warm_start_keeps_the_answer(hn, torch_cuda
         assert abs(w["objective"] - cold["objective"]) <= 1e-8 * (1 + abs(cold["objective"]))
     assert used == len(held)
     assert np.mean(it_warm) <= np.mean(it_cold) - 1.0, (it_warm, it_cold)
+
+
+@pytest.mark.parametrize("K1,K2,relu,M", [(16, 0, 1, 1000), (64, 64, 1, 4097), (64, 0, 0, 130), (32, 32, 1, 128)])
+def test_tcgen05_layer_matches_mma_sync_layer(hn, torch_cuda, K1, K2, relu, M):
+    """hn_gnn_linear_umma (tcgen05, TMEM accumulator) against hn_gnn_linear
+    (mma.sync): same BF16 operands, FP32 accumulation in a different order."""
+    torch = torch_cuda
+    g = torch.Generator(device="cuda").manual_seed(K1 + K2 + M)
+    X1 = torch.randn((M, K1), generator=g, device="cuda")
+    X2 = torch.randn((M, K2), generator=g, device="cuda") if K2 else None
+    K = K1 + K2
+    W = torch.randn(K * 64, generator=g, device="cuda") / K ** 0.5
+    b = torch.randn(64, generator=g, device="cuda")
+    Wt = torch.empty(K * 64, dtype=torch.bfloat16, device="cuda")
+    Wb = torch.empty(K * 64, dtype=torch.bfloat16, device="cuda")
+    lib = hn.load()
+    hn.check(lib.hn_gnn_cast_weights(K, W.data_ptr(), Wt.data_ptr(), Wb.data_ptr(), None))
+    ys = []
+    for fn in ("mma", "umma"):
+        Y = torch.full((M, 64), float("nan"), device="cuda")
+        x2 = None if X2 is None else X2.data_ptr()
+        if fn == "mma":
+            hn.check(lib.hn_gnn_linear(M, K1, K2, X1.data_ptr(), x2, Wt.data_ptr(), 64, b.data_ptr(), relu,
+                                       Y.data_ptr(), None))
+        else:
+            hn.check(lib.hn_gnn_linear_umma(M, K1, K2, X1.data_ptr(), x2, Wt.data_ptr(), b.data_ptr(), relu,
+                                            Y.data_ptr(), None))
+        torch.cuda.synchronize()
+        ys.append(Y.cpu().numpy().astype(np.float64))
+    assert np.all(np.isfinite(ys[1]))
+    scale = np.abs(ys[0]).max() + 1.0
+    assert np.max(np.abs(ys[1] - ys[0])) <= 1e-5 * scale
