@@ -520,6 +520,103 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
             "warm_batched_vs_plain_gpu": round(plain_est / warm_s, 2)}
 
 
+def pricing(A, m, n, steps, warmup, flush):
+    """Device simplex pricing on the bench LP: reduced costs (A^T SpMV with the
+    rc = c - A^T y epilogue), a Devex update (A^T u, masked max, weights),
+    the entering choice (Bland; ranked top-1 and top-16) and a 16-column
+    gather; per call time (CUDA events, L2 flushed) and algorithmic bytes."""
+    import torch
+
+    import hnb200 as hn
+
+    rng = np.random.default_rng(5)
+    dev = "cuda"
+    y = torch.as_tensor(rng.standard_normal(m), device=dev)
+    u = torch.as_tensor(rng.standard_normal(m), device=dev)
+    cost = torch.as_tensor(rng.standard_normal(n), device=dev)
+    nb = np.arange(n, dtype=np.int32)
+    nb[rng.choice(n, m, replace=False)] = -1
+    nonbasis = torch.as_tensor(nb, device=dev)
+    art = torch.zeros(n, dtype=torch.uint8, device=dev)
+    rc = torch.empty(n, dtype=torch.float64, device=dev)
+    w = torch.ones(n, dtype=torch.float64, device=dev)
+    alpha = torch.empty(n, dtype=torch.float64, device=dev)
+    out = torch.empty(17, dtype=torch.int64, device=dev)
+    cols = torch.as_tensor(rng.choice(n, 16, replace=False).astype(np.int64), device=dev)
+    colbuf = torch.empty((16, m), dtype=torch.float64, device=dev)
+    spmv_t = 12 * A.nnz_t + 4 * (n + 1) + 8 * m
+    ops = {
+        "reduced_costs": (lambda: hn.price_reduced_costs(A, y, cost, rc), spmv_t + 16 * n),
+        "devex_update": (lambda: hn.price_devex_update(A, u, nonbasis, w, alpha), spmv_t + 8 * n + 2 * (12 * n)),
+        "select_bland": (lambda: hn.price_select(n, rc, w, nonbasis, art, out, rule=hn.PRICE_BLAND), 21 * n),
+        "select_ranked_k1": (lambda: hn.price_select(n, rc, w, nonbasis, art, out, k=1), 3 * 21 * n),
+        "select_ranked_k16": (lambda: hn.price_select(n, rc, w, nonbasis, art, out, k=16), 33 * 21 * n),
+        "columns_k16": (lambda: hn.price_columns(A, cols, colbuf), 16 * 8 * m),
+    }
+    res = {}
+    for name, (fn, nbytes) in ops.items():
+        for _ in range(warmup):
+            flush.zero_()
+            fn()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.zero_()
+            evs[i][0].record()
+            fn()
+            evs[i][1].record()
+        torch.cuda.synchronize()
+        ms = sorted(a.elapsed_time(b) for a, b in evs)[steps // 2]
+        res[name] = {"us": round(ms * 1e3, 2), "bytes": int(nbytes), "GB/s": round(nbytes / (ms * 1e-3) / 1e9, 1)}
+    return {"workload": f"simplex pricing on the LP m={m} n={n} nnz={A.nnz} (m basic columns)", **res}
+
+
+def gnn_layer(steps, warmup, rows=1 << 20):
+    """One 128 -> 64 GNN layer over `rows` rows (X = [X1 | X2], FP32, 512 MB
+    at 2^20 rows): the tcgen05 kernel and the mma.sync kernel, per call time
+    (CUDA events; the input exceeds L2), bytes (X read, Y written) and flops."""
+    import torch
+
+    import hnb200 as hn
+
+    g = torch.Generator(device="cuda").manual_seed(3)
+    X1 = torch.randn((rows, 64), generator=g, device="cuda")
+    X2 = torch.randn((rows, 64), generator=g, device="cuda")
+    W = torch.randn(128 * 64, generator=g, device="cuda") / 128 ** 0.5
+    b = torch.zeros(64, device="cuda")
+    Wt = torch.empty(128 * 64, dtype=torch.bfloat16, device="cuda")
+    Wb = torch.empty(128 * 64, dtype=torch.bfloat16, device="cuda")
+    Y = torch.empty((rows, 64), device="cuda")
+    lib = hn.load()
+    hn.check(lib.hn_gnn_cast_weights(128, W.data_ptr(), Wt.data_ptr(), Wb.data_ptr(), None))
+    calls = {
+        "tcgen05": lambda: hn.check(lib.hn_gnn_linear_umma(rows, 64, 64, X1.data_ptr(), X2.data_ptr(), Wt.data_ptr(),
+                                                           b.data_ptr(), 1, Y.data_ptr(), None)),
+        "mma_sync": lambda: hn.check(lib.hn_gnn_linear(rows, 64, 64, X1.data_ptr(), X2.data_ptr(), Wt.data_ptr(), 64,
+                                                       b.data_ptr(), 1, Y.data_ptr(), None)),
+    }
+    nbytes = rows * (128 * 4 + 64 * 4)
+    flops = 2 * rows * 128 * 64
+    res = {"workload": f"GNN layer [X1 | X2] ({rows} x 128, FP32) x W (128 x 64, BF16) + b, ReLU"}
+    hn.check(lib.hn_gnn_check(None))
+    for name, fn in calls.items():
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = sorted(ts)[steps // 2]
+        hn.check(lib.hn_gnn_check(None))
+        res[name] = {"us": round(ms * 1e3, 1), "GB/s": round(nbytes / (ms * 1e-3) / 1e9, 1),
+                     "TFLOP/s": round(flops / (ms * 1e-3) / 1e12, 2)}
+    return res
+
+
 def run_only(args, local):
     """Single kernel group on the same LP (profiling aid). spmv / spmv_t flush
     L2 between launches by writing a 256 MB buffer; ada streams 11.6 GB."""
@@ -535,6 +632,8 @@ def run_only(args, local):
         return bb_batch(args.bb_k, args.bb_chunk)
     if args.only == "batch":
         return batched_ipm(args.batch_k, args.batch_sample)
+    if args.only == "gnn_layer":
+        return gnn_layer(args.steps, args.warmup)
     if args.only == "gnn":
         return gnn_warm(args.gnn_train, args.gnn_eval, args.gnn_mlo, args.gnn_mhi, args.gnn_epochs, args.gnn_chunk)
     lp, vec = make_inputs(1000, args.scale)
@@ -543,6 +642,8 @@ def run_only(args, local):
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
     flush = torch.empty(32 * 1024 * 1024, dtype=torch.float64, device=dev)
+    if args.only == "price":
+        return pricing(A, m, n, args.steps, args.warmup, flush)
     if args.only == "ada":
         P = hn.Pattern(A)
         D = torch.as_tensor(vec["D"], device=dev)
@@ -623,7 +724,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", default="step", choices=["step", "spmv", "spmv_t", "ada", "bb", "gnn", "batch"],
+    ap.add_argument("--only", default="step", choices=["step", "spmv", "spmv_t", "ada", "bb", "gnn", "batch", "price", "gnn_layer"],
                     help="time one kernel group alone (for profiling); 'step' is the measured workload")
     ap.add_argument("--no-ipm", action="store_true", help="skip the plain GPU IPM solve on the m=2000 LP")
     ap.add_argument("--scale", type=int, default=1, help="--only modes: shrink the LP by this factor (profiling)")

@@ -350,10 +350,12 @@ int hn_gnn_linear(int64_t M, int K1, int K2, const float* X1_dev, const float* X
 /* hn_gnn_linear with N = 64 on the 5th-generation tensor cores: tcgen05.mma
  * (kind::f16, BF16 operands from shared memory, FP32 accumulator in tensor
  * memory), 128 rows per CTA. Same operand rounding as hn_gnn_linear; results
- * differ from it only by accumulation order. Synchronises the stream (it
- * reports a timed-out completion wait as HN_ERR_CUDA). */
+ * differ from it only by accumulation order. A completion wait that times
+ * out leaves Y undefined and sets the stream's flag, which hn_gnn_check
+ * reports (HN_ERR_CUDA) and clears; hn_gnn_check synchronises the stream. */
 int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1_dev, const float* X2_dev, const void* Wt_bf16_dev,
                        const float* bias_dev, int relu, float* Y_dev, void* stream);
+int hn_gnn_check(void* stream);
 /* Backward of hn_gnn_linear with N = 64: G = dY * relu'(Y); dX (M x K, may be
  * NULL; K = 64 or 128) = G W^T; dW (K x 64) = [X1 | X2]^T G; db (64) = sum of
  * G's rows. scratch: >= ceil(M / 64) * (64 K + 64) floats. Deterministic. */

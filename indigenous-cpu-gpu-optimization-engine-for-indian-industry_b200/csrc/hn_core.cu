@@ -46,6 +46,7 @@ Workspace& workspace(cudaStream_t s) {
     w.counter = dmalloc<unsigned>(4);
     w.select = dmalloc<unsigned long long>(kSelectWords);
     check_cuda(cudaMemsetAsync(w.counter, 0, 4 * sizeof(unsigned), s), "workspace init");
+    check_cuda(cudaMemsetAsync(w.select, 0, kSelectWords * sizeof(unsigned long long), s), "workspace init");
     check_cuda(cudaStreamSynchronize(s), "workspace init sync");
     return g_ctx.ws.emplace(s, w).first->second;
 }

@@ -455,6 +455,11 @@ int hn_gnn_linear(int64_t M, int K1, int K2, const float* X1, const float* X2, c
     });
 }
 
+// Timeout flag of the tcgen05 layer: one word of the stream's workspace
+// (select word 7, which the pricing kernels do not use), read and cleared by
+// hn_gnn_check.
+int* umma_flag(cudaStream_t s) { return reinterpret_cast<int*>(workspace(s).select + 7); }
+
 int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1, const float* X2, const void* Wt_bf16,
                        const float* bias, int relu, float* Y, void* stream) {
     return guard("hn_gnn_linear_umma", [&] {
@@ -464,9 +469,6 @@ int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1, const float* 
             fail(HN_ERR_INVALID_ARG, "bad arguments (K1, K2 multiples of 16, K1 + K2 <= 128)");
         if (M == 0) return;
         cudaStream_t s = as_stream(stream);
-        Workspace& w = workspace(s);
-        int* err = reinterpret_cast<int*>(w.select);  // pricing scratch word 0, free between calls
-        check_cuda(cudaMemsetAsync(err, 0, sizeof(int), s), "memset");
         static int attr_device = -1;
         if (attr_device != ctx().device) {
             check_cuda(cudaFuncSetAttribute(gnn_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kUmmaSmem),
@@ -474,12 +476,21 @@ int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1, const float* 
             attr_device = ctx().device;
         }
         gnn_umma_kernel<<<(unsigned)((M + kUmmaM - 1) / kUmmaM), 128, kUmmaSmem, s>>>(
-            M, K1, K2, X1, X2, static_cast<const __nv_bfloat16*>(Wt_bf16), bias, relu, Y, err);
+            M, K1, K2, X1, X2, static_cast<const __nv_bfloat16*>(Wt_bf16), bias, relu, Y, umma_flag(s));
         launched("gnn_umma_kernel");
+    });
+}
+
+int hn_gnn_check(void* stream) {
+    return guard("hn_gnn_check", [&] {
+        require_init();
+        cudaStream_t s = as_stream(stream);
+        int* f = umma_flag(s);
         int h = 0;
-        check_cuda(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H flag");
-        check_cuda(cudaStreamSynchronize(s), "umma sync");
-        if (h) fail(HN_ERR_CUDA, "tensor-core layer: MMA completion wait timed out");
+        check_cuda(cudaMemcpyAsync(&h, f, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H flag");
+        check_cuda(cudaMemsetAsync(f, 0, sizeof(int), s), "memset flag");
+        check_cuda(cudaStreamSynchronize(s), "flag sync");
+        if (h) fail(HN_ERR_CUDA, "tensor-core layer: an MMA completion wait timed out");
     });
 }
 

@@ -236,6 +236,7 @@ def forward(model: Model, B: Batch):
         hv.append(lin(hv[-1], a, f"v{l}", 1, B.n))
     ov = lin(hv[-1], None, "hv", 0, B.n)
     oc = lin(hc[-1], None, "hc", 0, B.m)
+    hn.check(lib.hn_gnn_check(None))
     return {"hv": hv, "hc": hc, "ac": ac, "av": av, "ov": ov, "oc": oc}
 
 

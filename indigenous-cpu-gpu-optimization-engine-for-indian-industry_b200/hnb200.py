@@ -102,6 +102,7 @@ SIGNATURES = {
     "hn_gnn_cast_weights": [C.c_int, _vp, _vp, _vp, _vp],
     "hn_gnn_linear": [_i64, C.c_int, C.c_int, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp],
     "hn_gnn_linear_umma": [_i64, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp],
+    "hn_gnn_check": [_vp],
     "hn_gnn_linear_bwd": [_i64, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _i64,
                           _vp],
     "hn_gnn_split_grad": [_i64, _vp, _vp, _vp, _vp],

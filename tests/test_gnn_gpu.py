@@ -125,6 +125,7 @@ def test_tcgen05_layer_matches_mma_sync_layer(hn, torch_cuda, K1, K2, relu, M):
         else:
             hn.check(lib.hn_gnn_linear_umma(M, K1, K2, X1.data_ptr(), x2, Wt.data_ptr(), b.data_ptr(), relu,
                                             Y.data_ptr(), None))
+            hn.check(lib.hn_gnn_check(None))
         torch.cuda.synchronize()
         ys.append(Y.cpu().numpy().astype(np.float64))
     assert np.all(np.isfinite(ys[1]))
