@@ -349,10 +349,12 @@ int hn_gnn_linear(int64_t M, int K1, int K2, const float* X1_dev, const float* X
                   int N, const float* bias_dev, int relu, float* Y_dev, void* stream);
 /* hn_gnn_linear with N = 64 on the 5th-generation tensor cores: tcgen05.mma
  * (kind::f16, BF16 operands from shared memory, FP32 accumulator in tensor
- * memory), 128 rows per CTA. Same operand rounding as hn_gnn_linear; results
- * differ from it only by accumulation order. A completion wait that times
- * out leaves Y undefined and sets the stream's flag, which hn_gnn_check
- * reports (HN_ERR_CUDA) and clears; hn_gnn_check synchronises the stream. */
+ * memory); a persistent CTA per SM streams 128-row tiles of X in by bulk
+ * copy. X1, X2, Y and Wt must be 16-byte aligned. Same operand rounding as
+ * hn_gnn_linear; results differ from it only by accumulation order. A wait
+ * that times out leaves Y undefined and sets the stream's flag, which
+ * hn_gnn_check reports (HN_ERR_CUDA) and clears; hn_gnn_check synchronises
+ * the stream. */
 int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1_dev, const float* X2_dev, const void* Wt_bf16_dev,
                        const float* bias_dev, int relu, float* Y_dev, void* stream);
 int hn_gnn_check(void* stream);

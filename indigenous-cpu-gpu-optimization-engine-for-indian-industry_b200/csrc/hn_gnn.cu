@@ -155,20 +155,40 @@ __global__ void __launch_bounds__(kGT) gnn_gemm_kernel(int64_t M, int K1, int K2
 }
 
 // ---- the same layer on the 5th-generation tensor cores (tcgen05) ----
-// One CTA (4 warps) computes a 128-row x 64-column tile of Y with K <= 128:
-// both operands are staged in shared memory in the canonical K-major,
-// no-swizzle layout (core matrices of 8 rows x 16 bytes; the next 8-row
-// group 128 bytes on, the next 8-element K chunk LBO bytes on), one thread
-// issues K / 16 tcgen05.mma (kind::f16, BF16 in, FP32 accumulated in 64
-// TMEM columns), a commit signals an mbarrier, and each warp reads its 32
-// rows back with tcgen05.ld for the bias/ReLU epilogue. The mbarrier wait is
-// bounded: on a timeout the kernel records it in *err and still frees TMEM.
+// A persistent kernel, one CTA (8 warps) per SM, walks 128-row tiles of Y
+// (tile t, t + grid, ...). Per tile:
+//   1. the tile's rows of X1 and of X2, contiguous in memory, arrive by one
+//      bulk copy each (cp.async.bulk completing on the stage's mbarrier);
+//      two stages, so tile i + 2 is in flight while tile i is processed;
+//   2. the CTA rounds the staged FP32 rows to BF16 into A in the canonical
+//      K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes; the
+//      next 8-row group 128 bytes on, the next 8-element K chunk LBO on);
+//   3. one thread issues K / 16 tcgen05.mma (kind::f16, BF16 in, FP32
+//      accumulated in 64 TMEM columns) and commits to an mbarrier;
+//   4. each warp reads 32 rows x 32 columns back (tcgen05.ld), adds the bias,
+//      applies ReLU, writes the block into its own part of an output staging
+//      tile and reads it back row-wise, so that its global stores cover whole
+//      128-byte lines (no wait on the stores anywhere in the loop).
+// Lane mappings keep the 128-bit shared loads of step 2 and the stores of
+// steps 2 and 4 free of bank conflicts when K1 and K2 are multiples of 32:
+// in step 2 a half-warp converts one 8-element chunk of each of 8 rows, the
+// chunk index rotating with the row; in step 4 each lane rotates its 8
+// four-column groups by its lane index, and the row-wise read-back is
+// contiguous per quarter-warp. Every mbarrier wait is bounded: on a timeout
+// the CTA records it in *err, waits (bounded) for the copies and the MMA it
+// issued, frees TMEM and returns.
 constexpr int kUmmaM = 128;
+constexpr int kUmmaT = 256;
 constexpr uint32_t kUmmaSbo = 128;
 constexpr uint32_t kUmmaLboA = (kUmmaM / 8) * 128;  // 2048
 constexpr uint32_t kUmmaLboB = (kH / 8) * 128;      // 1024
 constexpr uint32_t kUmmaSpin = 1u << 24;
-constexpr int kUmmaSmem = (kUmmaM + kH) * kMaxK * 2;  // 48 KB dynamic
+constexpr int kUmmaStage = kUmmaM * kMaxK * 4;                // 64 KB of FP32 rows
+constexpr int kUmmaOffA = 2 * kUmmaStage;                     // 128 KB
+constexpr int kUmmaOffB = kUmmaOffA + kUmmaM * kMaxK * 2;     // + 32 KB
+constexpr int kUmmaOffOut = kUmmaOffB + kH * kMaxK * 2;       // + 16 KB
+constexpr int kUmmaSmem = kUmmaOffOut + kUmmaM * kH * 4;      // + 32 KB = 208 KB
+static_assert(kUmmaSmem <= 227 * 1024, "tcgen05 layer shared memory");
 
 __device__ __forceinline__ uint64_t umma_smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
     // start address, leading and stride byte offsets (16-byte units), version 1, no swizzle
@@ -183,119 +203,205 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-__global__ void __launch_bounds__(128) gnn_umma_kernel(int64_t M, int K1, int K2, const float* __restrict__ X1,
-                                                      const float* __restrict__ X2,
-                                                      const __nv_bfloat16* __restrict__ Bt,
-                                                      const float* __restrict__ bias, int relu,
-                                                      float* __restrict__ Y, int* err) {
-    extern __shared__ __align__(1024) uint8_t umma_smem[];
-    uint8_t* sA = umma_smem;                        // 128 x K BF16, 32 KB at K = 128
-    uint8_t* sB = umma_smem + kUmmaM * kMaxK * 2;   // 64 x K BF16, 16 KB
-    __shared__ __align__(8) uint64_t mbar;
-    __shared__ uint32_t s_tmem;
-    const int K = K1 + K2, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int64_t row0 = blockIdx.x * (int64_t)kUmmaM;
-    // operands: 8 consecutive K elements (16 bytes) per store
-    for (int idx = tid; idx < kUmmaM * (K / 8); idx += 128) {
-        const int r = idx / (K / 8), kc = idx % (K / 8);
-        const int64_t gr = row0 + r;
-        float v[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) v[u] = 0.f;
-        if (gr < M) {
-            const int k = kc * 8;
-            const float* src = k < K1 ? X1 + gr * K1 + k : X2 + gr * K2 + (k - K1);
-#pragma unroll
-            for (int u = 0; u < 8; ++u) v[u] = src[u];
-        }
-        uint32_t w[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const __nv_bfloat16 lo = __float2bfloat16_rn(v[2 * u]), hi = __float2bfloat16_rn(v[2 * u + 1]);
-            w[u] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
-        }
-        *reinterpret_cast<uint4*>(sA + kc * kUmmaLboA + (r >> 3) * kUmmaSbo + (r & 7) * 16) =
-            make_uint4(w[0], w[1], w[2], w[3]);
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < kUmmaSpin; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
     }
-    for (int idx = tid; idx < kH * (K / 8); idx += 128) {
-        const int n = idx / (K / 8), kc = idx % (K / 8);
+    return false;
+}
+
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ int umma_rows(int64_t M, int64_t tile) {
+    const int64_t r = M - tile * kUmmaM;
+    return (int)(r < kUmmaM ? r : kUmmaM);
+}
+
+__global__ void __launch_bounds__(kUmmaT, 1) gnn_umma_kernel(int64_t M, int K1, int K2, const float* __restrict__ X1,
+                                                             const float* __restrict__ X2,
+                                                             const __nv_bfloat16* __restrict__ Bt,
+                                                             const float* __restrict__ bias, int relu,
+                                                             float* __restrict__ Y, int* err) {
+    extern __shared__ __align__(1024) uint8_t umma_smem[];
+    uint8_t* sA = umma_smem + kUmmaOffA;
+    uint8_t* sB = umma_smem + kUmmaOffB;
+    uint8_t* sOut = umma_smem + kUmmaOffOut;
+    __shared__ __align__(8) uint64_t full[2];
+    __shared__ __align__(8) uint64_t mma_bar;
+    __shared__ uint32_t s_tmem;
+    __shared__ float s_bias[kH];
+    const int K = K1 + K2, Kc = K / 8;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t ntiles = (M + kUmmaM - 1) / kUmmaM;
+    const int64_t grid = gridDim.x;
+
+    // weights: 64 x K BF16 into the canonical layout, bias
+    for (int idx = tid; idx < kH * Kc; idx += kUmmaT) {
+        const int n = idx / Kc, kc = idx % Kc;
         *reinterpret_cast<uint4*>(sB + kc * kUmmaLboB + (n >> 3) * kUmmaSbo + (n & 7) * 16) =
             *reinterpret_cast<const uint4*>(Bt + (int64_t)n * K + kc * 8);
     }
+    if (tid < kH) s_bias[tid] = bias ? bias[tid] : 0.f;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                      "r"(kH));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
+    const uint32_t bar_full0 = smem_u32(&full[0]), bar_mma = smem_u32(&mma_bar);
+    const uint32_t stage0 = smem_u32(umma_smem);
+    // tile t into stage s: X1 rows at the stage start, X2 rows 128 * K1 floats on
+    auto issue = [&](int64_t t, int s) {
+        const uint32_t rows = (uint32_t)umma_rows(M, t), bar = bar_full0 + 8 * s;
+        mbar_expect(bar, rows * 4u * (uint32_t)K);
+        bulk_load(stage0 + s * kUmmaStage, X1 + t * kUmmaM * K1, rows * 4u * (uint32_t)K1, bar);
+        if (K2) bulk_load(stage0 + s * kUmmaStage + kUmmaM * 4 * K1, X2 + t * kUmmaM * K2, rows * 4u * (uint32_t)K2, bar);
+    };
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_full0));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_full0 + 8));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_mma));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int p = 0; p < 2; ++p)
+            if (blockIdx.x + p * grid < ntiles) issue(blockIdx.x + p * grid, p);
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // staged operands -> tensor core
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // staged weights -> tensor core
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
-    if (tid == 0) {
-        const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-        for (int ks = 0; ks < K / 16; ++ks) {
-            const uint64_t da = umma_smem_desc(a0 + 2 * ks * kUmmaLboA, kUmmaLboA, kUmmaSbo);
-            const uint64_t db = umma_smem_desc(b0 + 2 * ks * kUmmaLboB, kUmmaLboB, kUmmaSbo);
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                "l"(da), "l"(db), "r"(kUmmaIdesc), "r"(ks > 0 ? 1 : 0));
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         smem_u32(&mbar))
-                     : "memory");
-    }
-    uint32_t done = 0;
-    for (uint32_t it = 0; it < kUmmaSpin && !done; ++it) {
-        asm volatile(
-            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, P1;\n\t}\n"
-            : "=r"(done)
-            : "r"(smem_u32(&mbar)), "r"(0u)
-            : "memory");
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!done) {
-        if (lane == 0) atomicExch(err, 1);
-    } else {
-        uint32_t r[64];
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,"
-            "%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63},"
-            " [%64];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-              "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
-              "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-              "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]),
-              "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]),
-              "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]),
-              "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]),
-              "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
-            : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        const int64_t gr = row0 + warp * 32 + lane;  // TMEM lane = row of the tile
-        if (gr < M) {
-            float4* out = reinterpret_cast<float4*>(Y + gr * kH);
-#pragma unroll
-            for (int c = 0; c < kH; c += 4) {
-                float v[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    float t = __uint_as_float(r[c + u]) + (bias ? bias[c + u] : 0.f);
-                    v[u] = relu ? fmaxf(t, 0.f) : t;
+
+    const int q = warp & 3, half = warp >> 2;  // TMEM lanes 32q.., columns 32 half..
+    const int orow = 32 * q + lane, rot = lane & 7;
+    bool bad = false;
+    int64_t i = 0, t = blockIdx.x;
+    for (; t < ntiles; t += grid, ++i) {
+        const int s = (int)(i & 1);
+        const int rows = umma_rows(M, t);
+        const bool ok = !bad && mbar_wait(bar_full0 + 8 * s, (uint32_t)((i >> 1) & 1));
+        if (ok) {
+            const uint8_t* x1 = umma_smem + s * kUmmaStage;
+            const uint8_t* x2 = x1 + kUmmaM * 4 * K1;
+            // lane-item u: half-warp h = u / 16 converts chunk ((r / 2) + h / 16) mod Kc
+            // of rows 8 (h mod 16) + r, r = l mod 8; lane l < 8 takes the half
+            // (r mod 2) of it, lane l + 8 the other half
+            for (int u = tid; u < 256 * Kc; u += kUmmaT) {
+                const int h = u >> 4, l = u & 15;
+                const int rl = l & 7, p = (l & 1) ^ (l >> 3);
+                const int kc = ((rl >> 1) + (h >> 4)) % Kc;
+                const int r = ((h & 15) << 3) | rl;
+                const int k0 = 8 * kc + 4 * p;
+                uint2 w = make_uint2(0u, 0u);
+                if (r < rows) {
+                    const float4 a = k0 < K1 ? *reinterpret_cast<const float4*>(x1 + 4 * (r * K1 + k0))
+                                             : *reinterpret_cast<const float4*>(x2 + 4 * (r * K2 + k0 - K1));
+                    w.x = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a.x)) |
+                          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a.y)) << 16);
+                    w.y = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a.z)) |
+                          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a.w)) << 16);
                 }
-                out[c / 4] = make_float4(v[0], v[1], v[2], v[3]);
+                *reinterpret_cast<uint2*>(sA + kc * kUmmaLboA + (h & 15) * kUmmaSbo + rl * 16 + p * 8) = w;
             }
         }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // A -> tensor core
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        if (__syncthreads_or(!ok)) {
+            bad = true;
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+            if (t + 2 * grid < ntiles) issue(t + 2 * grid, s);  // stage s is free again
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+            for (int ks = 0; ks < K / 16; ++ks) {
+                const uint64_t da = umma_smem_desc(a0 + 2 * ks * kUmmaLboA, kUmmaLboA, kUmmaSbo);
+                const uint64_t db = umma_smem_desc(b0 + 2 * ks * kUmmaLboB, kUmmaLboB, kUmmaSbo);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(kUmmaIdesc), "r"(ks > 0 ? 1 : 0));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_mma)
+                         : "memory");
+        }
+        // warp-uniform outcome: tcgen05.ld below is a .sync.aligned warp instruction
+        if (!__all_sync(0xffffffffu, mbar_wait(bar_mma, (uint32_t)(i & 1)))) {
+            bad = true;  // the next iteration's barrier takes every thread to the exit
+            continue;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint32_t v[32];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+              "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+              "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+            : "r"(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * half)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        // rotate the 8 four-column groups left by rot (three conditional steps)
+#pragma unroll
+        for (int b = 1; b < 8; b <<= 1) {
+            uint32_t w[32];
+#pragma unroll
+            for (int e = 0; e < 32; ++e) w[e] = v[(e + 4 * b) & 31];
+            if (rot & b) {
+#pragma unroll
+                for (int e = 0; e < 32; ++e) v[e] = w[e];
+            }
+        }
+        if (orow < rows) {
+            uint8_t* o = sOut + orow * (kH * 4) + half * 128;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int g = (c + rot) & 7;  // column group held in v[4c .. 4c + 3]
+                float w[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const float x = __uint_as_float(v[4 * c + e]) + s_bias[32 * half + 4 * g + e];
+                    w[e] = relu ? fmaxf(x, 0.f) : x;
+                }
+                *reinterpret_cast<float4*>(o + 16 * g) = make_float4(w[0], w[1], w[2], w[3]);
+            }
+        }
+        __syncwarp();
+        // this warp's 32 x 32 block, 4 rows (4 x 128 bytes) per store instruction
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int rr = 32 * q + 4 * j + (lane >> 3);
+            if (rr < rows)
+                *reinterpret_cast<float4*>(Y + (t * kUmmaM + rr) * kH + 32 * half + 4 * (lane & 7)) =
+                    *reinterpret_cast<const float4*>(sOut + rr * (kH * 4) + half * 128 + 16 * (lane & 7));
+        }
+        __syncwarp();
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid == 0 && bad) {
+        // a wait timed out in iteration i: settle what is still in flight
+        // (the copies of tiles i and i + 1 and the MMA of iteration i - 1)
+        atomicExch(err, 1);
+        if (t < ntiles) mbar_wait(bar_full0 + 8 * (int)(i & 1), (uint32_t)((i >> 1) & 1));
+        if (t + grid < ntiles) mbar_wait(bar_full0 + 8 * (int)((i + 1) & 1), (uint32_t)(((i + 1) >> 1) & 1));
+        if (i > 0) mbar_wait(bar_mma, (uint32_t)((i - 1) & 1));
+    }
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kH));
 }
@@ -467,6 +573,9 @@ int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1, const float* 
         const int K = K1 + K2;
         if (M < 0 || K1 <= 0 || K2 < 0 || K > kMaxK || K1 % 16 || K2 % 16 || !X1 || (K2 && !X2) || !Wt_bf16 || !Y)
             fail(HN_ERR_INVALID_ARG, "bad arguments (K1, K2 multiples of 16, K1 + K2 <= 128)");
+        const auto misaligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) != 0; };
+        if (misaligned(X1) || (K2 && misaligned(X2)) || misaligned(Y) || misaligned(Wt_bf16))
+            fail(HN_ERR_INVALID_ARG, "X1, X2, Y and the weights must be 16-byte aligned (bulk copies)");
         if (M == 0) return;
         cudaStream_t s = as_stream(stream);
         static int attr_device = -1;
@@ -475,7 +584,8 @@ int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1, const float* 
                        "umma smem attribute");
             attr_device = ctx().device;
         }
-        gnn_umma_kernel<<<(unsigned)((M + kUmmaM - 1) / kUmmaM), 128, kUmmaSmem, s>>>(
+        const int64_t tiles = (M + kUmmaM - 1) / kUmmaM;
+        gnn_umma_kernel<<<(unsigned)std::min<int64_t>(tiles, ctx().sm_count), kUmmaT, kUmmaSmem, s>>>(
             M, K1, K2, X1, X2, static_cast<const __nv_bfloat16*>(Wt_bf16), bias, relu, Y, umma_flag(s));
         launched("gnn_umma_kernel");
     });

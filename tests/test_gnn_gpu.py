@@ -100,10 +100,13 @@ def test_training_lowers_the_loss_and_warm_start_keeps_the_answer(hn, torch_cuda
     assert np.mean(it_warm) <= np.mean(it_cold) - 1.0, (it_warm, it_cold)
 
 
-@pytest.mark.parametrize("K1,K2,relu,M", [(16, 0, 1, 1000), (64, 64, 1, 4097), (64, 0, 0, 130), (32, 32, 1, 128)])
+@pytest.mark.parametrize("K1,K2,relu,M", [(16, 0, 1, 1000), (64, 64, 1, 4097), (64, 0, 0, 130), (32, 32, 1, 128),
+                                            (64, 64, 1, 148 * 128 * 3 + 77), (16, 0, 0, 40000), (48, 16, 1, 20001)])
 def test_tcgen05_layer_matches_mma_sync_layer(hn, torch_cuda, K1, K2, relu, M):
     """hn_gnn_linear_umma (tcgen05, TMEM accumulator) against hn_gnn_linear
-    (mma.sync): same BF16 operands, FP32 accumulation in a different order."""
+    (mma.sync): same BF16 operands, FP32 accumulation in a different order.
+    The larger cases give every persistent CTA several tiles (both staging
+    buffers cycle more than once) and end on a partial tile."""
     torch = torch_cuda
     g = torch.Generator(device="cuda").manual_seed(K1 + K2 + M)
     X1 = torch.randn((M, K1), generator=g, device="cuda")
