@@ -617,6 +617,97 @@ def gnn_layer(steps, warmup, rows=1 << 20):
     return res
 
 
+def _mps_text(lp: dict, name: str) -> bytes:
+    """Free-layout MPS of an LP dict (EQ rows, x >= 0), column by column."""
+    m, n = lp["m"], lp["n"]
+    rp, ci, val = lp["rp"], lp["ci"], lp["val"]
+    order = np.argsort(ci, kind="stable")
+    rows = np.repeat(np.arange(m), np.diff(rp.astype(np.int64)))[order]
+    cols = ci[order].astype(np.int64)
+    vals = val[order]
+    out = [f"NAME {name}", "ROWS", " N obj"] + [f" E r{i}" for i in range(m)] + ["COLUMNS"]
+    starts = np.searchsorted(cols, np.arange(n + 1))
+    for j in range(n):
+        out.append(f"    v{j} obj {lp['c'][j]!r}")
+        out.extend(f"    v{j} r{i} {a!r}" for i, a in zip(rows[starts[j]:starts[j + 1]].tolist(),
+                                                        vals[starts[j]:starts[j + 1]].tolist()))
+    out.append("RHS")
+    out.extend(f"    rhs r{i} {b!r}" for i, b in enumerate(lp["b"].tolist()))
+    out.append("ENDATA")
+    return ("\n".join(out) + "\n").encode()
+
+
+def mps_io(sample_m: int = 2000):
+    """MPS reading into device CSR. (1) The product reader (hn_mps, host C++)
+    and the reference's MPSParser::parse_string on the same text: a seeded
+    LP of the C0 generator (m = sample_m, n = 2.5 m, 6 nonzeros per column).
+    (2) The large LP (m = 200k, n = 500k, 5.16M nonzeros) through the
+    product reader and hn_csr_create_coo; the reference's parser looks rows
+    up by linear search (quadratic in the row count) and is not run there.
+    (3) hn_csr_create_coo against the reference's SparseMatrix::from_triplets
+    on the large LP's triplets. Wall-clock, best of 3."""
+    import ctypes as C
+
+    import torch
+
+    import hnb200 as hn
+    import lpgen
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    def reader_ms(text):
+        best = float("inf")
+        for _ in range(3):
+            h = C.c_void_p()
+            t0 = time.perf_counter()
+            hn.host_check(hn.host().hn_mps_read_string(text, len(text), -1, C.byref(h)))
+            best = min(best, (time.perf_counter() - t0) * 1e3)
+            hn.host().hn_mps_free(h)
+        return best
+
+    res = {"workload": "MPS text -> device CSR"}
+    small = lpgen.lp_uniform(sample_m, int(2.5 * sample_m), 6, seed=1000)
+    t_small = _mps_text(small, "C0")
+    ref_ms = None
+    if oracle.ref() is not None:
+        ref_ms = min(oracle.ref_mps_parse_ms(t_small) for _ in range(3))
+    ours = reader_ms(t_small)
+    res["c0_sample"] = {"m": small["m"], "n": small["n"], "nnz": int(small["rp"][-1]), "bytes": len(t_small),
+                        "reader_ms": round(ours, 2), "reference_parser_ms": None if ref_ms is None else round(ref_ms, 2),
+                        "speedup": None if ref_ms is None else round(ref_ms / ours, 1)}
+    big = lpgen.lp_zipf()
+    t_big = _mps_text(big, "C1")
+    ours_big = reader_ms(t_big)
+    h = C.c_void_p()
+    hn.host_check(hn.host().hn_mps_read_string(t_big, len(t_big), -1, C.byref(h)))
+    nt = C.c_int64()
+    hn.host_check(hn.host().hn_mps_shape(h, None, None, C.byref(nt), None))
+    tr, tc, tv = np.empty(nt.value, np.int64), np.empty(nt.value, np.int64), np.empty(nt.value)
+    hn.host_check(hn.host().hn_mps_arrays(h, hn._p(tr, C.c_int64), hn._p(tc, C.c_int64), hn._p(tv, C.c_double),
+                                          None, None, None, None, None, None, None, None))
+    hn.host().hn_mps_free(h)
+    m, n = big["m"], big["n"]
+    coo = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        A = hn.Csr.from_coo(m, n, tr, tc, tv, transpose=False, autotune=False)
+        torch.cuda.synchronize()
+        coo.append((time.perf_counter() - t0) * 1e3)
+        A.close()
+    ref_ft = None
+    if oracle.ref() is not None:
+        t0 = time.perf_counter()
+        oracle.ref_from_triplets(m, n, tr, tc, tv)
+        ref_ft = (time.perf_counter() - t0) * 1e3
+    res["c1_5m"] = {"m": m, "n": n, "nnz": int(nt.value), "bytes": len(t_big), "reader_ms": round(ours_big, 1),
+                    "reader_MB/s": round(len(t_big) / (ours_big * 1e-3) / 1e6, 1),
+                    "coo_to_device_csr_ms": round(min(coo), 2),
+                    "reference_from_triplets_ms": None if ref_ft is None else round(ref_ft, 1)}
+    return res
+
+
 def run_only(args, local):
     """Single kernel group on the same LP (profiling aid). spmv / spmv_t flush
     L2 between launches by writing a 256 MB buffer; ada streams 11.6 GB."""
@@ -634,6 +725,8 @@ def run_only(args, local):
         return batched_ipm(args.batch_k, args.batch_sample)
     if args.only == "gnn_layer":
         return gnn_layer(args.steps, args.warmup)
+    if args.only == "mps":
+        return mps_io()
     if args.only == "gnn":
         return gnn_warm(args.gnn_train, args.gnn_eval, args.gnn_mlo, args.gnn_mhi, args.gnn_epochs, args.gnn_chunk)
     lp, vec = make_inputs(1000, args.scale)
@@ -724,7 +817,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", default="step", choices=["step", "spmv", "spmv_t", "ada", "bb", "gnn", "batch", "price", "gnn_layer"],
+    ap.add_argument("--only", default="step", choices=["step", "spmv", "spmv_t", "ada", "bb", "gnn", "batch", "price", "gnn_layer",
+                             "mps"],
                     help="time one kernel group alone (for profiling); 'step' is the measured workload")
     ap.add_argument("--no-ipm", action="store_true", help="skip the plain GPU IPM solve on the m=2000 LP")
     ap.add_argument("--scale", type=int, default=1, help="--only modes: shrink the LP by this factor (profiling)")

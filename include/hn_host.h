@@ -92,6 +92,31 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
                       int64_t* iterations, double* x_out, hn_batch_stats* stats, int* warm_used, double* y_out,
                       double* s_out);
 
+/* ---- MPS reader (MPSParser, core/model/mps_parser.hpp:18-78) ----
+ * Reads MPS text with the reference's results: free/fixed layout (format -1
+ * detects it as mps_parser.cpp:124-158 does, 0 free, 1 fixed), sections NAME,
+ * OBJSENSE, ROWS, COLUMNS (integer MARKER blocks), RHS (with its fixed-layout
+ * retry), RANGES, BOUNDS; SOS / QUADOBJ / QCMATRIX records are read past and
+ * counted. Rows and columns are looked up by hash (first occurrence of a
+ * name wins, as in the reference's linear searches). The constraint
+ * coefficients come out as triplets in file order; hn_csr_create_coo makes
+ * the device CSR the reference's from_triplets would make. */
+typedef struct hn_mps hn_mps;
+int hn_mps_read_file(const char* path, int format, hn_mps** out);
+int hn_mps_read_string(const char* text, int64_t len, int format, hn_mps** out);
+/* m rows (constraints), n columns, triplet count, objective sense (1 = MAX) */
+int hn_mps_shape(const hn_mps* h, int64_t* m, int64_t* n, int64_t* ntriplets, int* maximize);
+/* Copies out (each may be NULL): triplets (ntriplets), c / lb / ub / vtype
+ * (n; vtype in model::VarType numbering), rhs / sense (0 LE, 1 GE, 2 EQ) /
+ * range_lo / range_hi (m). */
+int hn_mps_arrays(const hn_mps* h, int64_t* trow, int64_t* tcol, double* tval, double* c, double* rhs,
+                  int32_t* sense, double* lb, double* ub, double* range_lo, double* range_hi, int32_t* vtype);
+int hn_mps_counts(const hn_mps* h, int64_t* warnings, int64_t* sos_records, int64_t* quadratic_records);
+const char* hn_mps_warning(const hn_mps* h, int64_t i);
+/* what -1: problem name; 0: row i's name; 1: column i's name (NULL if none) */
+const char* hn_mps_name(const hn_mps* h, int what, int64_t i);
+int hn_mps_free(hn_mps* h);
+
 /* B200Backend through C: the matrix arrives as the reference's three vectors
  * each call; the backend keeps it resident between calls. */
 typedef struct hn_backend hn_backend;

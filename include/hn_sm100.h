@@ -106,6 +106,15 @@ int hn_stream_sync(void* stream);
 int hn_csr_create(int64_t m, int64_t n, const uint64_t* row_ptr_host,
                   const uint64_t* col_idx_host, const double* val_host, unsigned flags,
                   hn_csr** out);
+/* A from `count` triplets (host arrays; rows in [0, m), cols in [0, n), any
+ * order, duplicates allowed), built on the device with the semantics of
+ * SparseMatrix::from_triplets (sparse_matrix.cpp:8-53, sum_duplicates
+ * :230-262): entries ordered by (row, column), equal (row, column) entries
+ * summed in input order, exact-zero sums dropped -- the matrix MPSParser
+ * assembles from its coefficient list (mps_parser.cpp:106-111). Two stable
+ * radix passes on the device, then the same set-up as hn_csr_create. */
+int hn_csr_create_coo(int64_t m, int64_t n, int64_t count, const int64_t* rows_host, const int64_t* cols_host,
+                      const double* val_host, unsigned flags, hn_csr** out);
 /* New values for the same pattern (host array, nnz entries); A^T follows. */
 int hn_csr_set_values(hn_csr* A, const double* val_host);
 int hn_csr_destroy(hn_csr* A);

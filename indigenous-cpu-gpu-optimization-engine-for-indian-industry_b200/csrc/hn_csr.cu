@@ -226,6 +226,34 @@ void free_transpose(hn_csr* A) {
     A->perm[1] = nullptr;
 }
 
+// Stable LSD radix sort of nnz (key, value) pairs on the keys' low bits
+// (keys in [0, range)); kA/vA hold the result, kB/vB are scratch.
+void radix_sort_pairs(int32_t*& kA, int32_t*& vA, int32_t*& kB, int32_t*& vB, int64_t nnz, int64_t range,
+                      cudaStream_t s) {
+    int bits = 0;
+    while (bits < 31 && (int64_t(1) << bits) < range) ++bits;
+    const int64_t ntiles = (nnz + kSortTile - 1) / kSortTile;
+    if (nnz == 0 || bits == 0) return;
+    int32_t* counts = dmalloc<int32_t>(kRadix * ntiles);
+    for (int shift = 0; shift < bits; shift += kRadixBits) {
+        radix_upsweep<<<(unsigned)ntiles, kSortThreads, 0, s>>>(kA, nnz, shift, counts, ntiles);
+        launched("radix_upsweep");
+        scan_exclusive_i32(counts, counts, kRadix * ntiles, s);
+        radix_downsweep<<<(unsigned)ntiles, kSortThreads, 0, s>>>(kA, vA, kB, vB, nnz, shift, counts, ntiles);
+        launched("radix_downsweep");
+        std::swap(kA, kB);
+        std::swap(vA, vB);
+    }
+    check_cuda(cudaStreamSynchronize(s), "radix sort sync");
+    dfree(counts);
+}
+
+__global__ void gather_i32_kernel(int64_t nnz, const int32_t* __restrict__ perm, const int32_t* __restrict__ src,
+                                  int32_t* __restrict__ dst) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p < nnz) dst[p] = src[perm[p]];
+}
+
 void build_transpose(hn_csr* A, cudaStream_t s) {
     const int64_t nnz = A->nnz, m = A->m, n = A->n;
     A->rpT = dmalloc<int32_t>(n + 1);
@@ -238,23 +266,7 @@ void build_transpose(hn_csr* A, cudaStream_t s) {
         iota_kernel<<<blocks(nnz), 256, 0, s>>>(vA, nnz);
         launched("iota_kernel");
     }
-    int bits = 0;
-    while (bits < 31 && (int64_t(1) << bits) < n) ++bits;
-    const int64_t ntiles = (nnz + kSortTile - 1) / kSortTile;
-    if (nnz > 0 && bits > 0) {
-        int32_t* counts = dmalloc<int32_t>(kRadix * ntiles);
-        for (int shift = 0; shift < bits; shift += kRadixBits) {
-            radix_upsweep<<<(unsigned)ntiles, kSortThreads, 0, s>>>(kA, nnz, shift, counts, ntiles);
-            launched("radix_upsweep");
-            scan_exclusive_i32(counts, counts, kRadix * ntiles, s);
-            radix_downsweep<<<(unsigned)ntiles, kSortThreads, 0, s>>>(kA, vA, kB, vB, nnz, shift,
-                                                                      counts, ntiles);
-            launched("radix_downsweep");
-            std::swap(kA, kB);
-            std::swap(vA, vB);
-        }
-        dfree(counts);
-    }
+    radix_sort_pairs(kA, vA, kB, vB, nnz, n, s);
     // kA: sorted column keys, vA: CSR position of each sorted entry
     int32_t* row_of = dmalloc<int32_t>(nnz);
     if (m > 0 && nnz > 0) {
@@ -494,6 +506,74 @@ void convert_csr(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci,
     }
 }
 
+// CSR (device rp, ci, val) of m x n from nnz triplets already on the device
+// (rows r, columns c, values v), with SparseMatrix::from_triplets semantics:
+// entries ordered by (row, column), equal (row, column) entries summed in
+// input order, exact-zero sums dropped. Two stable radix passes (columns,
+// then rows) carry each entry's input position.
+void coo_to_csr(int64_t m, int64_t n, int64_t nnz, const int32_t* r, const int32_t* c, const double* v,
+                int32_t** rp_out, int32_t** ci_out, double** val_out, int64_t* nnz_out, cudaStream_t s) {
+    int32_t* kA = dmalloc<int32_t>(nnz);
+    int32_t* kB = dmalloc<int32_t>(nnz);
+    int32_t* vA = dmalloc<int32_t>(nnz);
+    int32_t* vB = dmalloc<int32_t>(nnz);
+    if (nnz > 0) {
+        check_cuda(cudaMemcpyAsync(kA, c, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice, s), "copy keys");
+        iota_kernel<<<blocks(nnz), 256, 0, s>>>(vA, nnz);
+        launched("iota_kernel");
+    }
+    radix_sort_pairs(kA, vA, kB, vB, nnz, n, s);  // by column
+    if (nnz > 0) {
+        gather_i32_kernel<<<blocks(nnz), 256, 0, s>>>(nnz, vA, r, kA);
+        launched("gather_i32_kernel");
+    }
+    radix_sort_pairs(kA, vA, kB, vB, nnz, m, s);  // then by row (stable)
+    // kA: rows in (row, column) order, vA: input position of each entry
+    int32_t* ci_raw = kB;  // reuse
+    int32_t* keep = vB;    // reuse
+    double* val_raw = dmalloc<double>(nnz);
+    double* run_sum = dmalloc<double>(nnz);
+    unsigned long long* kept_d = dmalloc<unsigned long long>(1);
+    unsigned long long kept = 0;
+    if (nnz > 0) {
+        gather_t_kernel<<<blocks(nnz), 256, 0, s>>>(nnz, vA, c, v, ci_raw, val_raw);
+        launched("gather_t_kernel");
+        runs_kernel<<<blocks(nnz), 256, 0, s>>>(nnz, kA, ci_raw, val_raw, run_sum, keep);
+        launched("runs_kernel");
+        check_cuda(cudaMemsetAsync(kept_d, 0, sizeof(unsigned long long), s), "memset");
+        sum_i32_kernel<<<grid_for(nnz, 256, 1024), 256, 0, s>>>(nnz, keep, kept_d);
+        launched("sum_i32_kernel");
+        check_cuda(cudaMemcpyAsync(&kept, kept_d, sizeof(kept), cudaMemcpyDeviceToHost, s), "D2H kept");
+        check_cuda(cudaStreamSynchronize(s), "coo sync");
+    }
+    const int64_t nk = static_cast<int64_t>(kept);
+    int32_t* pos = dmalloc<int32_t>(nnz);
+    int32_t* ci = dmalloc<int32_t>(nk);
+    double* val = dmalloc<double>(nk);
+    int32_t* key = dmalloc<int32_t>(nk);
+    int32_t* cnt = dmalloc<int32_t>(m + 1);
+    check_cuda(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (m + 1), s), "memset cnt");
+    if (nnz > 0) {
+        scan_exclusive_i32(keep, pos, nnz, s);
+        compact_kernel<<<blocks(nnz), 256, 0, s>>>(nnz, keep, pos, kA, ci_raw, run_sum, ci, val, key);
+        launched("compact_kernel");
+    }
+    if (nk > 0) {
+        histogram_kernel<<<blocks(nk), 256, 0, s>>>(nk, key, cnt);
+        launched("histogram_kernel");
+    }
+    int32_t* rp = dmalloc<int32_t>(m + 1);
+    scan_exclusive_i32(cnt, rp, m + 1, s);
+    check_cuda(cudaStreamSynchronize(s), "coo sync");
+    for (void* p : {(void*)kA, (void*)kB, (void*)vA, (void*)vB, (void*)val_raw, (void*)run_sum, (void*)kept_d,
+                    (void*)pos, (void*)key, (void*)cnt})
+        dfree(p);
+    *rp_out = rp;
+    *ci_out = ci;
+    *val_out = val;
+    *nnz_out = nk;
+}
+
 }  // namespace
 
 void make_tile_table(const int32_t* rp, int64_t m, int64_t nnz, int64_t* ntiles, int32_t** trow, int32_t** tnz,
@@ -540,6 +620,60 @@ int hn_csr_create(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, 
             check_cuda(cudaStreamSynchronize(s), "hn_csr_create sync");
             if (!(flags & HN_CSR_NO_AUTOTUNE)) autotune(A, s);
         } catch (...) {
+            free_csr(A);
+            throw;
+        }
+        *out = A;
+    });
+}
+
+int hn_csr_create_coo(int64_t m, int64_t n, int64_t count, const int64_t* rows, const int64_t* cols,
+                      const double* val, unsigned flags, hn_csr** out) {
+    return guard("hn_csr_create_coo", [&] {
+        require_init();
+        if (!out) fail(HN_ERR_INVALID_ARG, "null output handle");
+        *out = nullptr;
+        if (m < 0 || n < 0 || count < 0) fail(HN_ERR_INVALID_ARG, "negative dimension or count");
+        if (m >= INT32_MAX || n >= INT32_MAX || count >= INT32_MAX || m + count >= INT32_MAX)
+            fail(HN_ERR_UNSUPPORTED, "dimension or count exceeds int32 range");
+        if (count > 0 && (!rows || !cols || !val)) fail(HN_ERR_INVALID_ARG, "null triplet arrays");
+        std::vector<int32_t> r32(static_cast<size_t>(count)), c32(static_cast<size_t>(count));
+        for (int64_t k = 0; k < count; ++k) {
+            if (rows[k] < 0 || rows[k] >= m || cols[k] < 0 || cols[k] >= n)
+                fail(HN_ERR_INVALID_ARG, "triplet " + std::to_string(k) + " (" + std::to_string(rows[k]) + ", " +
+                                             std::to_string(cols[k]) + ") outside " + std::to_string(m) + " x " +
+                                             std::to_string(n));
+            r32[k] = static_cast<int32_t>(rows[k]);
+            c32[k] = static_cast<int32_t>(cols[k]);
+        }
+        cudaStream_t s = nullptr;
+        int32_t* dr = dmalloc<int32_t>(count);
+        int32_t* dc = dmalloc<int32_t>(count);
+        double* dv = dmalloc<double>(count);
+        hn_csr* A = new hn_csr();
+        try {
+            if (count > 0) {
+                check_cuda(cudaMemcpy(dr, r32.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice), "H2D rows");
+                check_cuda(cudaMemcpy(dc, c32.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice), "H2D cols");
+                check_cuda(cudaMemcpy(dv, val, sizeof(double) * count, cudaMemcpyHostToDevice), "H2D values");
+            }
+            A->m = m;
+            A->n = n;
+            coo_to_csr(m, n, count, dr, dc, dv, &A->rp, &A->ci, &A->val, &A->nnz, s);
+            dfree(dr);
+            dfree(dc);
+            dfree(dv);
+            dr = dc = nullptr;
+            dv = nullptr;
+            build_tiles(A->rp, m, A->nnz, A->ntiles, A->tile_row, A->tile_nz, A->carry_row, A->carry_val,
+                        A->head_row, A->head_val, s);
+            if (!(flags & HN_CSR_NO_TRANSPOSE)) build_transpose(A, s);
+            check_cuda(cudaStreamSynchronize(s), "hn_csr_create_coo sync");
+            if (!(flags & HN_CSR_NO_AUTOTUNE)) autotune(A, s);
+        } catch (...) {
+            dfree(dr);
+            dfree(dc);
+            dfree(dv);
             free_csr(A);
             throw;
         }

@@ -65,6 +65,7 @@ SIGNATURES = {
     "hn_csr_destroy": [_vp],
     "hn_csr_shape": [_vp, _i64p, _i64p, _i64p, _i64p],
     "hn_csr_export": [_vp, C.c_int, _u64p, _u64p, _f64p],
+    "hn_csr_create_coo": [_i64, _i64, _i64, _i64p, _i64p, _f64p, C.c_uint, C.POINTER(_vp)],
     "hn_csr_tiles": [_vp, C.c_int, _i64p, _i64p],
     "hn_csr_export_tiles": [_vp, C.c_int, _i32p, _i32p],
     "hn_spmv": [_vp, C.c_int, C.c_double, _vp, C.c_double, _vp, _vp],
@@ -202,6 +203,26 @@ class Csr:
         m_, n_, nnz, nnzt = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
         check(load().hn_csr_shape(h, C.byref(m_), C.byref(n_), C.byref(nnz), C.byref(nnzt)))
         self.nnz, self.nnz_t = nnz.value, nnzt.value
+
+    @classmethod
+    def from_coo(cls, m: int, n: int, rows, cols, vals, transpose: bool = True, autotune: bool = True) -> "Csr":
+        """A from triplets in any order (duplicates summed in input order,
+        exact-zero sums dropped), sorted into CSR on the device
+        (hn_csr_create_coo)."""
+        self = cls.__new__(cls)
+        self.m, self.n = int(m), int(n)
+        r, c, v = (np.ascontiguousarray(rows, dtype=np.int64), np.ascontiguousarray(cols, dtype=np.int64),
+                   f64(vals))
+        h = C.c_void_p()
+        flags = (0 if transpose else HN_CSR_NO_TRANSPOSE) | (0 if autotune else HN_CSR_NO_AUTOTUNE)
+        check(load().hn_csr_create_coo(self.m, self.n, r.shape[0], _p(r, C.c_int64), _p(c, C.c_int64),
+                                       _p(v, C.c_double), flags, C.byref(h)))
+        self.h = h
+        m_, n_, nnz, nnzt = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        check(load().hn_csr_shape(h, C.byref(m_), C.byref(n_), C.byref(nnz), C.byref(nnzt)))
+        self.nnz, self.nnz_t = nnz.value, nnzt.value
+        self._rp = self._ci = self._val = None
+        return self
 
     def spmv_kind(self, trans: int = 0):
         """(kind, t): 0 merge path, 1 binned vector kernel with t nonzeros per lane."""
@@ -394,6 +415,14 @@ HOST_SIGNATURES = {
                                     C.POINTER(C.c_int), _f64p, _f64p, C.POINTER(C.c_int), _f64p,
                                     C.POINTER(IpmOptions), C.POINTER(C.c_int), _f64p, _i64p, _f64p, _vp,
                                     C.POINTER(C.c_int), _f64p, _f64p]),
+    "hn_mps_read_file": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),
+    "hn_mps_read_string": (C.c_int, [C.c_char_p, _i64, C.c_int, C.POINTER(_vp)]),
+    "hn_mps_shape": (C.c_int, [_vp, _i64p, _i64p, _i64p, C.POINTER(C.c_int)]),
+    "hn_mps_arrays": (C.c_int, [_vp, _i64p, _i64p, _f64p, _f64p, _f64p, _i32p, _f64p, _f64p, _f64p, _f64p, _i32p]),
+    "hn_mps_counts": (C.c_int, [_vp, _i64p, _i64p, _i64p]),
+    "hn_mps_warning": (C.c_char_p, [_vp, _i64]),
+    "hn_mps_name": (C.c_char_p, [_vp, C.c_int, _i64]),
+    "hn_mps_free": (C.c_int, [_vp]),
     "hn_be_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
     "hn_be_destroy": (C.c_int, [_vp]),
     "hn_be_spmv": (C.c_int, [_vp, _i64, _i64, _u64p, _u64p, _f64p, _i64, _f64p, _f64p]),
@@ -439,6 +468,62 @@ def _warm_arrays(opt, x0, y0, s0):
             keep.append(a)
             setattr(opt, name, _p(a, C.c_double))
     return keep
+
+
+def mps_read(text: bytes | str | None = None, path: str | None = None, fmt: int = -1) -> dict:
+    """The MPS reader (hn_mps_*, host): rows, columns, objective sense and the
+    constraint coefficients as triplets in file order. fmt -1 detects the
+    layout as the reference's MPSParser does, 0 free, 1 fixed."""
+    h = C.c_void_p()
+    if path is not None:
+        host_check(host().hn_mps_read_file(os.fsencode(path), fmt, C.byref(h)))
+    else:
+        data = text.encode() if isinstance(text, str) else bytes(text)
+        host_check(host().hn_mps_read_string(data, len(data), fmt, C.byref(h)))
+    try:
+        m, n, nt, mx = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int()
+        host_check(host().hn_mps_shape(h, C.byref(m), C.byref(n), C.byref(nt), C.byref(mx)))
+        m, n, nt = m.value, n.value, nt.value
+        o = {"m": m, "n": n, "maximize": mx.value,
+             "trow": np.zeros(max(nt, 1), dtype=np.int64), "tcol": np.zeros(max(nt, 1), dtype=np.int64),
+             "tval": np.zeros(max(nt, 1)), "c": np.zeros(max(n, 1)), "rhs": np.zeros(max(m, 1)),
+             "sense": np.zeros(max(m, 1), dtype=np.int32), "lb": np.zeros(max(n, 1)), "ub": np.zeros(max(n, 1)),
+             "range_lo": np.zeros(max(m, 1)), "range_hi": np.zeros(max(m, 1)),
+             "vtype": np.zeros(max(n, 1), dtype=np.int32)}
+        host_check(host().hn_mps_arrays(h, _p(o["trow"], C.c_int64), _p(o["tcol"], C.c_int64),
+                                        _p(o["tval"], C.c_double), _p(o["c"], C.c_double),
+                                        _p(o["rhs"], C.c_double), _p(o["sense"], C.c_int32),
+                                        _p(o["lb"], C.c_double), _p(o["ub"], C.c_double),
+                                        _p(o["range_lo"], C.c_double), _p(o["range_hi"], C.c_double),
+                                        _p(o["vtype"], C.c_int32)))
+        for k, size in (("trow", nt), ("tcol", nt), ("tval", nt), ("c", n), ("lb", n), ("ub", n), ("vtype", n),
+                        ("rhs", m), ("sense", m), ("range_lo", m), ("range_hi", m)):
+            o[k] = o[k][:size]
+        nw, nsos, nq = C.c_int64(), C.c_int64(), C.c_int64()
+        host_check(host().hn_mps_counts(h, C.byref(nw), C.byref(nsos), C.byref(nq)))
+        o["warnings"] = [host().hn_mps_warning(h, i).decode() for i in range(nw.value)]
+        o["sos_records"], o["quadratic_records"] = nsos.value, nq.value
+        o["name"] = host().hn_mps_name(h, -1, 0).decode()
+        o["row_names"] = [host().hn_mps_name(h, 0, i).decode() for i in range(m)]
+        o["col_names"] = [host().hn_mps_name(h, 1, j).decode() for j in range(n)]
+        return o
+    finally:
+        host().hn_mps_free(h)
+
+
+def read_mps(path: str | None = None, text: bytes | str | None = None, fmt: int = -1) -> dict:
+    """An MPS file as the LP dict lp_solve / lp_solve_batch take: the reader's
+    triplets go to the device (hn_csr_create_coo) and come back as the CSR the
+    reference's from_triplets builds; rhs -> b, sense, bounds, maximize."""
+    r = mps_read(text=text, path=path, fmt=fmt)
+    A = Csr.from_coo(r["m"], r["n"], r["trow"], r["tcol"], r["tval"], transpose=False, autotune=False)
+    try:
+        rp, ci, val = A.export()
+    finally:
+        A.close()
+    return {"m": r["m"], "n": r["n"], "rp": rp, "ci": ci, "val": val, "b": r["rhs"], "c": r["c"],
+            "sense": r["sense"], "lb": r["lb"], "ub": r["ub"], "maximize": bool(r["maximize"]),
+            "vtype": r["vtype"], "range_lo": r["range_lo"], "range_hi": r["range_hi"], "name": r["name"]}
 
 
 def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=0.0, max_iter=100,

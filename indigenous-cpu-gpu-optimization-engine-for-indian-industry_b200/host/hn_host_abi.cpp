@@ -6,6 +6,7 @@
 #include "hn_backend.hpp"
 #include "hn_host.h"
 #include "hn_lp.hpp"
+#include "hn_mps.hpp"
 #include "hn_sm100.h"
 
 namespace {
@@ -55,6 +56,13 @@ void hn_ipm_default_options(hn_ipm_options* o) {
 }
 
 const char* hn_host_last_error(void) { return g_err.c_str(); }
+}  // extern "C"
+
+namespace hn {
+void set_host_error(const std::string& msg) { g_err = msg; }
+}  // namespace hn
+
+extern "C" {
 
 int hn_lp_solve(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, const double* val, const double* c,
                 const double* b, const int* sense, const double* lb, const double* ub, int maximize,

@@ -25,6 +25,7 @@ _u64p = C.POINTER(C.c_uint64)
 _f64p = C.POINTER(C.c_double)
 _i32p = C.POINTER(C.c_int32)
 _u8p = C.POINTER(C.c_uint8)
+_vp = C.c_void_p
 
 _port = None
 _ref = None
@@ -95,6 +96,13 @@ def ref():
             "hnref_tmultiply": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p]),
             "hnref_transposed": (_i64, [_i64, _i64, _u64p, _u64p, _f64p, _u64p, _u64p, _f64p]),
             "hnref_from_triplets": (_i64, [_i64, _i64, _i64, _u64p, _u64p, _f64p, _u64p, _u64p, _f64p]),
+            "hnref_mps_parse": (_vp, [C.c_char_p, _i64, C.c_int]),
+            "hnref_mps_shape": (C.c_int, [_vp, _i64p, _i64p, _i64p, _i32p, _i32p, _i64p]),
+            "hnref_mps_arrays": (C.c_int, [_vp, _u64p, _u64p, _f64p, _f64p, _f64p, _i32p, _f64p, _f64p, _f64p,
+                                           _f64p, _i32p]),
+            "hnref_mps_name": (C.c_char_p, [_vp, C.c_int, _i64]),
+            "hnref_mps_free": (None, [_vp]),
+            "hnref_mps_parse_ms": (C.c_double, [C.c_char_p, _i64]),
             "hnref_cholesky_solve": (C.c_int, [_i64, _u64p, _u64p, _f64p, _f64p]),
             "hnref_ipm_solve": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, _i32p, _f64p,
                                           _f64p, C.c_int, C.c_int, C.c_int, _f64p, _i64p, _f64p, _f64p]),
@@ -281,6 +289,70 @@ def ref_from_triplets(rows, cols, ti, tj, tv):
     w = ref().hnref_from_triplets(rows, cols, ti.shape[0], _p(ti, C.c_uint64), _p(tj, C.c_uint64),
                                   _p(tv, C.c_double), _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double))
     return rp, ci[:w], val[:w]
+
+
+def from_triplets_port(rows: int, cols: int, ti, tj, tv):
+    """Restatement of SparseMatrix::from_triplets (sparse_matrix.cpp:8-53) and
+    sum_duplicates (:230-262): entries ordered by (row, column) -- equal keys
+    in input order (the reference's std::sort leaves their order
+    unspecified) -- each run of equal keys summed left to right from its
+    first value, exact-zero sums dropped. Returns (rp, ci, val)."""
+    ti = np.asarray(ti, dtype=np.int64)
+    tj = np.asarray(tj, dtype=np.int64)
+    tv = np.asarray(tv, dtype=np.float64)
+    order = np.lexsort((tj, ti))  # stable: primary row, secondary column
+    rp = np.zeros(rows + 1, dtype=np.uint64)
+    ci, val = [], []
+    k = 0
+    while k < order.shape[0]:
+        p = order[k]
+        s = tv[p]
+        q = k + 1
+        while q < order.shape[0] and ti[order[q]] == ti[p] and tj[order[q]] == tj[p]:
+            s = s + tv[order[q]]
+            q += 1
+        if s != 0.0:
+            ci.append(tj[p])
+            val.append(s)
+            rp[ti[p] + 1] += 1
+        k = q
+    rp = np.cumsum(rp).astype(np.uint64)
+    return rp, np.array(ci, dtype=np.uint64), np.array(val, dtype=np.float64)
+
+
+def ref_mps(text: bytes, fmt: int = -1) -> dict:
+    """model::MPSParser::parse_string on `text` (fmt -1: the parser's own
+    layout detection, 0 free, 1 fixed): the parsed problem's arrays, the
+    constraint matrix as the reference's CSR, and the row/column names."""
+    h = ref().hnref_mps_parse(text, len(text), fmt)
+    try:
+        m, n, nnz, mx, ok, nw = (C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32(), C.c_int32(), C.c_int64())
+        ref().hnref_mps_shape(h, C.byref(m), C.byref(n), C.byref(nnz), C.byref(mx), C.byref(ok), C.byref(nw))
+        m, n, nnz = m.value, n.value, nnz.value
+        out = {"m": m, "n": n, "maximize": mx.value, "success": ok.value, "warnings": nw.value,
+               "rp": np.zeros(m + 1, dtype=np.uint64), "ci": np.zeros(max(nnz, 1), dtype=np.uint64),
+               "val": np.zeros(max(nnz, 1)), "c": np.zeros(max(n, 1)), "rhs": np.zeros(max(m, 1)),
+               "sense": np.zeros(max(m, 1), dtype=np.int32), "lb": np.zeros(max(n, 1)), "ub": np.zeros(max(n, 1)),
+               "range_lo": np.zeros(max(m, 1)), "range_hi": np.zeros(max(m, 1)),
+               "vtype": np.zeros(max(n, 1), dtype=np.int32)}
+        ref().hnref_mps_arrays(h, *(_p(out[k], C.c_uint64) for k in ("rp", "ci")), _p(out["val"], C.c_double),
+                               _p(out["c"], C.c_double), _p(out["rhs"], C.c_double), _p(out["sense"], C.c_int32),
+                               _p(out["lb"], C.c_double), _p(out["ub"], C.c_double),
+                               _p(out["range_lo"], C.c_double), _p(out["range_hi"], C.c_double),
+                               _p(out["vtype"], C.c_int32))
+        for k, size in (("ci", nnz), ("val", nnz), ("c", n), ("lb", n), ("ub", n), ("vtype", n), ("rhs", m),
+                        ("sense", m), ("range_lo", m), ("range_hi", m)):
+            out[k] = out[k][:size]
+        out["name"] = ref().hnref_mps_name(h, -1, 0).decode()
+        out["row_names"] = [ref().hnref_mps_name(h, 0, i).decode() for i in range(m)]
+        out["col_names"] = [ref().hnref_mps_name(h, 1, j).decode() for j in range(n)]
+        return out
+    finally:
+        ref().hnref_mps_free(h)
+
+
+def ref_mps_parse_ms(text: bytes) -> float:
+    return ref().hnref_mps_parse_ms(text, len(text))
 
 
 def ref_backend_spmm(rp, ci, val, B, k, n):
