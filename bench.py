@@ -628,7 +628,7 @@ def _mps_text(lp: dict, name: str) -> bytes:
     out = [f"NAME {name}", "ROWS", " N obj"] + [f" E r{i}" for i in range(m)] + ["COLUMNS"]
     starts = np.searchsorted(cols, np.arange(n + 1))
     for j in range(n):
-        out.append(f"    v{j} obj {lp['c'][j]!r}")
+        out.append(f"    v{j} obj {float(lp['c'][j])!r}")
         out.extend(f"    v{j} r{i} {a!r}" for i, a in zip(rows[starts[j]:starts[j + 1]].tolist(),
                                                         vals[starts[j]:starts[j + 1]].tolist()))
     out.append("RHS")

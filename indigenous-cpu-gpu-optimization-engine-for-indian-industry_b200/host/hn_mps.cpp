@@ -14,6 +14,7 @@
 // and std::stod (strtod over a prefix; out_of_range/invalid_argument caught
 // where the reference catches them).
 #include <cerrno>
+#include <charconv>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -39,26 +40,50 @@ constexpr double kInf = std::numeric_limits<double>::infinity();
 enum class Section { NONE, NAME, ROWS, COLUMNS, RHS, RANGES, BOUNDS, SOS, QUADOBJ, QCMATRIX, OBJSENSE, ENDATA };
 enum VarType : int32_t { CONTINUOUS = 0, INTEGER = 1, BINARY = 2, SEMI_CONTINUOUS = 3, SEMI_INTEGER = 4 };
 
+using sv = std::string_view;
+
 inline bool is_ws(char ch) {  // isspace in the C locale
     return ch == ' ' || ch == '\t' || ch == '\n' || ch == '\v' || ch == '\f' || ch == '\r';
 }
+inline char up(char ch) { return ch >= 'a' && ch <= 'z' ? static_cast<char>(ch - 'a' + 'A') : ch; }
 
-std::string upper(std::string_view s) {
-    std::string u(s);
-    for (char& ch : u)
-        if (ch >= 'a' && ch <= 'z') ch = static_cast<char>(ch - 'a' + 'A');
-    return u;
+// a == kw after upper-casing a (kw is upper case)
+bool ieq(sv a, sv kw) {
+    if (a.size() != kw.size()) return false;
+    for (size_t i = 0; i < a.size(); ++i)
+        if (up(a[i]) != kw[i]) return false;
+    return true;
+}
+
+// strtod over a copy of s (NUL-terminated); `end` = characters used
+double strtod_sv(sv s, size_t* used, bool* erange) {
+    char buf[96];
+    std::string big;
+    const char* b = buf;
+    if (s.size() < sizeof(buf)) {
+        if (!s.empty()) std::memcpy(buf, s.data(), s.size());
+        buf[s.size()] = '\0';
+    } else {
+        big.assign(s);
+        b = big.c_str();
+    }
+    char* end = nullptr;
+    errno = 0;
+    const double v = std::strtod(b, &end);
+    if (erange) *erange = errno == ERANGE;
+    *used = static_cast<size_t>(end - b);
+    return v;
 }
 
 // A cursor over one line with the extraction rules of std::istringstream:
 // strings are whitespace-delimited tokens; a double reads the longest prefix
 // of libstdc++'s float grammar (sign, digits with one point, exponent after a
-// digit) and converts it with strtod, failing unless strtod used all of it or
-// when the value overflows. Any failure sticks (later extractions fail).
+// digit) and converts all of it (failing otherwise) with correct rounding,
+// failing on overflow. Any failure sticks (later extractions fail).
 class Tokens {
 public:
-    explicit Tokens(std::string_view s) : s_(s) {}
-    bool str(std::string& out) {
+    explicit Tokens(sv s) : s_(s) {}
+    bool str(sv& out) {
         if (fail_) return false;
         skip();
         if (p_ >= s_.size()) {
@@ -67,30 +92,26 @@ public:
         }
         const size_t b = p_;
         while (p_ < s_.size() && !is_ws(s_[p_])) ++p_;
-        out.assign(s_.substr(b, p_ - b));
+        out = s_.substr(b, p_ - b);
         return true;
     }
     bool num(double& out) {
         if (fail_) return false;
         skip();
-        std::string acc;
+        const size_t b = p_;
         size_t q = p_;
-        bool mant = false, point = false, sci = false;
-        if (q < s_.size() && (s_[q] == '+' || s_[q] == '-')) acc += s_[q++];
+        bool mant = false, point = false;
+        if (q < s_.size() && (s_[q] == '+' || s_[q] == '-')) ++q;
         while (q < s_.size()) {
             const char ch = s_[q];
             if (ch >= '0' && ch <= '9') {
-                acc += ch;
                 mant = true;
-            } else if (ch == '.' && !point && !sci) {
-                acc += ch;
+            } else if (ch == '.' && !point) {
                 point = true;
-            } else if ((ch == 'e' || ch == 'E') && mant && !sci) {
-                acc += ch;
-                sci = true;
+            } else if ((ch == 'e' || ch == 'E') && mant) {
                 ++q;
-                if (q < s_.size() && (s_[q] == '+' || s_[q] == '-')) acc += s_[q++];
-                while (q < s_.size() && s_[q] >= '0' && s_[q] <= '9') acc += s_[q++];
+                if (q < s_.size() && (s_[q] == '+' || s_[q] == '-')) ++q;
+                while (q < s_.size() && s_[q] >= '0' && s_[q] <= '9') ++q;
                 break;
             } else {
                 break;
@@ -99,101 +120,116 @@ public:
         }
         p_ = q;
         out = 0.0;
-        if (acc.empty()) {
-            fail_ = true;
-            return false;
+        sv acc = s_.substr(b, q - b);
+        if (acc.empty()) return fail();
+        // from_chars takes no '+'; its result is strtod's (both round correctly)
+        sv digits = acc[0] == '+' ? acc.substr(1) : acc;
+        double v = 0.0;
+        const auto r = std::from_chars(digits.data(), digits.data() + digits.size(), v);
+        if (r.ec == std::errc() && r.ptr == digits.data() + digits.size()) {
+            out = v;
+            return true;
         }
-        char* end = nullptr;
-        const double v = std::strtod(acc.c_str(), &end);
-        if (end != acc.c_str() + acc.size()) {
-            fail_ = true;
-            return false;
-        }
+        // the rare cases (range errors, malformed text): strtod's own answer
+        size_t used = 0;
+        v = strtod_sv(acc, &used, nullptr);
+        if (used != acc.size()) return fail();
         if (std::isinf(v)) {
             out = v > 0 ? std::numeric_limits<double>::max() : -std::numeric_limits<double>::max();
-            fail_ = true;
-            return false;
+            return fail();
         }
         out = v;
         return true;
     }
 
 private:
+    bool fail() {
+        fail_ = true;
+        return false;
+    }
     void skip() {
         while (p_ < s_.size() && is_ws(s_[p_])) ++p_;
     }
-    std::string_view s_;
+    sv s_;
     size_t p_ = 0;
     bool fail_ = false;
 };
 
-std::vector<std::string> split(std::string_view s) {
-    std::vector<std::string> out;
+template <size_t N>
+size_t split(sv s, sv (&out)[N]) {  // up to N tokens; returns the total count
     Tokens t(s);
-    std::string w;
-    while (t.str(w)) out.push_back(w);
-    return out;
+    sv w;
+    size_t k = 0;
+    while (t.str(w)) {
+        if (k < N) out[k] = w;
+        ++k;
+    }
+    return k;
 }
 
 // std::stod: strtod over a prefix; throws (here: nullopt) on no conversion or
 // ERANGE; `used` gets the characters consumed
-std::optional<double> stod_like(const std::string& s, size_t* used) {
-    const char* b = s.c_str();
-    char* end = nullptr;
-    errno = 0;
-    const double v = std::strtod(b, &end);
-    if (end == b || errno == ERANGE) return std::nullopt;
-    if (used) *used = static_cast<size_t>(end - b);
+std::optional<double> stod_like(sv s, size_t* used) {
+    size_t u = 0;
+    bool erange = false;
+    const double v = strtod_sv(s, &u, &erange);
+    if (u == 0 || erange) return std::nullopt;
+    if (used) *used = u;
     return v;
 }
 
-bool is_numeric(const std::string& s) {
+bool is_numeric(sv s) {
     if (s.empty()) return false;
     size_t used = 0;
     const auto v = stod_like(s, &used);
     return v && used == s.size();
 }
 
-std::string trim_ends(std::string_view s, const char* set) {
+sv trim_ends(sv s, const char* set) {
     const size_t b = s.find_first_not_of(set);
-    if (b == std::string_view::npos) return "";
+    if (b == sv::npos) return sv();
     const size_t e = s.find_last_not_of(set);
-    return std::string(s.substr(b, e - b + 1));
+    return s.substr(b, e - b + 1);
 }
 
-using Record = std::tuple<std::string, std::string, double, std::string, double>;
+struct Record {
+    sv a, b;
+    double v1;
+    sv c;
+    double v2;
+};
 
-Section detect_section(std::string_view line) {
+Section detect_section(sv line) {
     Tokens t(line);
-    std::string first, second;
+    sv first, second;
     t.str(first);
     const bool single = !t.str(second);
-    const std::string u = upper(first);
-    if (u == "NAME") return Section::NAME;
-    if (u == "OBJSENSE") return Section::OBJSENSE;
+    if (first.size() < 3 || first.size() > 8) return Section::NONE;
+    if (ieq(first, "NAME")) return Section::NAME;
+    if (ieq(first, "OBJSENSE")) return Section::OBJSENSE;
     if (!single) return Section::NONE;
-    if (u == "ROWS") return Section::ROWS;
-    if (u == "COLUMNS") return Section::COLUMNS;
-    if (u == "RHS") return Section::RHS;
-    if (u == "RANGES") return Section::RANGES;
-    if (u == "BOUNDS") return Section::BOUNDS;
-    if (u == "SOS") return Section::SOS;
-    if (u == "QUADOBJ") return Section::QUADOBJ;
-    if (u == "QCMATRIX") return Section::QCMATRIX;
-    if (u == "ENDATA") return Section::ENDATA;
+    if (ieq(first, "ROWS")) return Section::ROWS;
+    if (ieq(first, "COLUMNS")) return Section::COLUMNS;
+    if (ieq(first, "RHS")) return Section::RHS;
+    if (ieq(first, "RANGES")) return Section::RANGES;
+    if (ieq(first, "BOUNDS")) return Section::BOUNDS;
+    if (ieq(first, "SOS")) return Section::SOS;
+    if (ieq(first, "QUADOBJ")) return Section::QUADOBJ;
+    if (ieq(first, "QCMATRIX")) return Section::QCMATRIX;
+    if (ieq(first, "ENDATA")) return Section::ENDATA;
     return Section::NONE;
 }
 
 // the reference's layout probe (mps_parser.cpp:124-158): over the first 8
 // COLUMNS data lines, the position of the second non-blank character; fixed
 // layout when at least 3 were sampled and half of them sit at index 14
-bool detect_free(const std::vector<std::string_view>& lines) {
+bool detect_free(const std::vector<sv>& lines) {
     bool in_columns = false;
     int samples = 0, aligned = 0;
-    for (std::string_view line : lines) {
+    for (sv line : lines) {
         const size_t lead = line.find_first_not_of(" \t\r\n");
-        if (lead == std::string_view::npos) continue;
-        std::string_view trimmed = line.substr(lead);
+        if (lead == sv::npos) continue;
+        sv trimmed = line.substr(lead);
         if (trimmed[0] == '*') continue;
         const Section sec = detect_section(trimmed);
         if (sec != Section::NONE) {
@@ -202,9 +238,9 @@ bool detect_free(const std::vector<std::string_view>& lines) {
         }
         if (!in_columns) continue;
         const size_t a = line.find_first_not_of(" \t");
-        if (a == std::string_view::npos) continue;
+        if (a == sv::npos) continue;
         const size_t b = line.find_first_not_of(" \t", a + 1);
-        if (b == std::string_view::npos) continue;
+        if (b == sv::npos) continue;
         ++samples;
         if (b == 14) ++aligned;
         if (samples >= 8) break;
@@ -212,23 +248,81 @@ bool detect_free(const std::vector<std::string_view>& lines) {
     return !(samples >= 3 && aligned * 2 >= samples);
 }
 
+// Names -> first index: open addressing over (hash, index) slots, the names
+// themselves kept by the caller's vector; a slot is compared by hash first.
+class NameIndex {
+public:
+    explicit NameIndex(const std::vector<std::string>& names) : names_(names) { slots_.assign(64, Slot{0, -1}); }
+    int64_t find(sv name) const {
+        const uint64_t h = hash(name);
+        for (size_t i = h & (slots_.size() - 1);; i = (i + 1) & (slots_.size() - 1)) {
+            const Slot& s = slots_[i];
+            if (s.idx < 0) return -1;
+            if (s.h == h && names_[static_cast<size_t>(s.idx)] == name) return s.idx;
+        }
+    }
+    // records names_[idx] unless the name is already present (first wins)
+    void add(int64_t idx) {
+        if (4 * (count_ + 1) > 3 * slots_.size()) grow();
+        const sv name = names_[static_cast<size_t>(idx)];
+        const uint64_t h = hash(name);
+        for (size_t i = h & (slots_.size() - 1);; i = (i + 1) & (slots_.size() - 1)) {
+            Slot& s = slots_[i];
+            if (s.idx < 0) {
+                s = Slot{h, idx};
+                ++count_;
+                return;
+            }
+            if (s.h == h && names_[static_cast<size_t>(s.idx)] == name) return;
+        }
+    }
+
+private:
+    struct Slot {
+        uint64_t h;
+        int64_t idx;
+    };
+    static uint64_t hash(sv s) {  // FNV-1a, then a 64-bit finaliser
+        uint64_t h = 1469598103934665603ull;
+        for (const char ch : s) h = (h ^ static_cast<unsigned char>(ch)) * 1099511628211ull;
+        h ^= h >> 33;
+        h *= 0xff51afd7ed558ccdull;
+        h ^= h >> 33;
+        return h;
+    }
+    void grow() {
+        std::vector<Slot> old;
+        old.swap(slots_);
+        slots_.assign(old.size() * 2, Slot{0, -1});
+        for (const Slot& o : old) {
+            if (o.idx < 0) continue;
+            size_t i = o.h & (slots_.size() - 1);
+            while (slots_[i].idx >= 0) i = (i + 1) & (slots_.size() - 1);
+            slots_[i] = o;
+        }
+    }
+    const std::vector<std::string>& names_;
+    std::vector<Slot> slots_;
+    size_t count_ = 0;
+};
+
 class Reader {
 public:
-    explicit Reader(MpsProblem& out) : P(out) {}
+    explicit Reader(MpsProblem& out) : P(out), row_of_(out.row_names), col_of_(out.col_names) {}
 
-    void run(std::string_view text, int format) {
-        std::vector<std::string_view> lines;
+    void run(sv text, int format) {
+        std::vector<sv> lines;
         size_t b = 0;
         while (b < text.size()) {  // std::getline on '\n'
             size_t e = text.find('\n', b);
-            if (e == std::string_view::npos) e = text.size();
+            if (e == sv::npos) e = text.size();
             lines.push_back(text.substr(b, e - b));
             b = e + 1;
         }
         free_ = format < 0 ? detect_free(lines) : format == 0;
         Section cur = Section::NONE;
-        for (std::string_view line : lines) {
-            const std::string trimmed = trim_ends(line, " \t\r\n");
+        for (sv line : lines) {
+            const sv trimmed = trim_ends(line, " \t\r\n");
             if (trimmed.empty() || trimmed[0] == '*') continue;
             const Section sec = detect_section(trimmed);
             if (sec != Section::NONE) {
@@ -237,7 +331,7 @@ public:
                     name_line(trimmed);
                 } else if (sec == Section::OBJSENSE) {
                     Tokens t(trimmed);
-                    std::string s;
+                    sv s;
                     t.str(s);
                     t.str(s);
                     objsense(s);
@@ -256,7 +350,7 @@ public:
                 case Section::QCMATRIX: ++P.quadratic_records; break;
                 case Section::OBJSENSE: {
                     Tokens t(trimmed);
-                    std::string s;
+                    sv s;
                     t.str(s);
                     objsense(s);
                     break;
@@ -274,46 +368,46 @@ private:
     bool free_ = true;
     bool in_int_ = false;
     std::string obj_row_;
-    std::unordered_map<std::string, int64_t> row_of_, col_of_;
+    NameIndex row_of_, col_of_;
+    int64_t last_col_ = -1;  // COLUMNS lists a column's entries together
 
     void warn(std::string msg) { P.warnings.push_back(std::move(msg)); }
 
-    void objsense(const std::string& s) {
-        const std::string u = upper(s);
-        if (u == "MAX" || u == "MAXIMIZE") P.maximize = 1;
+    void objsense(sv s) {
+        if (ieq(s, "MAX") || ieq(s, "MAXIMIZE")) P.maximize = 1;
     }
 
-    void name_line(std::string_view line) {
+    void name_line(sv line) {
         Tokens t(line);
-        std::string s;
+        sv s;
         t.str(s);
-        if (t.str(s)) P.name = s;
+        if (t.str(s)) P.name.assign(s);
     }
 
-    std::optional<Record> record(std::string_view line) { return free_ ? free_record(line) : fixed_record(line); }
+    std::optional<Record> record(sv line) const { return free_ ? free_record(line) : fixed_record(line); }
 
-    static std::optional<Record> free_record(std::string_view line) {
+    static std::optional<Record> free_record(sv line) {
         Tokens t(line);
-        std::string a, b, c;
-        double v1 = 0.0, v2 = 0.0;
-        if (!t.str(a) || !t.str(b) || !t.num(v1)) return std::nullopt;
-        if (!t.str(c)) c.clear();
-        if (!t.num(v2)) v2 = 0.0;
-        return Record{a, b, v1, c, v2};
+        Record r{sv(), sv(), 0.0, sv(), 0.0};
+        if (!t.str(r.a) || !t.str(r.b) || !t.num(r.v1)) return std::nullopt;
+        if (!t.str(r.c)) r.c = sv();
+        if (!t.num(r.v2)) r.v2 = 0.0;
+        return r;
     }
 
-    static std::optional<Record> fixed_record(std::string_view line) {
+    static std::optional<Record> fixed_record(sv line) {
         // whole-token reading first (right-justified writers), then the fixed
         // column windows 5-12, 15-22, 25-36, 40-47, 50-61
-        const std::vector<std::string> tok = split(line);
-        if (tok.size() == 3 && !is_numeric(tok[0]) && !is_numeric(tok[1]) && is_numeric(tok[2]))
-            return Record{tok[0], tok[1], *stod_like(tok[2], nullptr), std::string(), 0.0};
-        if (tok.size() == 5 && !is_numeric(tok[0]) && !is_numeric(tok[1]) && is_numeric(tok[2]) &&
-            !is_numeric(tok[3]) && is_numeric(tok[4]))
+        sv tok[6];
+        const size_t nt = split(line, tok);
+        if (nt == 3 && !is_numeric(tok[0]) && !is_numeric(tok[1]) && is_numeric(tok[2]))
+            return Record{tok[0], tok[1], *stod_like(tok[2], nullptr), sv(), 0.0};
+        if (nt == 5 && !is_numeric(tok[0]) && !is_numeric(tok[1]) && is_numeric(tok[2]) && !is_numeric(tok[3]) &&
+            is_numeric(tok[4]))
             return Record{tok[0], tok[1], *stod_like(tok[2], nullptr), tok[3], *stod_like(tok[4], nullptr)};
-        auto field = [&](size_t off, size_t width) -> std::string {
-            if (off > line.size()) return "";
-            return std::string(line.substr(off, std::min(width, line.size() - off)));
+        auto field = [&](size_t off, size_t width) -> sv {
+            if (off > line.size()) return sv();
+            return line.substr(off, std::min(width, line.size() - off));
         };
         auto value = [&](size_t off) {
             const auto v = stod_like(trim_ends(field(off, 12), " \t"), nullptr);
@@ -323,13 +417,13 @@ private:
                       trim_ends(field(39, 8), " \t"), value(49)};
     }
 
-    void rows(std::string_view line) {
+    void rows(sv line) {
         Tokens t(line);
-        std::string kind, name;
+        sv kind, nm;
         t.str(kind);
-        t.str(name);
+        t.str(nm);
         if (kind == "N") {
-            obj_row_ = name;
+            obj_row_.assign(nm);
             return;
         }
         int32_t sense = 0;  // LE
@@ -340,72 +434,75 @@ private:
         else if (kind == "E")
             sense = 2;
         else
-            warn("Unknown row type: " + kind + " for row " + name);
+            warn("Unknown row type: " + std::string(kind) + " for row " + std::string(nm));
         const int64_t i = static_cast<int64_t>(P.sense.size());
-        if (name.empty()) name = "c" + std::to_string(i);
-        row_of_.emplace(name, i);  // first row of a name answers lookups
-        P.row_names.push_back(name);
+        P.row_names.push_back(nm.empty() ? "c" + std::to_string(i) : std::string(nm));
+        row_of_.add(i);  // the first row of a name answers lookups
         P.sense.push_back(sense);
         P.rhs.push_back(0.0);
         P.range_lo.push_back(-kInf);
         P.range_hi.push_back(kInf);
     }
 
-    int64_t row(const std::string& name) const {
-        const auto it = row_of_.find(name);
-        return it == row_of_.end() ? -1 : it->second;
-    }
+    int64_t row(sv name) const { return row_of_.find(name); }
 
-    static bool marker(std::string_view line, bool& in_int) {
-        std::vector<std::string> t = split(line);
-        for (std::string& w : t) {
-            if (w.size() >= 2 && w.front() == '\'') w.erase(0, 1);
-            if (!w.empty() && w.back() == '\'') w.pop_back();
-        }
-        if (t.size() < 2) return false;
+    static bool marker(sv line, bool& in_int) {
+        // a marker record has a token "MARKER" (quotes stripped, any case):
+        // no such substring, no marker
+        bool any = false;
+        for (size_t i = 0; i + 6 <= line.size() && !any; ++i)
+            any = up(line[i]) == 'M' && ieq(line.substr(i, 6), "MARKER");
+        if (!any) return false;
+        sv t[64];
+        const size_t nt = split(line, t);
+        if (nt < 2) return false;
         bool has = false;
-        std::string kind;
-        for (const std::string& w : t) {
-            const std::string u = upper(w);
-            if (u == "MARKER") {
+        int kind = 0;  // 1 INTORG, 2 INTEND
+        for (size_t i = 0; i < nt && i < 64; ++i) {
+            sv w = t[i];
+            if (w.size() >= 2 && w.front() == '\'') w.remove_prefix(1);
+            if (!w.empty() && w.back() == '\'') w.remove_suffix(1);
+            if (ieq(w, "MARKER")) {
                 has = true;
                 continue;
             }
-            if (u == "INTORG" || u == "INTEND") {
-                kind = u;
+            if (ieq(w, "INTORG")) {
+                kind = 1;
+                break;
+            }
+            if (ieq(w, "INTEND")) {
+                kind = 2;
                 break;
             }
         }
         if (!has) return false;
-        if (kind == "INTORG") in_int = true;
-        if (kind == "INTEND") in_int = false;
+        if (kind == 1) in_int = true;
+        if (kind == 2) in_int = false;
         return true;
     }
 
-    void columns(std::string_view line) {
+    void columns(sv line) {
         if (marker(line, in_int_)) return;
         const auto rec = record(line);
         if (!rec) return;
-        const auto& [col, r1, v1, r2, v2] = *rec;
-        if (col == "MARKER") return;
-        int64_t j;
-        const auto it = col_of_.find(col);
-        if (it == col_of_.end()) {
+        if (rec->a == "MARKER") return;
+        int64_t j = last_col_ >= 0 && P.col_names[static_cast<size_t>(last_col_)] == rec->a ? last_col_
+                                                                                            : col_of_.find(rec->a);
+        if (j < 0) {
             j = static_cast<int64_t>(P.c.size());
-            col_of_.emplace(col, j);
-            P.col_names.push_back(col);
+            P.col_names.emplace_back(rec->a);
+            col_of_.add(j);
             P.c.push_back(0.0);
             P.lb.push_back(0.0);
             P.ub.push_back(kInf);
             P.vtype.push_back(in_int_ ? INTEGER : CONTINUOUS);
-        } else {
-            j = it->second;
         }
-        coeff(j, r1, v1);
-        coeff(j, r2, v2);
+        last_col_ = j;
+        coeff(j, rec->b, rec->v1);
+        coeff(j, rec->c, rec->v2);
     }
 
-    void coeff(int64_t j, const std::string& r, double v) {
+    void coeff(int64_t j, sv r, double v) {
         if (r.empty() || v == 0.0) return;
         if (r == obj_row_) {
             P.c[j] = v;
@@ -419,15 +516,15 @@ private:
             return;
         }
         if (obj_row_.empty()) {  // no N row: the first unknown row is the objective
-            obj_row_ = r;
+            obj_row_.assign(r);
             P.c[j] = v;
-            warn("Implicit objective row '" + r + "' (no N row declared in ROWS)");
+            warn("Implicit objective row '" + std::string(r) + "' (no N row declared in ROWS)");
             return;
         }
-        warn("Unknown row '" + r + "' referenced in COLUMNS is ignored");
+        warn("Unknown row '" + std::string(r) + "' referenced in COLUMNS is ignored");
     }
 
-    bool set_rhs(const std::string& r, double v) {
+    bool set_rhs(sv r, double v) {
         const int64_t i = row(r);
         if (i < 0) return false;
         P.rhs[i] = v;
@@ -436,32 +533,31 @@ private:
 
     // the fixed-layout retry of an RHS line that free reading misplaced
     // (mps_parser.cpp:318-346); returns whether its first row matched
-    bool rhs_retry(std::string_view line) {
+    bool rhs_retry(sv line) {
         if (!(free_ && line.size() >= 50)) return false;
         const auto f = fixed_record(line);
         if (!f) return false;
-        const auto& [fn, f1, fv1, f2, fv2] = *f;
-        if (!f1.empty() && set_rhs(f1, fv1)) {
-            if (!f2.empty()) set_rhs(f2, fv2);
+        if (!f->b.empty() && set_rhs(f->b, f->v1)) {
+            if (!f->c.empty()) set_rhs(f->c, f->v2);
             return true;
         }
         return false;
     }
 
-    void rhs(std::string_view line) {
+    void rhs(sv line) {
         const auto rec = record(line);
         if (!rec) return;
-        const auto& [nm, r1, v1, r2, v2] = *rec;
-        const bool m1 = !r1.empty() && set_rhs(r1, v1);
+        const sv r1 = rec->b, r2 = rec->c;
+        const bool m1 = !r1.empty() && set_rhs(r1, rec->v1);
         if (!m1 && !r1.empty()) {
             if (rhs_retry(line)) return;
         } else if (r1.empty()) {
-            if (!r2.empty()) set_rhs(r2, v2);
+            if (!r2.empty()) set_rhs(r2, rec->v2);
         }
-        if (!r2.empty() && !set_rhs(r2, v2)) rhs_retry(line);
+        if (!r2.empty() && !set_rhs(r2, rec->v2)) rhs_retry(line);
     }
 
-    void range(const std::string& r, double v) {
+    void range(sv r, double v) {
         const int64_t i = row(r);
         if (i < 0) return;
         const double b = P.rhs[i];
@@ -477,26 +573,24 @@ private:
         }
     }
 
-    void ranges(std::string_view line) {
+    void ranges(sv line) {
         const auto rec = record(line);
         if (!rec) return;
-        const auto& [nm, r1, v1, r2, v2] = *rec;
-        if (!r1.empty()) range(r1, v1);
-        if (!r2.empty()) range(r2, v2);
+        if (!rec->b.empty()) range(rec->b, rec->v1);
+        if (!rec->c.empty()) range(rec->c, rec->v2);
     }
 
-    void bounds(std::string_view line) {
+    void bounds(sv line) {
         // type, bound-set name and column are always read as three tokens
         Tokens t(line);
-        std::string type, set, col;
+        sv type, set, col;
         double v = 0.0;
         t.str(type);
         t.str(set);
         t.str(col);
         if (type != "FR" && type != "MI" && type != "PL") t.num(v);
-        const auto it = col_of_.find(col);
-        if (it == col_of_.end()) return;
-        const int64_t j = it->second;
+        const int64_t j = col_of_.find(col);
+        if (j < 0) return;
         if (type == "LO") {
             P.lb[j] = v;
         } else if (type == "UP") {

@@ -34,7 +34,7 @@ def write_lp_small(path):
         for k in range(int(rp[i]), int(rp[i + 1])):
             cols[int(ci[k])].append((i, float(val[k])))
     for j in range(lp["n"]):
-        lines.append(f"    v{j} obj {lp['c'][j]!r}")
+        lines.append(f"    v{j} obj {float(lp['c'][j])!r}")
         for i, a in cols[j]:
             if rng.random() < 0.1:  # split the coefficient in two entries
                 h = float(np.float64(a) * 0.375)
@@ -45,7 +45,7 @@ def write_lp_small(path):
             i = int(rng.integers(lp["m"]))
             lines.append(f"    v{j} r{i} 0.25 r{i} -0.25")
     lines.append("RHS")
-    lines += [f"    rhs r{i} {lp['b'][i]!r}" for i in range(lp["m"])]
+    lines += [f"    rhs r{i} {float(lp['b'][i])!r}" for i in range(lp["m"])]
     lines += ["BOUNDS"] + [f" UP bnd v{j} {10.0 + j % 7}" for j in range(0, lp["n"], 5)] + ["ENDATA"]
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
