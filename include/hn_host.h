@@ -101,9 +101,19 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
  * name wins, as in the reference's linear searches). The constraint
  * coefficients come out as triplets in file order; hn_csr_create_coo makes
  * the device CSR the reference's from_triplets would make. */
-typedef struct hn_mps hn_mps;
+typedef struct hn_mps hn_mps; /* a problem read from MPS or LP text */
 int hn_mps_read_file(const char* path, int format, hn_mps** out);
 int hn_mps_read_string(const char* text, int64_t len, int format, hn_mps** out);
+/* ---- LP-format reader (LPParser, core/model/lp_parser.hpp:17-64) ----
+ * CPLEX-style LP text with the reference's results: MIN/MAX objective
+ * (bracketed quadratic groups read past; their variables still created in
+ * the reference's order), SUBJECT TO constraints over one or more lines
+ * (<=, >=, =), BOUNDS in its five whole-line forms, GENERAL(S), BINARY,
+ * SOS and QUADRATIC sections, END. Where the reference would report errors
+ * (and no problem) the call fails with HN_ERR_INVALID_ARG and the first
+ * error's text. The result is read with the hn_mps_* accessors below. */
+int hn_lp_read_file(const char* path, hn_mps** out);
+int hn_lp_read_string(const char* text, int64_t len, hn_mps** out);
 /* m rows (constraints), n columns, triplet count, objective sense (1 = MAX) */
 int hn_mps_shape(const hn_mps* h, int64_t* m, int64_t* n, int64_t* ntriplets, int* maximize);
 /* Copies out (each may be NULL): triplets (ntriplets), c / lb / ub / vtype

@@ -79,8 +79,8 @@ def build_host(verbose: bool = False) -> str | None:
         objs.append(obj)
         if _stale(obj, [src] + hdrs):
             contract = "-ffp-contract=fast" if os.path.basename(src) == "hn_ldlt.cpp" else "-ffp-contract=off"
-            # the MPS reader looks names up by string_view (C++20 heterogeneous lookup)
-            std = "-std=c++20" if os.path.basename(src) == "hn_mps.cpp" else "-std=c++17"
+            # the MPS and LP readers look names up by string_view (C++20 heterogeneous lookup)
+            std = "-std=c++20" if os.path.basename(src) == "hn_read.cpp" else "-std=c++17"
             cmd = [cxx, "-O3", std, "-fPIC", "-fopenmp", "-march=x86-64-v3", contract,
                    "-I", INCLUDE, "-I", HOST, "-c", src, "-o", obj]
             if verbose:

@@ -417,6 +417,8 @@ HOST_SIGNATURES = {
                                     C.POINTER(C.c_int), _f64p, _f64p]),
     "hn_mps_read_file": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),
     "hn_mps_read_string": (C.c_int, [C.c_char_p, _i64, C.c_int, C.POINTER(_vp)]),
+    "hn_lp_read_file": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
+    "hn_lp_read_string": (C.c_int, [C.c_char_p, _i64, C.POINTER(_vp)]),
     "hn_mps_shape": (C.c_int, [_vp, _i64p, _i64p, _i64p, C.POINTER(C.c_int)]),
     "hn_mps_arrays": (C.c_int, [_vp, _i64p, _i64p, _f64p, _f64p, _f64p, _i32p, _f64p, _f64p, _f64p, _f64p, _i32p]),
     "hn_mps_counts": (C.c_int, [_vp, _i64p, _i64p, _i64p]),
@@ -480,6 +482,22 @@ def mps_read(text: bytes | str | None = None, path: str | None = None, fmt: int 
     else:
         data = text.encode() if isinstance(text, str) else bytes(text)
         host_check(host().hn_mps_read_string(data, len(data), fmt, C.byref(h)))
+    return _read_result(h)
+
+
+def lp_read(text: bytes | str | None = None, path: str | None = None) -> dict:
+    """The LP-format reader (hn_lp_read_*, host), same result layout as
+    mps_read. Text the reference's LPParser would reject raises HnError."""
+    h = C.c_void_p()
+    if path is not None:
+        host_check(host().hn_lp_read_file(os.fsencode(path), C.byref(h)))
+    else:
+        data = text.encode() if isinstance(text, str) else bytes(text)
+        host_check(host().hn_lp_read_string(data, len(data), C.byref(h)))
+    return _read_result(h)
+
+
+def _read_result(h) -> dict:
     try:
         m, n, nt, mx = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int()
         host_check(host().hn_mps_shape(h, C.byref(m), C.byref(n), C.byref(nt), C.byref(mx)))
@@ -515,7 +533,16 @@ def read_mps(path: str | None = None, text: bytes | str | None = None, fmt: int 
     """An MPS file as the LP dict lp_solve / lp_solve_batch take: the reader's
     triplets go to the device (hn_csr_create_coo) and come back as the CSR the
     reference's from_triplets builds; rhs -> b, sense, bounds, maximize."""
-    r = mps_read(text=text, path=path, fmt=fmt)
+    return _lp_dict(mps_read(text=text, path=path, fmt=fmt))
+
+
+def read_lp(path: str | None = None, text: bytes | str | None = None) -> dict:
+    """An LP-format file as the LP dict lp_solve / lp_solve_batch take (device
+    CSR as in read_mps)."""
+    return _lp_dict(lp_read(text=text, path=path))
+
+
+def _lp_dict(r: dict) -> dict:
     A = Csr.from_coo(r["m"], r["n"], r["trow"], r["tcol"], r["tval"], transpose=False, autotune=False)
     try:
         rp, ci, val = A.export()

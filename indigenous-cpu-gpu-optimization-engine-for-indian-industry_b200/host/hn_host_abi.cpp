@@ -6,7 +6,7 @@
 #include "hn_backend.hpp"
 #include "hn_host.h"
 #include "hn_lp.hpp"
-#include "hn_mps.hpp"
+#include "hn_read.hpp"
 #include "hn_sm100.h"
 
 namespace {

@@ -1,4 +1,4 @@
-// MPS reader: HyperNova's MPSParser (core/model/mps_parser.cpp) restated with
+// Problem readers. MPS: HyperNova's MPSParser (core/model/mps_parser.cpp) restated with
 // the same results on the same text -- sections, free/fixed layouts and their
 // detection, the lenient fall-backs -- but without its quadratic name
 // lookups: rows and columns are found through hash maps (first occurrence
@@ -29,7 +29,7 @@
 #include <vector>
 
 #include "hn_host.h"
-#include "hn_mps.hpp"
+#include "hn_read.hpp"
 #include "hn_sm100.h"
 
 namespace hn::model {
@@ -308,7 +308,7 @@ private:
 
 class Reader {
 public:
-    explicit Reader(MpsProblem& out) : P(out), row_of_(out.row_names), col_of_(out.col_names) {}
+    explicit Reader(ReadProblem& out) : P(out), row_of_(out.row_names), col_of_(out.col_names) {}
 
     void run(sv text, int format) {
         std::vector<sv> lines;
@@ -364,7 +364,7 @@ public:
     }
 
 private:
-    MpsProblem& P;
+    ReadProblem& P;
     bool free_ = true;
     bool in_int_ = false;
     std::string obj_row_;
@@ -625,18 +625,510 @@ private:
     }
 };
 
+// ---- LP text: model::LPParser (core/model/lp_parser.cpp) restated ----
+// Variables are created where the reference creates them: at their first
+// mention in the objective's linear part, then its bracketed quadratic
+// groups, then constraint left-hand sides and the QUADRATIC section, so the
+// column order matches. Every place where the reference would record an
+// error or let std::stod throw makes the read fail.
+
+inline bool c_space(char ch) { return ch == ' ' || (ch >= '\t' && ch <= '\r'); }  // isspace, C locale
+inline bool c_digit(char ch) { return ch >= '0' && ch <= '9'; }
+inline bool c_alpha(char ch) { return (ch >= 'a' && ch <= 'z') || (ch >= 'A' && ch <= 'Z'); }
+inline bool c_alnum(char ch) { return c_digit(ch) || c_alpha(ch); }
+
+struct LpFail : std::exception {};
+
+double stod_or_throw(sv s) {  // std::stod: prefix conversion, throws on none or ERANGE
+    const auto v = stod_like(s, nullptr);
+    if (!v) throw LpFail();
+    return *v;
+}
+
+class LpReader {
+public:
+    explicit LpReader(ReadProblem& out) : P(out), col_of_(out.col_names) {}
+
+    void run(sv text) {
+        enum class Sec { NONE, OBJ, CONSTRAINTS, BOUNDS, GENERAL, BINARY, SEMI, SOS, QUADRATIC, END };
+        auto section = [&](sv t) -> Sec {
+            if (ieq(t, "MINIMIZE") || ieq(t, "MAXIMIZE") || ieq(t, "MIN") || ieq(t, "MAX")) {
+                P.maximize = (ieq(t, "MAXIMIZE") || ieq(t, "MAX")) ? 1 : 0;
+                return Sec::OBJ;
+            }
+            if (ieq(t, "SUBJECT TO") || ieq(t, "ST") || ieq(t, "S.T.") || ieq(t, "CONSTRAINTS")) return Sec::CONSTRAINTS;
+            if (ieq(t, "BOUNDS")) return Sec::BOUNDS;
+            if (ieq(t, "GENERAL") || ieq(t, "GENERALS")) return Sec::GENERAL;
+            if (ieq(t, "BINARY") || ieq(t, "BINARIES")) return Sec::BINARY;
+            if (ieq(t, "SEMI-CONTINUOUS") || ieq(t, "SEMI-CONT") || ieq(t, "SEMI-INTEGER") || ieq(t, "SEMI-INT"))
+                return Sec::SEMI;
+            if (ieq(t, "SOS")) return Sec::SOS;
+            if (ieq(t, "QUADRATIC") || ieq(t, "Q")) return Sec::QUADRATIC;
+            if (ieq(t, "END")) return Sec::END;
+            return Sec::NONE;
+        };
+        Sec cur = Sec::NONE;
+        int64_t line_no = 0;
+        size_t b = 0;
+        while (b < text.size()) {  // std::getline on '\n'
+            size_t e = text.find('\n', b);
+            if (e == sv::npos) e = text.size();
+            const sv line = text.substr(b, e - b);
+            b = e + 1;
+            ++line_no;
+            const sv t = trim_ends(line, " \t\r\n");
+            if (t.empty() || t[0] == '\\' || (t.size() >= 2 && t[0] == '*' && t[1] == '*')) continue;
+            const Sec ns = section(t);
+            if (ns != Sec::NONE) {
+                // the reference finalises outside its per-line try block
+                guarded(line_no, [&] {
+                    if (cur == Sec::OBJ) finalize_obj();
+                    if (cur == Sec::CONSTRAINTS) finalize_constraint();
+                });
+                cur = ns;
+                continue;
+            }
+            if (cur == Sec::END) break;
+            guarded(line_no, [&] {
+                switch (cur) {
+                    case Sec::OBJ: {
+                        sv ex = t;
+                        const size_t colon = ex.find(':');
+                        if (colon != sv::npos) ex = ex.substr(colon + 1);
+                        obj_buf_ += ' ';
+                        obj_buf_ += ex;
+                        break;
+                    }
+                    case Sec::CONSTRAINTS: {
+                        const size_t colon = t.find(':');
+                        if (colon != sv::npos) {
+                            if (!acc_.empty()) {
+                                error("Unterminated constraint before: " + std::string(t));
+                                acc_.clear();
+                                acc_name_.clear();
+                            }
+                            acc_name_.assign(trim_ends(t.substr(0, colon), " \t\r\n"));
+                            acc_.assign(trim_ends(t.substr(colon + 1), " \t\r\n"));
+                        } else {
+                            acc_ += ' ';
+                            acc_ += t;
+                        }
+                        if (acc_.find("<=") != std::string::npos || acc_.find(">=") != std::string::npos ||
+                            acc_.find('=') != std::string::npos)
+                            finalize_constraint();
+                        break;
+                    }
+                    case Sec::BOUNDS: bounds(t); break;
+                    case Sec::GENERAL: types(t, false); break;
+                    case Sec::BINARY: types(t, true); break;
+                    case Sec::SOS: ++P.sos_records; break;
+                    case Sec::QUADRATIC: P.quadratic_records += quadratic_expr(t); break;
+                    default: break;
+                }
+            });
+        }
+        guarded(line_no, [&] {
+            if (cur == Sec::OBJ) finalize_obj();
+            if (cur == Sec::CONSTRAINTS) finalize_constraint();
+        });
+    }
+
+private:
+    ReadProblem& P;
+    NameIndex col_of_;
+    std::string obj_buf_, acc_, acc_name_;
+
+    void error(std::string msg) { P.errors.push_back(std::move(msg)); }
+
+    template <class F>
+    void guarded(int64_t line_no, F&& f) {
+        try {
+            f();
+        } catch (const LpFail&) {
+            error("Line " + std::to_string(line_no) + ": stod");
+        }
+    }
+
+    int64_t column(sv name) {
+        int64_t j = col_of_.find(name);
+        if (j >= 0) return j;
+        j = static_cast<int64_t>(P.c.size());
+        P.col_names.emplace_back(name);
+        col_of_.add(j);
+        P.c.push_back(0.0);
+        P.lb.push_back(0.0);
+        P.ub.push_back(kInf);
+        P.vtype.push_back(CONTINUOUS);
+        return j;
+    }
+
+    // LPParser::parse_linear_expr (lp_parser.cpp:384-443)
+    std::vector<std::pair<int64_t, double>> linear_expr(sv s) {
+        std::vector<std::pair<int64_t, double>> terms;
+        size_t pos = 0;
+        const size_t n = s.size();
+        while (pos < n) {
+            while (pos < n && c_space(s[pos])) ++pos;
+            if (pos >= n) break;
+            double sign = 1.0;
+            if (s[pos] == '+') {
+                ++pos;
+            } else if (s[pos] == '-') {
+                sign = -1.0;
+                ++pos;
+            }
+            while (pos < n && c_space(s[pos])) ++pos;
+            const size_t old = pos;
+            double coeff = 1.0;
+            size_t ce = pos;
+            while (ce < n && (c_digit(s[ce]) || s[ce] == '.')) ++ce;
+            if (ce < n && (s[ce] == 'e' || s[ce] == 'E')) {
+                size_t en = ce + 1;
+                if (en < n && (s[en] == '+' || s[en] == '-')) ++en;
+                size_t ed = en;
+                while (ed < n && c_digit(s[ed])) ++ed;
+                if (ed > en) ce = ed;
+            }
+            if (ce > pos) {
+                coeff = stod_or_throw(s.substr(pos, ce - pos));
+                pos = ce;
+            }
+            while (pos < n && c_space(s[pos])) ++pos;
+            const size_t vs = pos;
+            while (pos < n && (c_alnum(s[pos]) || s[pos] == '_')) ++pos;
+            if (pos > vs) {
+                const int64_t j = column(s.substr(vs, pos - vs));
+                terms.emplace_back(j, sign * coeff);
+            } else if (pos == old) {
+                ++pos;
+            }
+        }
+        return terms;
+    }
+
+    // LPParser::parse_quadratic_expr (lp_parser.cpp:445-584): only its
+    // variable creation matters to an LP; returns the number of terms
+    int64_t quadratic_expr(sv ex) {
+        enum class K { NUM, NAME, SEP, POWER };
+        struct Tok {
+            K k;
+            sv name;
+        };
+        std::vector<Tok> toks;
+        size_t pos = 0;
+        const size_t n = ex.size();
+        auto skip = [&] {
+            while (pos < n && c_space(ex[pos])) ++pos;
+        };
+        while (pos < n) {
+            skip();
+            if (pos >= n) break;
+            char ch = ex[pos];
+            if (ch == '\\') break;
+            if (ch == '*' || ch == '/') {
+                toks.push_back({K::SEP, sv()});
+                ++pos;
+                continue;
+            }
+            if (ch == '^') {
+                toks.push_back({K::POWER, sv()});
+                ++pos;
+                continue;
+            }
+            if (ch == '[' || ch == ']' || ch == '"' || ch == ',') {
+                ++pos;
+                continue;
+            }
+            if (ch == '+' || ch == '-') {
+                ++pos;
+                skip();
+                if (pos >= n) break;
+                ch = ex[pos];
+            }
+            if (c_digit(ch) || ch == '.') {
+                const size_t st = pos;
+                while (pos < n && (c_digit(ex[pos]) || ex[pos] == '.' || ex[pos] == 'e' || ex[pos] == 'E' ||
+                                   ex[pos] == '+' || ex[pos] == '-'))
+                    ++pos;
+                stod_or_throw(ex.substr(st, pos - st));
+                toks.push_back({K::NUM, sv()});
+                continue;
+            }
+            if (c_alpha(ch) || ch == '_') {
+                const size_t st = pos;
+                while (pos < n && (c_alnum(ex[pos]) || ex[pos] == '_')) ++pos;
+                toks.push_back({K::NAME, ex.substr(st, pos - st)});
+                continue;
+            }
+            ++pos;  // stray character
+        }
+        int64_t count = 0;
+        size_t i = 0;
+        const size_t nt = toks.size();
+        while (i < nt) {
+            if (toks[i].k == K::SEP || toks[i].k == K::POWER) {
+                ++i;
+                continue;
+            }
+            bool lead = false;
+            if (toks[i].k == K::NUM) {
+                lead = true;
+                ++i;
+                while (i < nt && (toks[i].k == K::SEP || toks[i].k == K::POWER)) ++i;
+            }
+            if (i >= nt) break;
+            if (toks[i].k != K::NAME) {
+                if (toks[i].k == K::NUM) ++i;
+                continue;
+            }
+            const sv v1 = toks[i].name;
+            ++i;
+            sv v2 = v1;
+            if (i < nt && toks[i].k == K::POWER) {
+                ++i;
+                if (i < nt && toks[i].k == K::NUM) ++i;
+            } else if (i < nt && toks[i].k == K::SEP) {
+                ++i;
+                if (i < nt && toks[i].k == K::NAME) {
+                    v2 = toks[i].name;
+                    ++i;
+                }
+            } else if (i < nt && toks[i].k == K::NAME) {
+                v2 = toks[i].name;
+                ++i;
+            }
+            if (!lead && i < nt && toks[i].k == K::NUM) ++i;
+            column(v1);
+            column(v2);
+            ++count;
+        }
+        return count;
+    }
+
+    void finalize_obj() {
+        if (obj_buf_.empty()) return;
+        std::string linear, cur;
+        std::vector<std::string> groups;
+        int depth = 0;
+        for (const char ch : obj_buf_) {
+            if (ch == '[') {
+                ++depth;
+                continue;
+            }
+            if (ch == ']') {
+                if (depth > 0 && --depth == 0) {
+                    groups.emplace_back(trim_ends(cur, " \t\r\n"));
+                    cur.clear();
+                }
+                continue;
+            }
+            (depth > 0 ? cur : linear) += ch;
+        }
+        if (depth > 0 && !trim_ends(cur, " \t\r\n").empty()) groups.emplace_back(trim_ends(cur, " \t\r\n"));
+        for (const auto& [j, v] : linear_expr(linear)) P.c[static_cast<size_t>(j)] = v;
+        for (const std::string& g : groups)
+            if (!g.empty()) P.quadratic_records += quadratic_expr(g);
+        obj_buf_.clear();
+    }
+
+    void finalize_constraint() {
+        if (acc_.empty() && acc_name_.empty()) return;
+        const std::string ex = acc_;
+        int32_t sense = 0;
+        size_t sp = std::string::npos;
+        for (size_t i = 0; i + 1 < ex.size(); ++i) {
+            if (ex[i] == '<' && ex[i + 1] == '=') {
+                sp = i;
+                sense = 0;
+                break;
+            }
+            if (ex[i] == '>' && ex[i + 1] == '=') {
+                sp = i;
+                sense = 1;
+                break;
+            }
+        }
+        if (sp == std::string::npos) {
+            sp = ex.find('=');
+            if (sp != std::string::npos) sense = 2;
+        }
+        if (sp == std::string::npos) {
+            error("Invalid constraint format: " + ex);
+            acc_.clear();
+            acc_name_.clear();
+            return;
+        }
+        const sv lhs = trim_ends(sv(ex).substr(0, sp), " \t\r\n");
+        const sv rhs_s = trim_ends(sv(ex).substr(sp + (sense == 2 ? 1 : 2)), " \t\r\n");
+        if (rhs_s.empty()) return;  // the reference keeps the text for the next line
+        const auto rhs = stod_like(rhs_s, nullptr);
+        if (!rhs) {
+            error("Invalid constraint RHS: " + std::string(rhs_s));
+            acc_.clear();
+            acc_name_.clear();
+            return;
+        }
+        const auto terms = linear_expr(lhs);
+        const int64_t i = static_cast<int64_t>(P.sense.size());
+        P.row_names.push_back(acc_name_.empty() ? "c" + std::to_string(i) : acc_name_);
+        P.sense.push_back(sense);
+        P.rhs.push_back(*rhs);
+        P.range_lo.push_back(-kInf);
+        P.range_hi.push_back(kInf);
+        for (const auto& [j, v] : terms) {
+            P.trow.push_back(i);
+            P.tcol.push_back(j);
+            P.tval.push_back(v);
+        }
+        acc_.clear();
+        acc_name_.clear();
+    }
+
+    // NUM of the bound patterns: -?(\d+\.?\d*|\.\d+|inf)
+    static bool bound_num(sv s, size_t& p, sv& out) {
+        const size_t st = p;
+        size_t q = p;
+        if (q < s.size() && s[q] == '-') ++q;
+        if (s.substr(q, 3) == "inf") {
+            q += 3;
+        } else if (q < s.size() && c_digit(s[q])) {
+            while (q < s.size() && c_digit(s[q])) ++q;
+            if (q < s.size() && s[q] == '.') ++q;
+            while (q < s.size() && c_digit(s[q])) ++q;
+        } else if (q + 1 < s.size() && s[q] == '.' && c_digit(s[q + 1])) {
+            ++q;
+            while (q < s.size() && c_digit(s[q])) ++q;
+        } else {
+            return false;
+        }
+        out = s.substr(st, q - st);
+        p = q;
+        return true;
+    }
+    // NAME of the bound patterns: [a-zA-Z_][a-zA-Z0-9_]*
+    static bool bound_name(sv s, size_t& p, sv& out) {
+        if (p >= s.size() || !(c_alpha(s[p]) || s[p] == '_')) return false;
+        const size_t st = p++;
+        while (p < s.size() && (c_alnum(s[p]) || s[p] == '_')) ++p;
+        out = s.substr(st, p - st);
+        return true;
+    }
+    static void ws(sv s, size_t& p) {
+        while (p < s.size() && c_space(s[p])) ++p;
+    }
+    static bool lit(sv s, size_t& p, sv op) {
+        if (s.substr(p, op.size()) != op) return false;
+        p += op.size();
+        return true;
+    }
+    static double bound_value(sv tok) {
+        std::string low(tok);
+        for (char& ch : low)
+            if (ch >= 'A' && ch <= 'Z') ch = static_cast<char>(ch - 'A' + 'a');
+        if (low == "inf" || low == "+inf" || low == "infinity") return kInf;
+        if (low == "-inf" || low == "-infinity") return -kInf;
+        return stod_or_throw(tok);
+    }
+
+    // LPParser::parse_bounds (lp_parser.cpp:242-313): the five whole-line
+    // patterns in the reference's order
+    void bounds(sv line) {
+        sv name, a, c;
+        bool has_lb = false, has_ub = false, fixed = false;
+        double lb = -kInf, ub = kInf;
+        auto at_end = [&](size_t p) {
+            ws(line, p);
+            return p == line.size();
+        };
+        size_t p = 0;
+        bool ok = false;
+        // NUM <= NAME <= NUM  |  NUM <= NAME
+        ws(line, p);
+        if (bound_num(line, p, a) && (ws(line, p), lit(line, p, "<=")) && (ws(line, p), bound_name(line, p, name))) {
+            const size_t after = p;
+            size_t q = p;
+            ws(line, q);
+            if (lit(line, q, "<=") && (ws(line, q), bound_num(line, q, c)) && at_end(q)) {
+                lb = bound_value(a);
+                ub = bound_value(c);
+                has_lb = has_ub = ok = true;
+            } else if (at_end(after)) {
+                lb = bound_value(a);
+                has_lb = ok = true;
+            }
+        }
+        if (!ok) {
+            // NAME <= NUM  |  NAME >= NUM  |  NAME = NUM
+            p = 0;
+            ws(line, p);
+            sv nm;
+            if (bound_name(line, p, nm)) {
+                ws(line, p);
+                const sv ops[3] = {"<=", ">=", "="};
+                for (int k = 0; k < 3 && !ok; ++k) {
+                    size_t q = p;
+                    if (lit(line, q, ops[k]) && (ws(line, q), bound_num(line, q, c)) && at_end(q)) {
+                        name = nm;
+                        const double v = bound_value(c);
+                        if (k == 0) {
+                            ub = v;
+                            has_ub = true;
+                        } else if (k == 1) {
+                            lb = v;
+                            has_lb = true;
+                        } else {
+                            lb = ub = v;
+                            has_lb = has_ub = fixed = true;
+                        }
+                        ok = true;
+                    }
+                }
+            }
+        }
+        if (!ok) name = line;  // no pattern: the whole line as a name
+        const int64_t j = col_of_.find(name);
+        if (j < 0) return;
+        if (fixed) {
+            P.lb[j] = lb;
+            P.ub[j] = ub;
+        } else {
+            if (has_lb) P.lb[j] = lb;
+            if (has_ub) P.ub[j] = ub;
+        }
+    }
+
+    void types(sv line, bool binary) {
+        Tokens t(line);
+        sv w;
+        while (t.str(w)) {
+            const int64_t j = col_of_.find(w);
+            if (j < 0) continue;
+            P.vtype[j] = binary ? BINARY : INTEGER;
+            if (binary) {
+                P.lb[j] = 0.0;
+                P.ub[j] = 1.0;
+            }
+        }
+    }
+};
+
 }  // namespace
 
-void read_mps(std::string_view text, int format, MpsProblem& out) {
-    out = MpsProblem{};
+void read_mps(std::string_view text, int format, ReadProblem& out) {
+    out = ReadProblem{};
     Reader(out).run(text, format);
+}
+
+void read_lp(std::string_view text, ReadProblem& out) {
+    out = ReadProblem{};
+    LpReader(out).run(text);
 }
 
 }  // namespace hn::model
 
 // ---- C ABI ----
 struct hn_mps {
-    hn::model::MpsProblem p;
+    hn::model::ReadProblem p;
 };
 
 namespace {
@@ -669,6 +1161,35 @@ int hn_mps_read_file(const char* path, int format, hn_mps** out) {
     buf << f.rdbuf();
     const std::string text = buf.str();
     return hn_mps_read_string(text.data(), static_cast<int64_t>(text.size()), format, out);
+}
+
+int hn_lp_read_string(const char* text, int64_t len, hn_mps** out) {
+    if (!out || (!text && len > 0) || len < 0) return mps_fail(HN_ERR_INVALID_ARG, "hn_lp_read_string: bad arguments");
+    *out = nullptr;
+    try {
+        auto* h = new hn_mps;
+        hn::model::read_lp(std::string_view(text ? text : "", static_cast<size_t>(len)), h->p);
+        if (!h->p.errors.empty()) {
+            const std::string msg = "LP text rejected (" + std::to_string(h->p.errors.size()) +
+                                    " errors), first: " + h->p.errors.front();
+            delete h;
+            return mps_fail(HN_ERR_INVALID_ARG, msg);
+        }
+        *out = h;
+        return HN_OK;
+    } catch (const std::bad_alloc&) {
+        return mps_fail(HN_ERR_OUT_OF_MEMORY, "hn_lp_read_string: out of host memory");
+    }
+}
+
+int hn_lp_read_file(const char* path, hn_mps** out) {
+    if (!path || !out) return mps_fail(HN_ERR_INVALID_ARG, "hn_lp_read_file: bad arguments");
+    std::ifstream f(path, std::ios::binary);
+    if (!f.is_open()) return mps_fail(HN_ERR_INVALID_ARG, std::string("Cannot open file: ") + path);
+    std::ostringstream buf;
+    buf << f.rdbuf();
+    const std::string text = buf.str();
+    return hn_lp_read_string(text.data(), static_cast<int64_t>(text.size()), out);
 }
 
 int hn_mps_shape(const hn_mps* h, int64_t* m, int64_t* n, int64_t* ntriplets, int* maximize) {

@@ -1,5 +1,5 @@
-// MPS reader of the host layer (hn_mps.cpp): the problem as arrays, the
-// constraint coefficients as triplets in file order.
+// Problem readers of the host layer (hn_read.cpp): MPS and LP text to the
+// problem as arrays, the constraint coefficients as triplets in file order.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -8,7 +8,7 @@
 
 namespace hn::model {
 
-struct MpsProblem {
+struct ReadProblem {
     std::string name;
     int maximize = 0;
     // rows: sense 0 LE, 1 GE, 2 EQ (model::ConstraintSense); rhs; the RANGES
@@ -24,11 +24,14 @@ struct MpsProblem {
     std::vector<int64_t> trow, tcol;
     std::vector<double> tval;
     std::vector<std::string> warnings;
+    std::vector<std::string> errors;  // the reference would report the read as failed
     int64_t sos_records = 0, quadratic_records = 0;  // read past, not kept
 };
 
 // format: -1 detect as the reference does, 0 free, 1 fixed
-void read_mps(std::string_view text, int format, MpsProblem& out);
+void read_mps(std::string_view text, int format, ReadProblem& out);
+// CPLEX-style LP text with model::LPParser's results
+void read_lp(std::string_view text, ReadProblem& out);
 
 }  // namespace hn::model
 

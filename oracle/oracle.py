@@ -103,6 +103,8 @@ def ref():
             "hnref_mps_name": (C.c_char_p, [_vp, C.c_int, _i64]),
             "hnref_mps_free": (None, [_vp]),
             "hnref_mps_parse_ms": (C.c_double, [C.c_char_p, _i64]),
+            "hnref_lp_parse": (_vp, [C.c_char_p, _i64]),
+            "hnref_parse_errors": (_i64, [_vp]),
             "hnref_cholesky_solve": (C.c_int, [_i64, _u64p, _u64p, _f64p, _f64p]),
             "hnref_ipm_solve": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, _i32p, _f64p,
                                           _f64p, C.c_int, C.c_int, C.c_int, _f64p, _i64p, _f64p, _f64p]),
@@ -320,11 +322,12 @@ def from_triplets_port(rows: int, cols: int, ti, tj, tv):
     return rp, np.array(ci, dtype=np.uint64), np.array(val, dtype=np.float64)
 
 
-def ref_mps(text: bytes, fmt: int = -1) -> dict:
+def ref_mps(text: bytes, fmt: int = -1, lp_format: bool = False) -> dict:
     """model::MPSParser::parse_string on `text` (fmt -1: the parser's own
-    layout detection, 0 free, 1 fixed): the parsed problem's arrays, the
-    constraint matrix as the reference's CSR, and the row/column names."""
-    h = ref().hnref_mps_parse(text, len(text), fmt)
+    layout detection, 0 free, 1 fixed), or model::LPParser::parse_string when
+    lp_format: the parsed problem's arrays, the constraint matrix as the
+    reference's CSR, the row/column names and the error count."""
+    h = ref().hnref_lp_parse(text, len(text)) if lp_format else ref().hnref_mps_parse(text, len(text), fmt)
     try:
         m, n, nnz, mx, ok, nw = (C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32(), C.c_int32(), C.c_int64())
         ref().hnref_mps_shape(h, C.byref(m), C.byref(n), C.byref(nnz), C.byref(mx), C.byref(ok), C.byref(nw))
@@ -343,6 +346,7 @@ def ref_mps(text: bytes, fmt: int = -1) -> dict:
         for k, size in (("ci", nnz), ("val", nnz), ("c", n), ("lb", n), ("ub", n), ("vtype", n), ("rhs", m),
                         ("sense", m), ("range_lo", m), ("range_hi", m)):
             out[k] = out[k][:size]
+        out["errors"] = ref().hnref_parse_errors(h)
         out["name"] = ref().hnref_mps_name(h, -1, 0).decode()
         out["row_names"] = [ref().hnref_mps_name(h, 0, i).decode() for i in range(m)]
         out["col_names"] = [ref().hnref_mps_name(h, 1, j).decode() for j in range(n)]

@@ -1,6 +1,7 @@
-// extern "C" shim over the reference's MPS reader (model::MPSParser,
-// core/model/mps_parser.cpp), compiled from the reference's own sources into
-// oracle/_ref/libhnref.so by oracle/Makefile.
+// extern "C" shim over the reference's problem readers (model::MPSParser,
+// core/model/mps_parser.cpp; model::LPParser, core/model/lp_parser.cpp),
+// compiled from the reference's own sources into oracle/_ref/libhnref.so by
+// oracle/Makefile.
 //
 // TEST INFRASTRUCTURE ONLY: the checker for tests/ and bench.py's CPU leg.
 // Nothing in the product links or calls it.
@@ -11,6 +12,8 @@
 //                        matrix (CSR from SparseMatrix::from_triplets), rows,
 //                        columns, objective sense
 //   hnref_mps_parse_ms -> wall time of one parse_string (CPU baseline)
+//   hnref_lp_parse    -> LPParser::parse_string; read with the same accessors
+#include "lp_parser.hpp"
 #include "mps_parser.hpp"
 
 #include <chrono>
@@ -18,13 +21,25 @@
 #include <cstring>
 #include <string>
 
+using hypernova::model::LPParser;
 using hypernova::model::MPSParser;
-using hypernova::model::MPSParseResult;
 
 namespace {
-struct RefMps {
-    MPSParseResult r;
+struct RefMps {  // the parts of MPSParseResult / LPParseResult read here
+    struct {
+        hypernova::model::Problem problem;
+        bool success = false;
+        std::vector<std::string> warnings, errors;
+    } r;
 };
+
+template <class R>
+void keep(RefMps* h, R&& res) {
+    h->r.problem = std::move(res.problem);
+    h->r.success = res.success;
+    h->r.warnings = res.warnings;
+    h->r.errors = res.errors;
+}
 }  // namespace
 
 extern "C" {
@@ -33,8 +48,26 @@ void* hnref_mps_parse(const char* text, int64_t len, int format) {
     MPSParser p;
     if (format >= 0) p.set_free_format(format == 0);
     auto* h = new RefMps;
-    h->r = p.parse_string(std::string(text, static_cast<std::size_t>(len)));
+    keep(h, p.parse_string(std::string(text, static_cast<std::size_t>(len))));
     return h;
+}
+
+// LPParser::parse_string; an exception escaping it (the reference finalises
+// pending statements outside its per-line try block) counts as a failed read
+void* hnref_lp_parse(const char* text, int64_t len) {
+    LPParser p;
+    auto* h = new RefMps;
+    try {
+        keep(h, p.parse_string(std::string(text, static_cast<std::size_t>(len))));
+    } catch (const std::exception& e) {
+        h->r.success = false;
+        h->r.errors.push_back(e.what());
+    }
+    return h;
+}
+
+int64_t hnref_parse_errors(const void* hv) {
+    return static_cast<int64_t>(static_cast<const RefMps*>(hv)->r.errors.size());
 }
 
 int hnref_mps_shape(const void* hv, int64_t* m, int64_t* n, int64_t* nnz, int* maximize, int* success,
@@ -92,7 +125,7 @@ double hnref_mps_parse_ms(const char* text, int64_t len) {
     const std::string s(text, static_cast<std::size_t>(len));
     MPSParser p;
     const auto t0 = std::chrono::steady_clock::now();
-    MPSParseResult r = p.parse_string(s);
+    auto r = p.parse_string(s);
     const auto t1 = std::chrono::steady_clock::now();
     return r.success ? std::chrono::duration<double, std::milli>(t1 - t0).count() : -1.0;
 }
