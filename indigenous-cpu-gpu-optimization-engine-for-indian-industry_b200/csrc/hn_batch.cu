@@ -395,25 +395,35 @@ __global__ void __launch_bounds__(kT, 4) batch_ldlt_update_kernel(int s, int cnt
                                                                const int32_t* __restrict__ status,
                                                                double* __restrict__ dense,
                                                                const double* __restrict__ dD) {
-    // k-major copies of the two panel slices, kFb / 2 columns at a time:
-    // sW[q][r] = L[rb+r, k0+kh+q] D_(kh+q), sL[q][c] = L[cb+c, k0+kh+q]
-    // row stride 68 doubles: a half-warp's fragment loads (k = l%4, column
-    // l/4) fall in 16 distinct banks
-    constexpr int kUP = kFb + 4;
-    __shared__ double sW[kFb / 2][kUP];
-    __shared__ double sL[kFb / 2][kUP];
+    // row-major copies of the two panel slices, kFb / 2 columns at a time:
+    // sW[r][q] = L[rb+r, k0+kh+q] D_(kh+q), sL[c][q] = L[cb+c, k0+kh+q].
+    // A warp stages one row (32 consecutive doubles: conflict-free stores);
+    // the row stride of 36 doubles puts a half-warp's fragment loads (row
+    // l/4, k = l%4) on 16 distinct bank pairs.
+    constexpr int kUP = kFb / 2 + 4;
+    __shared__ double sW[kFb][kUP];
+    __shared__ double sL[kFb][kUP];
     const int tid = threadIdx.x;
-    const int ty = tid >> 4, tx = tid & 15;
     const int k0 = s * kFb;
+    int lo = 0;  // the instance of the previous pair: pairs arrive in increasing order
     for (int64_t pidx = blockIdx.x; pidx < npairs; pidx += gridDim.x) {
-        // instance of this pair: first b with pairs[b] > pidx (pairs is inclusive)
-        int lo = 0, hi = cnt - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (pairs[mid] <= pidx)
-                lo = mid + 1;
-            else
-                hi = mid;
+        // instance of this pair: first b with pairs[b] > pidx (pairs is
+        // inclusive), searched from the previous one by doubling steps
+        if (pairs[lo] <= pidx) {
+            int step = 1, base = lo;
+            while (base + step < cnt - 1 && pairs[base + step] <= pidx) {
+                base += step;
+                step <<= 1;
+            }
+            int a = base + 1, b = min(base + step, cnt - 1);
+            while (a < b) {
+                const int mid = (a + b) >> 1;
+                if (pairs[mid] <= pidx)
+                    a = mid + 1;
+                else
+                    b = mid;
+            }
+            lo = a;
         }
         const int inst = order[lo];
         if (status[inst] != ST_RUN) continue;  // uniform across the CTA
@@ -443,17 +453,17 @@ __global__ void __launch_bounds__(kT, 4) batch_ldlt_update_kernel(int s, int cnt
             for (int idx = tid; idx < kFb * (kFb / 2); idx += kT) {
                 const int rr = idx / (kFb / 2), q = idx % (kFb / 2);
                 const bool okr = rb + rr < m && kh + q < nb, okc = cb + rr < m && kh + q < nb;
-                sW[q][rr] = okr ? A[(int64_t)(rb + rr) * m + k0 + kh + q] * Dv[kh + q] : 0.0;
-                sL[q][rr] = okc ? A[(int64_t)(cb + rr) * m + k0 + kh + q] : 0.0;
+                sW[rr][q] = okr ? A[(int64_t)(rb + rr) * m + k0 + kh + q] * Dv[kh + q] : 0.0;
+                sL[rr][q] = okc ? A[(int64_t)(cb + rr) * m + k0 + kh + q] : 0.0;
             }
             __syncthreads();
 #pragma unroll
             for (int kq = 0; kq < kFb / 2; kq += 4) {
                 double a[2], b[4];
 #pragma unroll
-                for (int i = 0; i < 2; ++i) a[i] = sW[kq + fk][wr + 8 * i + fr];  // A(8x4)[fr][fk]
+                for (int i = 0; i < 2; ++i) a[i] = sW[wr + 8 * i + fr][kq + fk];  // A(8x4)[fr][fk]
 #pragma unroll
-                for (int j = 0; j < 4; ++j) b[j] = sL[kq + fk][wc + 8 * j + fr];  // B(4x8)[fk][fr]
+                for (int j = 0; j < 4; ++j) b[j] = sL[wc + 8 * j + fr][kq + fk];  // B(4x8)[fk][fr]
 #pragma unroll
                 for (int i = 0; i < 2; ++i)
 #pragma unroll
