@@ -127,6 +127,15 @@ const char* hn_mps_warning(const hn_mps* h, int64_t i);
 const char* hn_mps_name(const hn_mps* h, int what, int64_t i);
 int hn_mps_free(hn_mps* h);
 
+/* ---- crossover seam (InteriorPointSolver::solve, interior_point.cpp:792-876) ----
+ * The warm basis the reference's crossover hands SimplexSolver::
+ * solve_with_basis (simplex.hpp:64), computed from a barrier endpoint x
+ * (e.g. hn_lp_solve's x_out) and the variable bounds: var_status[j] = -1 at
+ * lower bound, +1 at upper bound, 0 basic candidate, by the reference's rule
+ * (tolerance 1e-6 (1 + max(|lb|, |ub|)), lower tested first). The simplex
+ * polish itself stays the caller's (host) code. */
+int hn_crossover_basis(int64_t n, const double* x, const double* lb, const double* ub, int* var_status);
+
 /* B200Backend through C: the matrix arrives as the reference's three vectors
  * each call; the backend keeps it resident between calls. */
 typedef struct hn_backend hn_backend;

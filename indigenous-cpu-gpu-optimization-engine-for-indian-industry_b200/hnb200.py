@@ -425,6 +425,7 @@ HOST_SIGNATURES = {
     "hn_mps_warning": (C.c_char_p, [_vp, _i64]),
     "hn_mps_name": (C.c_char_p, [_vp, C.c_int, _i64]),
     "hn_mps_free": (C.c_int, [_vp]),
+    "hn_crossover_basis": (C.c_int, [_i64, _f64p, _f64p, _f64p, C.POINTER(C.c_int)]),
     "hn_be_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
     "hn_be_destroy": (C.c_int, [_vp]),
     "hn_be_spmv": (C.c_int, [_vp, _i64, _i64, _u64p, _u64p, _f64p, _i64, _f64p, _f64p]),
@@ -551,6 +552,16 @@ def _lp_dict(r: dict) -> dict:
     return {"m": r["m"], "n": r["n"], "rp": rp, "ci": ci, "val": val, "b": r["rhs"], "c": r["c"],
             "sense": r["sense"], "lb": r["lb"], "ub": r["ub"], "maximize": bool(r["maximize"]),
             "vtype": r["vtype"], "range_lo": r["range_lo"], "range_hi": r["range_hi"], "name": r["name"]}
+
+
+def crossover_basis(x, lb, ub) -> np.ndarray:
+    """The warm basis the reference's crossover gives its simplex polisher
+    (hn_crossover_basis): -1 at lower bound, +1 at upper bound, 0 basic."""
+    x, lb, ub = f64(x), f64(lb), f64(ub)
+    out = np.zeros(x.shape[0], dtype=np.int32)
+    host_check(host().hn_crossover_basis(x.shape[0], _p(x, C.c_double), _p(lb, C.c_double), _p(ub, C.c_double),
+                                         out.ctypes.data_as(C.POINTER(C.c_int))))
+    return out
 
 
 def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=0.0, max_iter=100,

@@ -1,4 +1,6 @@
 // C ABI of the host layer (include/hn_host.h).
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -56,6 +58,25 @@ void hn_ipm_default_options(hn_ipm_options* o) {
 }
 
 const char* hn_host_last_error(void) { return g_err.c_str(); }
+
+// The starting basis HyperNova's crossover offers its simplex polisher
+// (interior_point.cpp:825-842), from a barrier endpoint x: a variable within
+// 1e-6 (1 + max(|lb|, |ub|)) of a bound is nonbasic there (-1 lower, +1
+// upper, lower tested first), every other one a basic candidate (0). With an
+// infinite bound the tolerance is infinite, as in the reference: a variable
+// with a finite lower and no upper bound is always offered at its lower
+// bound. IEEE arithmetic as the reference's (no contraction).
+int hn_crossover_basis(int64_t n, const double* x, const double* lb, const double* ub, int* var_status) {
+    if (n < 0 || (n > 0 && (!x || !lb || !ub || !var_status))) {
+        g_err = "hn_crossover_basis: bad arguments";
+        return HN_ERR_INVALID_ARG;
+    }
+    for (int64_t j = 0; j < n; ++j) {
+        const double at_tol = 1e-6 * (1.0 + std::max(std::abs(lb[j]), std::abs(ub[j])));
+        var_status[j] = x[j] <= lb[j] + at_tol ? -1 : (x[j] >= ub[j] - at_tol ? 1 : 0);
+    }
+    return HN_OK;
+}
 }  // extern "C"
 
 namespace hn {

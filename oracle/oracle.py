@@ -106,6 +106,8 @@ def ref():
             "hnref_lp_parse": (_vp, [C.c_char_p, _i64]),
             "hnref_parse_errors": (_i64, [_vp]),
             "hnref_cholesky_solve": (C.c_int, [_i64, _u64p, _u64p, _f64p, _f64p]),
+            "hnref_crossover_polish": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, _i32p, _f64p,
+                                                 _f64p, C.c_int, C.c_int, _i32p, _f64p, _i64p]),
             "hnref_ipm_solve": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, _i32p, _f64p,
                                           _f64p, C.c_int, C.c_int, C.c_int, _f64p, _i64p, _f64p, _f64p]),
             "hnref_bench_spmv_pair": (C.c_double, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, C.c_int,
@@ -383,6 +385,25 @@ def ref_ipm_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, max_it
                                _p(ub, C.c_double), int(maximize), int(max_iter), int(crossover), C.byref(obj),
                                C.byref(iters), C.byref(tms), _p(x, C.c_double))
     return {"status": st, "objective": obj.value, "iterations": iters.value, "time_ms": tms.value, "x": x}
+
+
+def ref_crossover_polish(lp: dict, var_status, barrier_status: int, sense=None, lb=None, ub=None,
+                         maximize=False) -> dict:
+    """The reference's crossover polish (interior_point.cpp:792-876) from the
+    caller's warm basis `var_status` and barrier verdict."""
+    m, n = lp["m"], lp["n"]
+    rp, ci, val = u64(lp["rp"]), u64(lp["ci"]), f64(lp["val"])
+    c, b = f64(lp["c"]), f64(lp["b"])
+    sense = np.ascontiguousarray(np.full(m, 2) if sense is None else sense, dtype=np.int32)
+    lb = f64(np.zeros(n) if lb is None else lb)
+    ub = f64(np.full(n, np.inf) if ub is None else ub)
+    vs = np.ascontiguousarray(var_status, dtype=np.int32)
+    obj, iters = C.c_double(), C.c_int64()
+    st = ref().hnref_crossover_polish(m, n, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
+                                      _p(c, C.c_double), _p(b, C.c_double), _p(sense, C.c_int32),
+                                      _p(lb, C.c_double), _p(ub, C.c_double), int(maximize), int(barrier_status),
+                                      _p(vs, C.c_int32), C.byref(obj), C.byref(iters))
+    return {"status": st, "objective": obj.value, "iterations": iters.value}
 
 
 def ref_normal_equations(rp, ci, val, D, reg, n):

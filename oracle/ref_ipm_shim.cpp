@@ -1,7 +1,8 @@
 // Second shim over the reference (TEST INFRASTRUCTURE ONLY): reaches the IPM
 // helpers that core/lp/interior_point.cpp keeps in an anonymous namespace --
-// build_normal_equations (:144-200), matvec (:52-59), matvec_t (:61-69) and
-// max_step (:134-142) -- by compiling that file into this translation unit.
+// build_normal_equations (:144-200), matvec (:52-59), matvec_t (:61-69),
+// max_step (:134-142) and remove_duplicate_rows (the crossover's problem) --
+// by compiling that file into this translation unit.
 // oracle/Makefile links this object in place of interior_point.o, so the
 // library still holds exactly one InteriorPointSolver.
 #include "interior_point.cpp"
@@ -108,6 +109,67 @@ double hnref_step_sample(int64_t m, int64_t n, const uint64_t* rp, const uint64_
         *nnzn_out = s;
     }
     return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// The reference's crossover polish (interior_point.cpp:792-876) from a given
+// barrier endpoint: SimplexSolver::solve_with_basis on the problem with
+// duplicate rows removed, from `var_status` (the caller's warm basis), with
+// crossover_max_iter iterations; if that gives no definitive verdict, a
+// cold SimplexSolver::solve. `barrier_status` is the barrier's verdict
+// (OPTIMAL = converged). Returns the final status; objective, iterations.
+int hnref_crossover_polish(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, const double* val,
+                           const double* c, const double* b, const int* sense, const double* lb,
+                           const double* ub, int maximize, int barrier_status, const int* var_status,
+                           double* obj, int64_t* iters) {
+    using namespace hypernova::model;
+    ProblemBuilder builder("hnref");
+    for (int64_t j = 0; j < n; ++j) builder.add_variable(lb[j], ub[j]);
+    for (int64_t i = 0; i < m; ++i) {
+        std::vector<std::pair<std::size_t, double>> coeffs;
+        for (uint64_t k = rp[i]; k < rp[i + 1]; ++k) coeffs.emplace_back(ci[k], val[k]);
+        const ConstraintSense s =
+            sense[i] == 0 ? ConstraintSense::LE : (sense[i] == 1 ? ConstraintSense::GE : ConstraintSense::EQ);
+        builder.add_constraint(coeffs, s, b[i]);
+    }
+    std::vector<std::pair<std::size_t, double>> objc;
+    for (int64_t j = 0; j < n; ++j) objc.emplace_back(j, c[j]);
+    builder.set_objective(objc, maximize ? ObjectiveSense::MAXIMIZE : ObjectiveSense::MINIMIZE);
+    Problem cleaned = hypernova::lp::remove_duplicate_rows(builder.build());
+    const bool done = barrier_status == static_cast<int>(ProblemStatus::OPTIMAL);
+    int status = barrier_status;
+    *obj = 0.0;
+    *iters = 0;
+    auto adopt = [&](const hypernova::lp::SimplexResult& sim) {
+        if (sim.status == ProblemStatus::OPTIMAL) {
+            status = static_cast<int>(ProblemStatus::OPTIMAL);
+            *obj = sim.objective_value;
+            *iters = static_cast<int64_t>(sim.iterations);
+        } else if (!done && sim.status == ProblemStatus::INFEASIBLE) {
+            status = static_cast<int>(ProblemStatus::INFEASIBLE);
+        } else if (sim.status == ProblemStatus::UNBOUNDED) {
+            status = static_cast<int>(ProblemStatus::UNBOUNDED);
+        }
+    };
+    const auto tol = hypernova::numerical::ToleranceConfig::industrial_defaults();
+    bool resolved = false;
+    try {
+        hypernova::lp::SimplexOptions warm;
+        warm.max_iterations = hypernova::lp::InteriorPointOptions{}.crossover_max_iter;
+        hypernova::lp::SimplexSolver polisher(tol, warm);
+        auto sim = polisher.solve_with_basis(cleaned, std::vector<int>(var_status, var_status + n));
+        adopt(sim);
+        resolved = sim.status == ProblemStatus::OPTIMAL || sim.status == ProblemStatus::UNBOUNDED ||
+                   (sim.status == ProblemStatus::INFEASIBLE && !done);
+    } catch (...) {
+    }
+    if (!resolved) {
+        try {
+            hypernova::lp::SimplexSolver polisher(tol, hypernova::lp::SimplexOptions{});
+            adopt(polisher.solve(cleaned));
+        } catch (...) {
+        }
+    }
+    return status;
 }
 
 }  // extern "C"
