@@ -647,11 +647,14 @@ int hn_csr_create_coo(int64_t m, int64_t n, int64_t count, const int64_t* rows, 
             c32[k] = static_cast<int32_t>(cols[k]);
         }
         cudaStream_t s = nullptr;
-        int32_t* dr = dmalloc<int32_t>(count);
-        int32_t* dc = dmalloc<int32_t>(count);
-        double* dv = dmalloc<double>(count);
+        int32_t* dr = nullptr;
+        int32_t* dc = nullptr;
+        double* dv = nullptr;
         hn_csr* A = new hn_csr();
         try {
+            dr = dmalloc<int32_t>(count);
+            dc = dmalloc<int32_t>(count);
+            dv = dmalloc<double>(count);
             if (count > 0) {
                 check_cuda(cudaMemcpy(dr, r32.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice), "H2D rows");
                 check_cuda(cudaMemcpy(dc, c32.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice), "H2D cols");
