@@ -42,6 +42,10 @@ typedef struct hn_ipm_options {
     /* the warm start's final shift is at least this times the default
      * start's entries (0.01) */
     double warm_start_floor;
+    /* hn_lp_solve's normal-matrix factorisation on the host (the reference's
+     * SparseCholesky seat): 0 auto = dense LDL^T up to 12,000 rows, sparse
+     * LDL^T (AMD + supernodal, hn_sparse_ldlt_solve) above; 1 dense; 2 sparse */
+    int factorization;
 } hn_ipm_options;
 
 /* InteriorPointResult (core/lp/interior_point.hpp:29-38) plus phase times;
@@ -126,6 +130,23 @@ const char* hn_mps_warning(const hn_mps* h, int64_t i);
 /* what -1: problem name; 0: row i's name; 1: column i's name (NULL if none) */
 const char* hn_mps_name(const hn_mps* h, int what, int64_t i);
 int hn_mps_free(hn_mps* h);
+
+/* ---- sparse LDL^T (the SparseCholesky interface, core/numerical/factorization.hpp:162-208) ----
+ * Approximate minimum degree ordering, supernodes, multifrontal numerics
+ * with the reference's pivot clamp (d <= singular_tol -> singular_tol,
+ * factorization.cpp:1310-1313). The matrix is given in CSR with both
+ * triangles (the IPM's normal-matrix layout). hn_amd_order returns the
+ * ordering alone (perm[new] = old); hn_sparse_ldlt_solve analyses,
+ * factorises and solves nrhs right-hand sides in place (x: nrhs x m). */
+typedef struct hn_sparse_ldlt_stats {
+    int64_t nnz_L;       /* strictly lower entries of L */
+    int64_t supernodes;
+    int singular;        /* a pivot was clamped */
+    double analyze_ms, factor_ms;
+} hn_sparse_ldlt_stats;
+int hn_amd_order(int64_t m, const uint64_t* rp, const uint64_t* ci, int64_t* perm);
+int hn_sparse_ldlt_solve(int64_t m, const uint64_t* rp, const uint64_t* ci, const double* val, double singular_tol,
+                         int64_t nrhs, double* x, hn_sparse_ldlt_stats* stats);
 
 /* ---- crossover seam (InteriorPointSolver::solve, interior_point.cpp:792-876) ----
  * The warm basis the reference's crossover hands SimplexSolver::

@@ -395,7 +395,8 @@ class IpmOptions(C.Structure):
     _fields_ = [("max_iterations", C.c_int), ("time_limit_seconds", C.c_double), ("convergence_tol", C.c_double),
                 ("complementarity_tol", C.c_double), ("regularization", C.c_double), ("device", C.c_int),
                 ("verbose", C.c_int), ("interrupt_cb", INTERRUPT_CB), ("interrupt_user", C.c_void_p),
-                ("initial_x", _f64p), ("initial_y", _f64p), ("initial_s", _f64p), ("warm_start_floor", C.c_double)]
+                ("initial_x", _f64p), ("initial_y", _f64p), ("initial_s", _f64p), ("warm_start_floor", C.c_double),
+                ("factorization", C.c_int)]
 
 
 class IpmResult(C.Structure):
@@ -403,6 +404,11 @@ class IpmResult(C.Structure):
                 ("solve_time_ms", C.c_double), ("device_ms", C.c_double), ("factor_ms", C.c_double),
                 ("solve_ms", C.c_double), ("nnz_normal", C.c_int64), ("warm_start_used", C.c_int),
                 ("kkt_default", C.c_double), ("kkt_warm", C.c_double)]
+
+
+class SparseLdltStats(C.Structure):
+    _fields_ = [("nnz_L", C.c_int64), ("supernodes", C.c_int64), ("singular", C.c_int), ("analyze_ms", C.c_double),
+                ("factor_ms", C.c_double)]
 
 
 HOST_SIGNATURES = {
@@ -426,6 +432,9 @@ HOST_SIGNATURES = {
     "hn_mps_name": (C.c_char_p, [_vp, C.c_int, _i64]),
     "hn_mps_free": (C.c_int, [_vp]),
     "hn_crossover_basis": (C.c_int, [_i64, _f64p, _f64p, _f64p, C.POINTER(C.c_int)]),
+    "hn_amd_order": (C.c_int, [_i64, _u64p, _u64p, _i64p]),
+    "hn_sparse_ldlt_solve": (C.c_int, [_i64, _u64p, _u64p, _f64p, C.c_double, _i64, _f64p,
+                                       C.POINTER(SparseLdltStats)]),
     "hn_be_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
     "hn_be_destroy": (C.c_int, [_vp]),
     "hn_be_spmv": (C.c_int, [_vp, _i64, _i64, _u64p, _u64p, _f64p, _i64, _f64p, _f64p]),
@@ -554,6 +563,30 @@ def _lp_dict(r: dict) -> dict:
             "vtype": r["vtype"], "range_lo": r["range_lo"], "range_hi": r["range_hi"], "name": r["name"]}
 
 
+def amd_order(rp, ci) -> np.ndarray:
+    """Approximate-minimum-degree ordering of a symmetric pattern (both
+    triangles): perm[new] = old (hn_amd_order)."""
+    rp, ci = u64(rp), u64(ci)
+    m = rp.shape[0] - 1
+    perm = np.zeros(m, dtype=np.int64)
+    host_check(host().hn_amd_order(m, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(perm, C.c_int64)))
+    return perm
+
+
+def sparse_ldlt_solve(rp, ci, val, B, singular_tol: float = 1e-12):
+    """Solve N X = B with the host sparse LDL^T (hn_sparse_ldlt_solve); N in
+    CSR with both triangles, B of shape (m,) or (nrhs, m). Returns (X, stats)."""
+    rp, ci, val = u64(rp), u64(ci), f64(val)
+    m = rp.shape[0] - 1
+    X = np.array(B, dtype=np.float64, order="C", copy=True)
+    nrhs = 1 if X.ndim == 1 else X.shape[0]
+    st = SparseLdltStats()
+    host_check(host().hn_sparse_ldlt_solve(m, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double),
+                                           float(singular_tol), nrhs, _p(X, C.c_double), C.byref(st)))
+    return X, {"nnz_L": st.nnz_L, "supernodes": st.supernodes, "singular": bool(st.singular),
+               "analyze_ms": st.analyze_ms, "factor_ms": st.factor_ms}
+
+
 def crossover_basis(x, lb, ub) -> np.ndarray:
     """The warm basis the reference's crossover gives its simplex polisher
     (hn_crossover_basis): -1 at lower bound, +1 at upper bound, 0 basic."""
@@ -565,7 +598,8 @@ def crossover_basis(x, lb, ub) -> np.ndarray:
 
 
 def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=0.0, max_iter=100,
-             time_limit=0.0, device=0, interrupt=None, verbose=False, x0=None, y0=None, s0=None, warm_floor=None):
+             time_limit=0.0, device=0, interrupt=None, verbose=False, x0=None, y0=None, s0=None, warm_floor=None,
+             factorization=0):
     """GPU IPM on an LP given as CSR (rows EQ and x >= 0 unless told otherwise);
     x0/y0/s0: optional warm start in the original space."""
     m, n = int(lp["m"]), int(lp["n"])
@@ -585,6 +619,7 @@ def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=
     keep = _warm_arrays(opt, x0, y0, s0)  # noqa: F841 (alive through the call)
     if warm_floor is not None:
         opt.warm_start_floor = warm_floor
+    opt.factorization = int(factorization)  # 0 auto, 1 dense, 2 sparse (host normal-matrix factorisation)
     res = IpmResult()
     x = np.zeros(n)
     y = np.full(m, np.nan)

@@ -1,5 +1,7 @@
 // C ABI of the host layer (include/hn_host.h).
 #include <algorithm>
+#include <climits>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -55,9 +57,53 @@ void hn_ipm_default_options(hn_ipm_options* o) {
     o->initial_y = nullptr;
     o->initial_s = nullptr;
     o->warm_start_floor = 1e-2;
+    o->factorization = 0;
 }
 
 const char* hn_host_last_error(void) { return g_err.c_str(); }
+
+int hn_amd_order(int64_t m, const uint64_t* rp, const uint64_t* ci, int64_t* perm) {
+    return wrap([&] {
+        if (m < 0 || m >= INT32_MAX || !rp || (m > 0 && !perm)) throw std::invalid_argument("hn_amd_order: bad arguments");
+        std::vector<int> r(m + 1), c(rp[m]);
+        for (int64_t i = 0; i <= m; ++i) r[i] = static_cast<int>(rp[i]);
+        for (uint64_t k = 0; k < rp[m]; ++k) {
+            if (ci[k] >= static_cast<uint64_t>(m)) throw std::invalid_argument("hn_amd_order: column out of range");
+            c[k] = static_cast<int>(ci[k]);
+        }
+        const auto ord = hn::lp::amd_order(static_cast<int>(m), r, c);
+        for (int64_t k = 0; k < m; ++k) perm[k] = ord[k];
+    });
+}
+
+int hn_sparse_ldlt_solve(int64_t m, const uint64_t* rp, const uint64_t* ci, const double* val, double singular_tol,
+                         int64_t nrhs, double* x, hn_sparse_ldlt_stats* stats) {
+    return wrap([&] {
+        if (m < 0 || m >= INT32_MAX || !rp || (m > 0 && (!val || !ci)) || nrhs < 0 || (nrhs > 0 && !x))
+            throw std::invalid_argument("hn_sparse_ldlt_solve: bad arguments");
+        for (uint64_t k = 0; k < rp[m]; ++k)
+            if (ci[k] >= static_cast<uint64_t>(m)) throw std::invalid_argument("hn_sparse_ldlt_solve: column out of range");
+        hn::lp::SparseLDLT f;
+        const auto t0 = std::chrono::steady_clock::now();
+        f.analyze(static_cast<std::size_t>(m), rp, ci);
+        const auto t1 = std::chrono::steady_clock::now();
+        f.factorize(val, singular_tol);
+        const auto t2 = std::chrono::steady_clock::now();
+        std::vector<double> b(static_cast<std::size_t>(m));
+        for (int64_t r = 0; r < nrhs; ++r) {
+            std::memcpy(b.data(), x + r * m, sizeof(double) * m);
+            f.solve(b);
+            std::memcpy(x + r * m, b.data(), sizeof(double) * m);
+        }
+        if (stats) {
+            stats->nnz_L = static_cast<int64_t>(f.nnz_L());
+            stats->supernodes = static_cast<int64_t>(f.supernodes());
+            stats->singular = f.singular() ? 1 : 0;
+            stats->analyze_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+            stats->factor_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        }
+    });
+}
 
 // The starting basis HyperNova's crossover offers its simplex polisher
 // (interior_point.cpp:825-842), from a barrier endpoint x: a variable within
@@ -122,6 +168,7 @@ int hn_lp_solve(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, co
                 o.interrupt_callback = [cb, user]() { return cb(user) != 0; };
             }
             o.warm_start_floor = opt->warm_start_floor;
+            o.factorization = opt->factorization;
             if (opt->initial_x) {
                 o.initial_point.x = vec(opt->initial_x, n);
                 if (opt->initial_y) o.initial_point.y = vec(opt->initial_y, m);
@@ -190,6 +237,7 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
             o.regularization = opt->regularization;
             o.device = opt->device;
             o.warm_start_floor = opt->warm_start_floor;
+            o.factorization = opt->factorization;
         }
         std::vector<hn::lp::WarmStart> warm;
         if (opt && opt->initial_x) {

@@ -2,7 +2,7 @@
 // lp::InteriorPointSolver::solve (core/lp/interior_point.cpp:402-886), with
 // the iterate, residuals, directions, step lengths and A D A^T assembly on
 // the B200 (include/hn_sm100.h) and the normal-equation factorisation on the
-// host (DenseLDLT). Only scalars, N's values and the m-vectors of the two
+// host (DenseLDLT, or SparseLDLT above 12,000 rows / on request). Only scalars, N's values and the m-vectors of the two
 // normal-equation solves cross PCIe each iteration.
 #include <omp.h>
 
@@ -449,7 +449,8 @@ struct HostNormal {
 
 // iterative_refinement(fac, N, x, rhs) with its defaults 1e-10 / 5 sweeps
 // (core/numerical/refinement.cpp:7-37).
-void refine(const DenseLDLT& fac, const HostNormal& N, std::vector<double>& x, const std::vector<double>& rhs) {
+template <class Fac>
+void refine(const Fac& fac, const HostNormal& N, std::vector<double>& x, const std::vector<double>& rhs) {
     const std::size_t n = x.size();
     double norm_rhs = 0.0;
     for (double v : rhs) norm_rhs = std::max(norm_rhs, std::abs(v));
@@ -571,7 +572,8 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
             result.objective_value = obj;
             return result;
         }
-        if (f.m > kMaxDenseRows)
+        const bool sparse_fac = O.factorization == 2 || (O.factorization == 0 && f.m > kMaxDenseRows);
+        if (!sparse_fac && f.m > kMaxDenseRows)
             throw std::runtime_error("standard form has " + std::to_string(f.m) +
                                      " rows; the host dense factorisation supports up to 12000");
         const std::size_t m = f.m, n = f.n;
@@ -623,13 +625,24 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
             return O.time_limit_seconds > 0.0 && ms_since(start) >= O.time_limit_seconds * 1e3;
         };
         DenseLDLT fac;
+        SparseLDLT sfac;  // the pattern of N is fixed: analysed once, refactorised per iteration
+        if (sparse_fac) {
+            auto ta = Clock::now();
+            sfac.analyze(m, N.rp.data(), N.ci.data());
+            result.factor_ms += ms_since(ta);
+        }
         std::vector<double> hrhs(m), hdlam(m);
         auto solve_normal = [&](const DevBuf& rhs_dev) {
             auto t = Clock::now();
             ck(hn_memcpy_d2h(hrhs.data(), rhs_dev.p, 8 * m, st), "D2H rhs");
             hdlam = hrhs;
-            fac.solve(hdlam);
-            refine(fac, N, hdlam, hrhs);
+            if (sparse_fac) {
+                sfac.solve(hdlam);
+                refine(sfac, N, hdlam, hrhs);
+            } else {
+                fac.solve(hdlam);
+                refine(fac, N, hdlam, hrhs);
+            }
             ck(hn_memcpy_h2d(dlam.p, hdlam.data(), 8 * m, st), "H2D dlam");
             result.solve_ms += ms_since(t);
         };
@@ -664,8 +677,12 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
                 break;
             }
             auto tf = Clock::now();
-            N.to_dense();
-            fac.factorize(N.dense, m, O.singular_tol);
+            if (sparse_fac) {
+                sfac.factorize(N.val.data(), O.singular_tol);
+            } else {
+                N.to_dense();
+                fac.factorize(N.dense, m, O.singular_tol);
+            }
             result.factor_ms += ms_since(tf);
             if (deadline_passed()) {
                 time_up = true;

@@ -84,6 +84,9 @@ struct InteriorPointOptions {
     // its KKT residual is below the default start's.
     WarmStart initial_point;
     double warm_start_floor = 1e-2;
+    // Normal-matrix factorisation on the host: 0 auto (dense LDL^T up to
+    // 12,000 rows, sparse LDL^T above), 1 dense, 2 sparse (SparseLDLT).
+    int factorization = 0;
 };
 
 struct InteriorPointResult {
@@ -188,5 +191,31 @@ private:
     std::size_t m_ = 0;
     bool singular_ = false;
 };
+
+// Sparse LDL^T (hn_sparse_ldlt.cpp): approximate-minimum-degree ordering,
+// supernodes, multifrontal numerics with the reference's pivot clamp.
+// analyze() takes the symmetric pattern with both triangles (the layout of
+// the IPM's normal matrix); factorize() the values in that pattern.
+class SparseLDLT {
+public:
+    void analyze(std::size_t m, const uint64_t* rp, const uint64_t* ci);
+    bool factorize(const double* val, double singular_tol);  // false when a pivot was clamped
+    void solve(std::vector<double>& x) const;                // in place
+    std::size_t size() const { return m_; }
+    std::size_t nnz_L() const { return nnz_L_; }              // strictly lower entries of L
+    std::size_t supernodes() const { return snode_start_.empty() ? 0 : snode_start_.size() - 1; }
+    bool singular() const { return singular_; }
+    const std::vector<int>& perm() const { return perm_; }   // new -> old
+
+private:
+    std::size_t m_ = 0, nnz_L_ = 0;
+    std::vector<int> perm_, iperm_, parent_, snode_start_, snode_of_, snode_parent_, srows_;
+    std::vector<std::size_t> srows_off_, panel_off_, amap_off_;
+    std::vector<std::pair<uint64_t, std::size_t>> amap_;  // (input entry, front position)
+    std::vector<double> L_, D_;
+    bool analyzed_ = false, factored_ = false, singular_ = false;
+};
+// ordering alone: pattern of a symmetric matrix (both triangles), new -> old
+std::vector<int> amd_order(int n, const std::vector<int>& rp, const std::vector<int>& ci);
 
 }  // namespace hn::lp

@@ -97,6 +97,34 @@ def lp_uniform(m: int, n: int, k: int, seed: int) -> dict:
     return lp_from_counts(m, np.full(n, k, dtype=np.int64), seed)
 
 
+def lp_staircase(periods: int, k: int, seed: int) -> dict:
+    """A multi-period (staircase) LP: `periods` blocks of k EQ rows, 2k
+    columns per block, each column with 4 distinct rows in its own block and
+    2 in the next; values and feasibility as lp_from_counts (b = A x0,
+    c = A^T y0 + s0). Its normal matrix is block tridiagonal, so a
+    fill-reducing ordering keeps the factor sparse."""
+    rng = np.random.default_rng(seed)
+    m, n = periods * k, periods * 2 * k
+    rows, cols = [], []
+    for j in range(n):
+        t = j // (2 * k)
+        own = rng.choice(k, 4, replace=False) + t * k
+        nxt = rng.choice(k, 2, replace=False) + (t + 1) * k if t + 1 < periods else np.zeros(0, dtype=np.int64)
+        r = np.concatenate([own, nxt])
+        rows.append(r)
+        cols.append(np.full(r.shape[0], j))
+    rows = np.concatenate(rows)
+    cols = np.concatenate(cols)
+    sign = np.where(rng.random(cols.shape[0]) < 0.5, -1.0, 1.0)
+    vals = sign * rng.uniform(0.1, 1.0, size=cols.shape[0])
+    rp, ci, val = _csr_from_cols(m, n, cols, rows, vals)
+    x0 = rng.uniform(0.5, 2.0, size=n)
+    y0 = rng.standard_normal(m)
+    s0 = rng.uniform(0.5, 2.0, size=n)
+    return {"m": m, "n": n, "rp": rp, "ci": ci, "val": val, "b": csr_matvec(rp, ci, val, x0),
+            "c": csr_tmatvec(rp, ci, val, y0, n) + s0, "x0": x0, "y0": y0, "s0": s0, "seed": seed}
+
+
 def lp_zipf(m: int = 200_000, n: int = 500_000, seed: int = 1000, target_nnz: int | None = 5_000_000) -> dict:
     """Large LP with Zipf(1.5) column counts clipped to [1, 2000]; with
     target_nnz the counts are rescaled (c_j <- max(1, round(c_j * t / sum c)))."""

@@ -106,6 +106,7 @@ def ref():
             "hnref_lp_parse": (_vp, [C.c_char_p, _i64]),
             "hnref_parse_errors": (_i64, [_vp]),
             "hnref_cholesky_solve": (C.c_int, [_i64, _u64p, _u64p, _f64p, _f64p]),
+            "hnref_cholesky_stats": (C.c_int, [_i64, _u64p, _u64p, _f64p, _i64p, _f64p, _f64p, _f64p]),
             "hnref_crossover_polish": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, _i32p, _f64p,
                                                  _f64p, C.c_int, C.c_int, _i32p, _f64p, _i64p]),
             "hnref_ipm_solve": (C.c_int, [_i64, _i64, _u64p, _u64p, _f64p, _f64p, _f64p, _i32p, _f64p,
@@ -385,6 +386,18 @@ def ref_ipm_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, max_it
                                _p(ub, C.c_double), int(maximize), int(max_iter), int(crossover), C.byref(obj),
                                C.byref(iters), C.byref(tms), _p(x, C.c_double))
     return {"status": st, "objective": obj.value, "iterations": iters.value, "time_ms": tms.value, "x": x}
+
+
+def ref_cholesky_stats(rp, ci, val, b=None) -> dict:
+    """SparseCholesky analyze + factorize (+ solve of b): nnz(L), singular,
+    phase times, solution."""
+    rp, ci, val = u64(rp), u64(ci), f64(val)
+    m = rp.shape[0] - 1
+    x = None if b is None else f64(np.array(b, dtype=np.float64, copy=True))
+    nnz, ta, tf = C.c_int64(), C.c_double(), C.c_double()
+    sing = ref().hnref_cholesky_stats(m, _p(rp, C.c_uint64), _p(ci, C.c_uint64), _p(val, C.c_double), C.byref(nnz),
+                                      C.byref(ta), C.byref(tf), None if x is None else _p(x, C.c_double))
+    return {"nnz_L": nnz.value, "singular": bool(sing), "analyze_ms": ta.value, "factor_ms": tf.value, "x": x}
 
 
 def ref_crossover_polish(lp: dict, var_status, barrier_status: int, sense=None, lb=None, ub=None,

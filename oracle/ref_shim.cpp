@@ -13,6 +13,7 @@
 //   hnref_transposed    -> numerical::SparseMatrix::transposed (:84-96)
 //   hnref_from_triplets -> numerical::SparseMatrix::from_triplets (:8-53)
 //   hnref_cholesky_*    -> numerical::SparseCholesky (factorization.hpp:162-208)
+//                          (solve; stats: nnz(L), singular, phase times)
 //   hnref_ipm_solve     -> lp::InteriorPointSolver::solve (interior_point.cpp:402-886)
 #include "sparse_matrix.hpp"
 #include "factorization.hpp"
@@ -150,6 +151,29 @@ int hnref_cholesky_solve(int64_t m, const uint64_t* rp, const uint64_t* ci, cons
     std::vector<double> b(x, x + m);
     ch.solve(b);
     std::memcpy(x, b.data(), sizeof(double) * m);
+    return ch.stats().singular ? 1 : 0;
+}
+
+// SparseCholesky::analyze + factorize on N (CSR, both triangles): nnz(L),
+// the singular flag and the two phase times (ms); x (m, may be null) is a
+// right-hand side replaced by the solution.
+int hnref_cholesky_stats(int64_t m, const uint64_t* rp, const uint64_t* ci, const double* val, int64_t* nnz_L,
+                         double* analyze_ms, double* factor_ms, double* x) {
+    SparseMatrix N = make_csr(m, m, rp, ci, val);
+    hypernova::numerical::SparseCholesky ch;
+    const auto t0 = std::chrono::steady_clock::now();
+    ch.analyze(N);
+    const auto t1 = std::chrono::steady_clock::now();
+    ch.factorize(N);
+    const auto t2 = std::chrono::steady_clock::now();
+    *nnz_L = static_cast<int64_t>(ch.stats().nnz_L);
+    *analyze_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    *factor_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+    if (x) {
+        std::vector<double> b(x, x + m);
+        ch.solve(b);
+        std::memcpy(x, b.data(), sizeof(double) * m);
+    }
     return ch.stats().singular ? 1 : 0;
 }
 
