@@ -13,9 +13,9 @@
 //              merging children, fundamental supernodes
 //   numeric    multifrontal: per supernode a dense front assembled from N
 //              and the children's update matrices, its pivot columns
-//              factorised with the reference's pivot clamp (d <= tol ->
-//              tol, factorization.cpp:1310-1313), the Schur complement
-//              passed to the parent
+//              factorised (blocked right-looking) with the reference's pivot
+//              clamp (d <= tol -> tol, factorization.cpp:1310-1313), the
+//              Schur complement passed to the parent
 //   solve      forward with unit L, divide by D, backward, in supernodes
 #include <omp.h>
 
@@ -291,7 +291,7 @@ void SparseLDLT::analyze(std::size_t m, const uint64_t* rp, const uint64_t* ci) 
     snode_start_.clear();
     for (int j = 0; j < n; ++j) {
         const bool join = j > 0 && parent_[j - 1] == j && child[j].size() == 1 &&
-                          cstruct[j - 1].size() == cstruct[j].size() + 1 && j - snode_start_.back() < 256;
+                          cstruct[j - 1].size() == cstruct[j].size() + 1 && j - snode_start_.back() < 4096;
         if (!join) snode_start_.push_back(j);
     }
     snode_start_.push_back(n);
@@ -352,49 +352,65 @@ void SparseLDLT::analyze(std::size_t m, const uint64_t* rp, const uint64_t* ci) 
 // ---- numeric factorisation (multifrontal) ----
 namespace {
 // front F (nf x nf, column-major, lower used): factor the first w columns
-// with the pivot clamp, leave L there, and form the Schur complement
-// U = F22 - L21 D L21^T (r x r lower, column-major) in `upd`
+// with the pivot clamp, leave L there, and return the Schur complement
+// U = F22 - L21 D L21^T (r x r lower, column-major) in `upd`. Blocked
+// right-looking: a panel of up to 32 pivot columns is factorised against
+// itself, then the whole trailing lower triangle takes its rank-32 update,
+// each column in row chunks held across the panel's pivots.
 void factor_front(double* F, std::size_t nf, std::size_t w, double tol, double* Dout, bool& singular,
                   std::vector<double>& upd) {
-    for (std::size_t k = 0; k < w; ++k) {
-        double* fk = F + k * nf;
-        double d = fk[k];
-        if (d <= tol) {
-            d = tol;
-            singular = true;
+    constexpr std::size_t kNb = 32, kChunk = 64;
+    for (std::size_t kb = 0; kb < w; kb += kNb) {
+        const std::size_t ke = std::min(w, kb + kNb), nbk = ke - kb;
+        for (std::size_t k = kb; k < ke; ++k) {
+            double* fk = F + k * nf;
+            double d = fk[k];
+            if (d <= tol) {
+                d = tol;
+                singular = true;
+            }
+            Dout[k] = d;
+            fk[k] = 1.0;
+            const double inv = 1.0 / d;
+            for (std::size_t i = k + 1; i < nf; ++i) fk[i] *= inv;
+            for (std::size_t j = k + 1; j < ke; ++j) {
+                const double ljd = fk[j] * d;
+                if (ljd == 0.0) continue;
+                double* fj = F + j * nf;
+                for (std::size_t i = j; i < nf; ++i) fj[i] -= fk[i] * ljd;
+            }
         }
-        Dout[k] = d;
-        fk[k] = 1.0;
-        const double inv = 1.0 / d;
-        for (std::size_t i = k + 1; i < nf; ++i) fk[i] *= inv;
-        // update the remaining pivot columns of the panel
-        for (std::size_t j = k + 1; j < w; ++j) {
-            const double ljd = fk[j] * d;
-            if (ljd == 0.0) continue;
+        if (ke >= nf) continue;
+        const std::size_t t = nf - ke;
+        const bool par = t * t * nbk > (std::size_t(1) << 21);
+#pragma omp parallel for schedule(dynamic, 4) if (par)
+        for (std::size_t j = ke; j < nf; ++j) {
+            double c[kNb];
+            bool any = false;
+            for (std::size_t k = 0; k < nbk; ++k) {
+                c[k] = F[(kb + k) * nf + j] * Dout[kb + k];
+                any = any || c[k] != 0.0;
+            }
+            if (!any) continue;
             double* fj = F + j * nf;
-            for (std::size_t i = j; i < nf; ++i) fj[i] -= fk[i] * ljd;
+            for (std::size_t i0 = j; i0 < nf; i0 += kChunk) {
+                const std::size_t len = std::min(kChunk, nf - i0);
+                double acc[kChunk];
+                for (std::size_t i = 0; i < len; ++i) acc[i] = fj[i0 + i];
+                for (std::size_t k = 0; k < nbk; ++k) {
+                    const double ck = c[k];
+                    const double* lk = F + (kb + k) * nf + i0;
+#pragma omp simd
+                    for (std::size_t i = 0; i < len; ++i) acc[i] -= lk[i] * ck;
+                }
+                for (std::size_t i = 0; i < len; ++i) fj[i0 + i] = acc[i];
+            }
         }
     }
     const std::size_t r = nf - w;
     upd.assign(r * r, 0.0);
-    if (r == 0) return;
-    // U(i, j) = F22(i, j) - sum_k L(w+i, k) D_k L(w+j, k), i >= j
-    std::vector<double> LD(r * w);
-    for (std::size_t k = 0; k < w; ++k)
-        for (std::size_t i = 0; i < r; ++i) LD[k * r + i] = F[k * nf + w + i] * Dout[k];
-    const bool par = r * r * w > (1u << 22);
-#pragma omp parallel for schedule(dynamic, 8) if (par)
-    for (std::size_t j = 0; j < r; ++j) {
-        double* u = upd.data() + j * r;
-        const double* f = F + (w + j) * nf + w;
-        for (std::size_t i = j; i < r; ++i) u[i] = f[i];
-        for (std::size_t k = 0; k < w; ++k) {
-            const double ljk = F[k * nf + w + j];
-            if (ljk == 0.0) continue;
-            const double* ld = LD.data() + k * r;
-            for (std::size_t i = j; i < r; ++i) u[i] -= ld[i] * ljk;
-        }
-    }
+    for (std::size_t j = 0; j < r; ++j)
+        std::memcpy(upd.data() + j * r + j, F + (w + j) * nf + w + j, sizeof(double) * (r - j));
 }
 }  // namespace
 
