@@ -420,41 +420,90 @@ bool SparseLDLT::factorize(const double* val, double tol) {
     L_.assign(panel_off_[ns], 0.0);
     D_.assign(m_, 0.0);
     singular_ = false;
-    struct Upd {
-        int s;
-        std::vector<double> u;
-    };
-    std::vector<Upd> stack;
-    std::vector<int> pos(m_, -1);
-    std::vector<double> F;
+    // supernodal tree: children, first descendant (subtrees are contiguous
+    // id ranges in postorder) and the front work of every subtree
+    std::vector<std::vector<int>> kids(ns);
+    std::vector<int> first(ns);
+    std::vector<double> sub(ns, 0.0);
+    double total = 0.0;
     for (int s = 0; s < ns; ++s) {
+        const double nf = static_cast<double>(srows_off_[s + 1] - srows_off_[s]);
+        const double w = static_cast<double>(snode_start_[s + 1] - snode_start_[s]);
+        sub[s] += nf * nf * (w + 1.0);
+        const int p = snode_parent_[s];
+        if (p != -1) {
+            kids[p].push_back(s);
+            sub[p] += sub[s];
+        } else {
+            total += sub[s];
+        }
+    }
+    for (int s = 0; s < ns; ++s) first[s] = s;
+    for (int s = 0; s < ns; ++s)
+        if (snode_parent_[s] != -1) first[snode_parent_[s]] = std::min(first[snode_parent_[s]], first[s]);
+    // independent subtrees below a work cut are factorised in parallel, the
+    // top of the tree afterwards in postorder (its big fronts use the
+    // parallel front kernel)
+    const int threads = std::max(1, omp_get_max_threads());
+    const double cut = total / (4.0 * threads);
+    std::vector<int> roots;
+    std::vector<char> low(ns, 0);
+    for (int s = 0; s < ns; ++s) {
+        const int p = snode_parent_[s];
+        if (sub[s] <= cut && (p == -1 || sub[p] > cut)) roots.push_back(s);
+    }
+    std::sort(roots.begin(), roots.end(), [&](int x, int y) { return sub[x] > sub[y]; });
+    for (int r : roots)
+        for (int t = first[r]; t <= r; ++t) low[t] = 1;
+    std::vector<std::vector<double>> U(ns);  // update matrices awaiting their parent
+
+    auto process = [&](int s, std::vector<int>& pos, std::vector<double>& F, bool& sing) {
         const std::size_t r0 = srows_off_[s], nf = srows_off_[s + 1] - r0;
         const std::size_t w = static_cast<std::size_t>(snode_start_[s + 1] - snode_start_[s]);
         F.assign(nf * nf, 0.0);
         for (std::size_t a = amap_off_[s]; a < amap_off_[s + 1]; ++a) F[amap_[a].second] += val[amap_[a].first];
         for (std::size_t t = 0; t < nf; ++t) pos[srows_[r0 + t]] = static_cast<int>(t);
-        // extend-add the children's update matrices (the top of the stack in postorder)
-        while (!stack.empty() && snode_parent_[stack.back().s] == s) {
-            const Upd& c = stack.back();
-            const std::size_t cr0 = srows_off_[c.s], cw = snode_start_[c.s + 1] - snode_start_[c.s];
-            const std::size_t cr = srows_off_[c.s + 1] - cr0 - cw;
+        // extend-add the children's update matrices
+        for (int c : kids[s]) {
+            if (U[c].empty()) continue;
+            const std::size_t cr0 = srows_off_[c], cw = snode_start_[c + 1] - snode_start_[c];
+            const std::size_t cr = srows_off_[c + 1] - cr0 - cw;
             const int* rows = srows_.data() + cr0 + cw;
             for (std::size_t j = 0; j < cr; ++j) {
-                const std::size_t pj = static_cast<std::size_t>(pos[rows[j]]);
-                double* fcol = F.data() + pj * nf;
-                const double* ucol = c.u.data() + j * cr;
+                double* fcol = F.data() + static_cast<std::size_t>(pos[rows[j]]) * nf;
+                const double* ucol = U[c].data() + j * cr;
                 for (std::size_t i = j; i < cr; ++i) fcol[pos[rows[i]]] += ucol[i];
             }
-            stack.pop_back();
+            std::vector<double>().swap(U[c]);
         }
         for (std::size_t t = 0; t < nf; ++t) pos[srows_[r0 + t]] = -1;
-        Upd u;
-        u.s = s;
-        factor_front(F.data(), nf, w, tol, D_.data() + snode_start_[s], singular_, u.u);
+        std::vector<double> u;
+        factor_front(F.data(), nf, w, tol, D_.data() + snode_start_[s], sing, u);
         double* Lp = L_.data() + panel_off_[s];
         for (std::size_t k = 0; k < w; ++k) std::memcpy(Lp + k * nf, F.data() + k * nf, sizeof(double) * nf);
-        if (nf > w && snode_parent_[s] != -1) stack.push_back(std::move(u));
+        if (nf > w && snode_parent_[s] != -1) U[s] = std::move(u);
+    };
+
+    bool any_singular = false;
+#pragma omp parallel if (roots.size() > 1) reduction(|| : any_singular)
+    {
+        std::vector<int> pos(m_, -1);
+        std::vector<double> F;
+        bool sing = false;
+#pragma omp for schedule(dynamic, 1)
+        for (std::size_t i = 0; i < roots.size(); ++i)
+            for (int t = first[roots[i]]; t <= roots[i]; ++t) process(t, pos, F, sing);
+        any_singular = any_singular || sing;
     }
+    {
+        std::vector<int> pos(m_, -1);
+        std::vector<double> F;
+        bool sing = false;
+        for (int s = 0; s < ns; ++s)
+            if (!low[s]) process(s, pos, F, sing);
+        any_singular = any_singular || sing;
+    }
+    singular_ = any_singular;
     factored_ = true;
     return !singular_;
 }
