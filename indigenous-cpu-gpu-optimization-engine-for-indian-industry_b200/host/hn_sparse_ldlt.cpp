@@ -351,15 +351,53 @@ void SparseLDLT::analyze(std::size_t m, const uint64_t* rp, const uint64_t* ci) 
 
 // ---- numeric factorisation (multifrontal) ----
 namespace {
+// F(i, j) -= sum_{k in [kb, ke)} L(i, k) (L(j, k) D_k) for ke <= j <= i < nf:
+// the trailing triangle's update by one panel, in register tiles of 8 rows
+// x 4 columns (per pivot one 8-wide load of L and 4 broadcasts feed 32
+// multiply-adds). Tiles on the diagonal also write above it; those entries
+// of a front are never read.
+void trailing_update(double* F, std::size_t nf, std::size_t kb, std::size_t ke, const double* D) {
+    const std::size_t nbk = ke - kb, t = nf - ke, tp = (t + 7) & ~std::size_t(7);
+    std::vector<double> LT(nbk * tp, 0.0), C(tp * nbk, 0.0);  // LT[k][i] = L(ke+i, kb+k), C[j][k] = L(ke+j, kb+k) D_k
+    for (std::size_t k = 0; k < nbk; ++k) {
+        const double* lk = F + (kb + k) * nf + ke;
+        std::memcpy(LT.data() + k * tp, lk, sizeof(double) * t);
+        for (std::size_t j = 0; j < t; ++j) C[j * nbk + k] = lk[j] * D[kb + k];
+    }
+    const std::size_t nj = (t + 3) / 4;
+    const bool par = t * t * nbk > (std::size_t(1) << 21);
+#pragma omp parallel for schedule(dynamic, 2) if (par)
+    for (std::size_t jb = 0; jb < nj; ++jb) {
+        const std::size_t j0 = jb * 4, nc = std::min<std::size_t>(4, t - j0);
+        const double* c0 = C.data() + j0 * nbk;
+        for (std::size_t i0 = j0 & ~std::size_t(7); i0 < t; i0 += 8) {
+            double acc[4][8] = {};
+            for (std::size_t k = 0; k < nbk; ++k) {
+                const double* l = LT.data() + k * tp + i0;
+                for (std::size_t jj = 0; jj < 4; ++jj) {
+                    const double c = c0[jj * nbk + k];
+#pragma omp simd
+                    for (std::size_t ii = 0; ii < 8; ++ii) acc[jj][ii] += l[ii] * c;
+                }
+            }
+            const std::size_t nr = std::min<std::size_t>(8, t - i0);
+            for (std::size_t jj = 0; jj < nc; ++jj) {
+                double* f = F + (ke + j0 + jj) * nf + ke + i0;
+                for (std::size_t ii = 0; ii < nr; ++ii) f[ii] -= acc[jj][ii];
+            }
+        }
+    }
+}
+
 // front F (nf x nf, column-major, lower used): factor the first w columns
 // with the pivot clamp, leave L there, and return the Schur complement
 // U = F22 - L21 D L21^T (r x r lower, column-major) in `upd`. Blocked
 // right-looking: a panel of up to 32 pivot columns is factorised against
-// itself, then the whole trailing lower triangle takes its rank-32 update,
-// each column in row chunks held across the panel's pivots.
+// itself, then the whole trailing lower triangle takes its rank-32 update
+// (trailing_update).
 void factor_front(double* F, std::size_t nf, std::size_t w, double tol, double* Dout, bool& singular,
                   std::vector<double>& upd) {
-    constexpr std::size_t kNb = 32, kChunk = 64;
+    constexpr std::size_t kNb = 32;
     for (std::size_t kb = 0; kb < w; kb += kNb) {
         const std::size_t ke = std::min(w, kb + kNb), nbk = ke - kb;
         for (std::size_t k = kb; k < ke; ++k) {
@@ -380,32 +418,7 @@ void factor_front(double* F, std::size_t nf, std::size_t w, double tol, double* 
                 for (std::size_t i = j; i < nf; ++i) fj[i] -= fk[i] * ljd;
             }
         }
-        if (ke >= nf) continue;
-        const std::size_t t = nf - ke;
-        const bool par = t * t * nbk > (std::size_t(1) << 21);
-#pragma omp parallel for schedule(dynamic, 4) if (par)
-        for (std::size_t j = ke; j < nf; ++j) {
-            double c[kNb];
-            bool any = false;
-            for (std::size_t k = 0; k < nbk; ++k) {
-                c[k] = F[(kb + k) * nf + j] * Dout[kb + k];
-                any = any || c[k] != 0.0;
-            }
-            if (!any) continue;
-            double* fj = F + j * nf;
-            for (std::size_t i0 = j; i0 < nf; i0 += kChunk) {
-                const std::size_t len = std::min(kChunk, nf - i0);
-                double acc[kChunk];
-                for (std::size_t i = 0; i < len; ++i) acc[i] = fj[i0 + i];
-                for (std::size_t k = 0; k < nbk; ++k) {
-                    const double ck = c[k];
-                    const double* lk = F + (kb + k) * nf + i0;
-#pragma omp simd
-                    for (std::size_t i = 0; i < len; ++i) acc[i] -= lk[i] * ck;
-                }
-                for (std::size_t i = 0; i < len; ++i) fj[i0 + i] = acc[i];
-            }
-        }
+        if (ke < nf) trailing_update(F, nf, kb, ke, Dout);
     }
     const std::size_t r = nf - w;
     upd.assign(r * r, 0.0);
