@@ -473,7 +473,10 @@ bool SparseLDLT::factorize(const double* val, double tol) {
     auto process = [&](int s, std::vector<int>& pos, std::vector<double>& F, bool& sing) {
         const std::size_t r0 = srows_off_[s], nf = srows_off_[s + 1] - r0;
         const std::size_t w = static_cast<std::size_t>(snode_start_[s + 1] - snode_start_[s]);
-        F.assign(nf * nf, 0.0);
+        // only a front's lower triangle is ever read: the buffer is reused and
+        // just that part cleared
+        if (F.size() < nf * nf) F.resize(nf * nf);
+        for (std::size_t j = 0; j < nf; ++j) std::memset(F.data() + j * nf + j, 0, sizeof(double) * (nf - j));
         for (std::size_t a = amap_off_[s]; a < amap_off_[s + 1]; ++a) F[amap_[a].second] += val[amap_[a].first];
         for (std::size_t t = 0; t < nf; ++t) pos[srows_[r0 + t]] = static_cast<int>(t);
         // extend-add the children's update matrices
