@@ -10,8 +10,9 @@ scaled the way HyperNova's IPM scales it):
 The metric is algorithmic GB/s of the whole step (bytes each kernel must
 move by the formulas printed in `kernels`), measured with CUDA events on the
 launching stream. `e2e` repeats the step through the same C ABI with the
-inputs copied in from pinned host memory and the results copied back inside
-the timed region. The step writes the 11.6 GB normal matrix, so every step
+inputs copied in from pinned host memory and the results -- y, t, the
+scalars and the 7.8 GB of normal-matrix values the host factorisation reads
+-- copied back inside the timed region. The step writes the 11.6 GB normal matrix, so every step
 streams far more than the 126 MB L2 (no separate flush needed).
 
 --impl reference times the reference's own CPU code for the same step
@@ -221,13 +222,17 @@ def run_ours(args, rank, world, local):
     hy = torch.empty(m, dtype=f64).pin_memory()
     ht = torch.empty(n, dtype=f64).pin_memory()
     hs = torch.empty(8, dtype=f64).pin_memory()
+    # the normal matrix's values go back to the host every step: the IPM's
+    # host factorisation reads them each iteration (hn_ipm.cpp, as the
+    # reference's build_normal_equations leaves N on the host)
+    hN = torch.empty(P.nnz, dtype=f64).pin_memory()
     lib = hn.load()
 
     def e2e_step():
         for dst, src, nb_ in ((x, hx, 8 * n), (z, hz, 8 * n), (lam, hl, 8 * m), (D, hD, 8 * n)):
             hn.check(lib.hn_memcpy_h2d(dst.data_ptr(), src.data_ptr(), nb_, sp))
         step()
-        for dst, src, nb_ in ((hy, y, 8 * m), (ht, t, 8 * n), (hs, scal, 64)):
+        for dst, src, nb_ in ((hy, y, 8 * m), (ht, t, 8 * n), (hs, scal, 64), (hN, nval, 8 * P.nnz)):
             hn.check(lib.hn_memcpy_d2h(dst.data_ptr(), src.data_ptr(), nb_, sp))
 
     for _ in range(max(1, args.warmup)):
@@ -241,7 +246,11 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
     h2d = 8 * (3 * n + m)
-    d2h = 8 * (m + n) + 64
+    d2h = 8 * (m + n) + 64 + 8 * P.nnz
+
+    # SpMV on the spec-literal large LP (Zipf(1.5) columns on [1, 2000], no
+    # rescaling: ~17M nonzeros), alone, L2 flushed between launches
+    lit = spmv_literal(args, dev, stream) if not args.no_literal else None
 
     # the batched IPM runs on every rank (sharded when there are several)
     batch_result = None if args.no_batch else batched_ipm(args.batch_k, args.batch_sample, rank, world)
@@ -269,6 +278,8 @@ def run_ours(args, rank, world, local):
                          "traffic_source": traffic_src, "bytes_per_launch": nb[dom]},
             "clocks": clk,
         }
+        if lit is not None:
+            result["kernels"].update(lit)
         if not args.no_ipm:
             result["plain_ipm"] = plain_ipm()
         if batch_result is not None:
@@ -276,6 +287,43 @@ def run_ours(args, rank, world, local):
         if not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(lp, vec, threads=os.cpu_count() or 1, reps=1)
     return result
+
+
+def spmv_literal(args, dev, stream):
+    """y = A x and y = A^T x on the spec-literal LP (m 200k, n 500k, Zipf(1.5)
+    column counts on [1, 2000] without rescaling, ~17M nonzeros, seed 1000),
+    autotuned path, CUDA events around each launch, a 256 MB write between
+    launches (cold L2), mean over the timed launches."""
+    import torch
+
+    import hnb200 as hn
+    import lpgen
+
+    lp = lpgen.lp_zipf(seed=1000, target_nnz=None)
+    m, n = lp["m"], lp["n"]
+    A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
+    sp = stream.cuda_stream
+    flush = torch.empty(32 * 1024 * 1024, dtype=torch.float64, device=dev)
+    out = {}
+    for name, trans in (("spmv_A_c1_literal", 0), ("spmv_At_c1_literal", 1)):
+        xin = torch.as_tensor(lp["y0"] if trans else lp["x0"], device=dev)
+        yout = torch.empty(n if trans else m, dtype=torch.float64, device=dev)
+        nbytes = (12 * A.nnz_t + 4 * (n + 1) + 8 * m + 8 * n) if trans else (12 * A.nnz + 4 * (m + 1) + 8 * n + 8 * m)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for _ in range(args.warmup):
+            flush.zero_()
+            A.spmv(xin, yout, trans=trans, stream=sp)
+        for i in range(args.steps):
+            flush.zero_()
+            evs[i][0].record(stream)
+            A.spmv(xin, yout, trans=trans, stream=sp)
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+        out[name] = {"ms": round(ms, 4), "bytes": nbytes, "GB/s": round(nbytes / (ms * 1e-3) / 1e9, 1),
+                     "nnz": A.nnz if not trans else A.nnz_t, "path": list(A.spmv_kind(trans))}
+    A.close()
+    return out
 
 
 def plain_ipm():
@@ -291,6 +339,7 @@ def plain_ipm():
     if os.path.exists(gp):
         ref = json.load(open(gp))["lp_uniform_2000_5000_8_seed0"]
     out = {"lp": "m=2000 n=5000 8 nnz/col seed 0", "status": r["status_name"], "iterations": r["iterations"],
+           "reference_rule_iterations": r["reference_iterations"], "relative_kkt": r["kkt"],
            "objective": r["objective"], "ms": round(r["time_ms"], 1), "solves_per_s": round(1e3 / r["time_ms"], 3),
            "factor_ms": round(r["factor_ms"], 1), "device_ms": round(r["device_ms"], 1),
            "host_threads": os.cpu_count()}
@@ -323,7 +372,12 @@ def batched_ipm(K: int, sample_per_stratum: int = 4, rank: int = 0, world: int =
         torch.distributed.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r = shard.solve_sharded(lps, hn.lp_solve_batch, rank, world)
+        def solve_part(part, **kw):
+            res = hn.lp_solve_batch(part, **kw)
+            res["kkt0"] = res["kkt"][:, 0]
+            return res
+
+        r = shard.solve_sharded(lps, solve_part, rank, world, keys=("status", "objective", "iterations", "kkt0"))
         torch.cuda.synchronize()
         wall_t = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(wall_t, op=torch.distributed.ReduceOp.MAX)
@@ -335,6 +389,7 @@ def batched_ipm(K: int, sample_per_stratum: int = 4, rank: int = 0, world: int =
                 "ranks": world, "sharding": "LPT greedy on m^3/3 + nnz, one gather of the results",
                 "instances_per_rank": [int(p.size) for p in r["parts"]], "batched_s": round(wall, 3),
                 "batched_solves_per_s": round(K / wall, 1), "optimal": int((st == 1).sum()),
+                "kkt_le_1e-8": int(((st == 1) & (r["kkt0"] <= 1e-8)).sum()), "kkt_max": float(np.nanmax(r["kkt0"])),
                 "iterations_mean": round(float(np.mean(r["iterations"])), 2)}
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -342,12 +397,14 @@ def batched_ipm(K: int, sample_per_stratum: int = 4, rank: int = 0, world: int =
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     st = r["status"]
+    kkt = r["kkt"][:, 0]
+    at_kkt = (st == 1) & (kkt <= 1e-8)
     # dense LDL^T work: one factorisation of m_i^3 / 3 multiply-adds per iteration of each instance
     factor_flops = float(np.sum(r["iterations"].astype(np.float64) * sizes.astype(np.float64) ** 3 * 2.0 / 3.0))
     # stratified plain sample
     edges = np.exp(np.linspace(np.log(50), np.log(2000) + 1e-9, 9))
     rng = np.random.default_rng(7)
-    est, matched, sampled, plain_iters = 0.0, 0, 0, []
+    est, matched, sampled, plain_iters, plain_kkt_ok = 0.0, 0, 0, [], 0
     for a, b in zip(edges[:-1], edges[1:]):
         idx = np.nonzero((sizes >= a) & (sizes < b))[0]
         if idx.size == 0 or sample_per_stratum == 0:
@@ -364,18 +421,23 @@ def batched_ipm(K: int, sample_per_stratum: int = 4, rank: int = 0, world: int =
             sampled += 1
             rel = abs(p["objective"] - r["objective"][i]) / (1.0 + abs(p["objective"]))
             matched += int(p["status"] == st[i] == 1 and rel <= 1e-8)
+            plain_kkt_ok += int(p["status"] == 1 and p["kkt"] <= 1e-8)
         est += float(np.mean(times)) * idx.size
     return {"workload": f"{K} LPs, m log-uniform [50,2000], n=2.5m, 6 nnz/col (seeds 20000+i)",
             "rows": int(sizes.sum()), "batched_s": round(wall, 3), "batched_solves_per_s": round(K / wall, 1),
-            "optimal": int((st == 1).sum()), "iterations_max": int(r["stats"]["iterations"]),
+            "optimal": int((st == 1).sum()), "kkt_le_1e-8": int(at_kkt.sum()),
+            "batched_solves_per_s_at_1e-8_kkt": round(int(at_kkt.sum()) / wall, 1),
+            "kkt_max": float(np.nanmax(kkt)), "kkt_median": float(np.nanmedian(kkt)),
+            "iterations_max": int(r["stats"]["iterations"]),
             "iterations_mean": round(float(r["iterations"].mean()), 2),
+            "reference_rule_iterations_mean": round(float(r["reference_iterations"].mean()), 2),
             "factor_ms": round(r["stats"]["factor_ms"], 1), "solve_ms": round(r["stats"]["solve_ms"], 1),
             "factor_fp64_tflops": round(factor_flops / (r["stats"]["factor_ms"] * 1e-3) / 1e12, 2),
             "plain_gpu_s_extrapolated": round(est, 2) if sampled else None,
             "plain_gpu_solves_per_s_extrapolated": round(K / est, 2) if sampled else None,
             "speedup_vs_plain_gpu": round(est / wall, 2) if sampled else None,
             "plain_sample": {"instances": sampled, "per_stratum": sample_per_stratum,
-                             "matching_status_and_objective_1e-8": matched,
+                             "matching_status_and_objective_1e-8": matched, "kkt_le_1e-8": plain_kkt_ok,
                              "iterations_mean": round(float(np.mean(plain_iters)), 2) if sampled else None}}
 
 
@@ -729,16 +791,25 @@ def run_only(args, local):
         return mps_io()
     if args.only == "gnn":
         return gnn_warm(args.gnn_train, args.gnn_eval, args.gnn_mlo, args.gnn_mhi, args.gnn_epochs, args.gnn_chunk)
-    lp, vec = make_inputs(1000, args.scale)
+    if args.literal:
+        import lpgen
+
+        lp = lpgen.lp_zipf(seed=1000, target_nnz=None)
+        vec = {"x": lp["x0"], "lam": lp["y0"], "D": np.ones(lp["n"])}
+    else:
+        lp, vec = make_inputs(1000, args.scale)
     m, n = lp["m"], lp["n"]
     A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
+    if args.spmv_kind >= 0:
+        A.set_spmv_kind(args.spmv_kind, args.spmv_t, trans=0)
+        A.set_spmv_kind(args.spmv_kind, args.spmv_t, trans=1)
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
     flush = torch.empty(32 * 1024 * 1024, dtype=torch.float64, device=dev)
     if args.only == "price":
         return pricing(A, m, n, args.steps, args.warmup, flush)
     if args.only == "ada":
-        P = hn.Pattern(A)
+        P = hn.Pattern(A, layout=None if args.ada_layout < 0 else args.ada_layout)
         D = torch.as_tensor(vec["D"], device=dev)
         nval = torch.empty(P.nnz, dtype=torch.float64, device=dev)
         nbytes = step_bytes(m, n, A.nnz, A.nnz_t, P.nnz)["ada_numeric"]
@@ -761,7 +832,13 @@ def run_only(args, local):
     torch.cuda.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
     hbm, how = peaks()
-    return {"only": args.only, "scale": args.scale, "m": m, "n": n, "nnz": A.nnz, "ms": round(ms, 4), "bytes": nbytes, "GB/s": round(nbytes / (ms * 1e-3) / 1e9, 1),
+    extra = {}
+    if args.only == "ada":
+        extra["layout"] = P.mode()[0]
+    else:
+        extra["path"] = list(A.spmv_kind(1 if args.only == "spmv_t" else 0))
+    return {"only": args.only, "scale": args.scale, "literal": args.literal, **extra, "m": m, "n": n, "nnz": A.nnz,
+            "ms": round(ms, 4), "bytes": nbytes, "GB/s": round(nbytes / (ms * 1e-3) / 1e9, 1),
             "frac_of_" + how + "_hbm": round(nbytes / (ms * 1e-3) / 1e9 / hbm, 4)}
 
 
@@ -823,6 +900,12 @@ def main():
     ap.add_argument("--no-ipm", action="store_true", help="skip the plain GPU IPM solve on the m=2000 LP")
     ap.add_argument("--scale", type=int, default=1, help="--only modes: shrink the LP by this factor (profiling)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-IPM key")
+    ap.add_argument("--no-literal", action="store_true", help="skip the spec-literal (17M nonzeros) SpMV lines")
+    ap.add_argument("--literal", action="store_true", help="--only spmv / spmv_t: the spec-literal LP")
+    ap.add_argument("--spmv-kind", type=int, default=-1, help="--only spmv / spmv_t: pin a path (0 merge, 1 binned)")
+    ap.add_argument("--spmv-t", type=int, default=8, help="--only spmv / spmv_t: nonzeros per lane of the binned path")
+    ap.add_argument("--ada-layout", type=int, default=-1,
+                    help="--only ada: numeric layout (0 gather, 1 row, 2 relative map; -1 the library's choice)")
     ap.add_argument("--batch-k", type=int, default=4096, help="instances in the batched-IPM key")
     ap.add_argument("--batch-sample", type=int, default=4, help="plain GPU IPM solves per size stratum")
     ap.add_argument("--bb-k", type=int, default=2048, help="--only bb: node relaxations")

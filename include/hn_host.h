@@ -46,6 +46,14 @@ typedef struct hn_ipm_options {
      * SparseCholesky seat): 0 auto = dense LDL^T up to 12,000 rows, sparse
      * LDL^T (AMD + supernodal, hn_sparse_ldlt_solve) above; 1 dense; 2 sparse */
     int factorization;
+    /* Tightening past the reference's stop (no reference counterpart): once
+     * the reference's absolute tests on the scaled form hold (the status is
+     * theirs), keep iterating until the relative KKT residual of the unscaled
+     * LP (hn_ipm_kkt in hn_sm100.h) is <= kkt_tol or kkt_extra_iterations more
+     * iterations have run, and return the better of the two iterates.
+     * kkt_tol <= 0: the reference's rule alone. Defaults 1e-8, 10. */
+    double kkt_tol;
+    int kkt_extra_iterations;
 } hn_ipm_options;
 
 /* InteriorPointResult (core/lp/interior_point.hpp:29-38) plus phase times;
@@ -62,6 +70,11 @@ typedef struct hn_ipm_result {
     int warm_start_used;  /* 1 when the warm start was taken */
     double kkt_default;   /* relative KKT residual of the default start */
     double kkt_warm;      /* ... of the shifted warm start (0 if none) */
+    /* relative KKT residual of the returned iterate on the unscaled LP: the
+     * max of its primal, dual and duality-gap parts (hn_ipm_kkt) */
+    double kkt, kkt_primal, kkt_dual, kkt_gap;
+    /* iteration at which the reference's stopping rule first held (-1: never) */
+    int64_t reference_iterations;
 } hn_ipm_result;
 
 void hn_ipm_default_options(hn_ipm_options* opt);
@@ -83,7 +96,8 @@ const char* hn_host_last_error(void);
  * entries row_off[i]+i .. row_off[i+1]+i+1 of row_ptr (local, starting at 0).
  * Per-instance outputs: status (model::ProblemStatus), objective, iterations;
  * optional (NULL = not wanted): x_out / s_out packed by col_off, y_out by
- * row_off, warm_used (K). */
+ * row_off, warm_used (K), kkt_out (K x 4: relative KKT residual, primal, dual,
+ * gap parts as hn_ipm_result's) and reference_iterations (K). */
 typedef struct hn_batch_stats {
     int64_t rows, cols, nnz, nnz_normal;
     int64_t iterations;
@@ -94,7 +108,7 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
                       const double* b, const int* sense, const double* lb, const double* ub, const int* maximize,
                       const double* obj_offset, const hn_ipm_options* opt, int* status, double* objective,
                       int64_t* iterations, double* x_out, hn_batch_stats* stats, int* warm_used, double* y_out,
-                      double* s_out);
+                      double* s_out, double* kkt_out, int64_t* reference_iterations);
 
 /* ---- MPS reader (MPSParser, core/model/mps_parser.hpp:18-78) ----
  * Reads MPS text with the reference's results: free/fixed layout (format -1

@@ -180,15 +180,23 @@ int hn_nrm2(int64_t n, const double* v_dev, double* result_dev, void* stream);
  * (the span from its smallest to its largest k; block-diagonal batches are
  * limited by their largest block only), and nnz(N) < 2^31. */
 int hn_ada_symbolic(const hn_csr* A, hn_pattern** out);
-/* The numeric phase has two layouts with bit-identical results. Gather
- * mode (the default) keeps an 8-byte source pair per slot of N and is the
- * faster one. Row mode, asked for with HN_ADA_COMPACT and used when every row
- * of N has <= 65,534 slots and every row of A <= 256 entries, keeps a 2-byte
- * slot offset per term (about a quarter of the memory) and assembles each
- * row of N in shared-memory windows. */
+/* The numeric phase has three layouts with bit-identical results.
+ *  - Gather mode keeps an 8-byte source pair (A^T entry, A entry) per slot of
+ *    N; one thread per slot, in slot order.
+ *  - Relative map keeps 4 bytes per slot: the single term's entry within its
+ *    row of A and within its row of A^T (or the slot's index among its row's
+ *    multi-term slots); one warp per row of N, longest rows first. Chosen by
+ *    default when rows of N average >= 256 slots and the offsets fit 32 bits
+ *    (longest row of A x longest row of A^T < 2^31); HN_ADA_RELATIVE asks for
+ *    it whenever the offsets fit, HN_ADA_GATHER8 asks for gather mode.
+ *  - Row mode, asked for with HN_ADA_COMPACT and used when every row of N has
+ *    <= 65,534 slots and every row of A <= 256 entries, keeps a 2-byte slot
+ *    offset per term and assembles each row of N in shared-memory windows. */
 #define HN_ADA_COMPACT 1u
+#define HN_ADA_GATHER8 2u
+#define HN_ADA_RELATIVE 4u
 int hn_ada_symbolic_ex(const hn_csr* A, unsigned flags, hn_pattern** out);
-/* row_mode: 1 for row mode, 0 for gather mode; max_row: longest row of N. */
+/* row_mode: 0 gather mode, 1 row mode, 2 relative map; max_row: longest row of N. */
 int hn_pattern_mode(const hn_pattern* P, int* row_mode, int64_t* max_row);
 int hn_pattern_info(const hn_pattern* P, int64_t* m, int64_t* nnz);
 /* Host copy of the pattern: rp m+1, ci nnz (reference layout). */
@@ -250,6 +258,23 @@ int hn_ipm_corrector(const hn_csr* M, const double* x_dev, const double* dx_dev,
 int hn_ipm_update(int64_t n, int64_t m, double* x_dev, const double* dx_dev, double* z_dev,
                   const double* dz_dev, double* lam_dev, const double* dlam_dev, double* scal_dev,
                   void* stream);
+/* Relative KKT residual of an iterate on the LP with the standard form's row
+ * and column scaling undone. No reference counterpart: the reference stops on
+ * absolute tests of the scaled form (interior_point.cpp:525-530) and never
+ * measures this; it is the accuracy measure of the solves/s metric.
+ *   P = max_i |rp_i| ru_i / (1 + max_i |b_i| ru_i)
+ *   D = max_j |rd_j| cu_j / (1 + max_j |c_j| cu_j)
+ *   G = |c^T x - b^T lam| / (1 + |c^T x + offset|)
+ * kkt_dev[0..3] = max(P, D, G), P, D, G (a non-finite residual entry makes
+ * its part infinite). rp = M x - b, rd = M^T lam + z - c as hn_ipm_residuals
+ * leaves them for the same (x, lam, z); ru_i = 1 / |scale of row i|, cu_j =
+ * 1 / (scale of column j), offset = the objective's constant. For an LP given
+ * as min c^T x, A x = b, x >= 0 this is max(||Ax-b||/(1+||b||),
+ * ||A^T y + s - c||/(1+||c||), |c^T x - b^T y|/(1+|c^T x|)) (inf-norms) of the
+ * original LP at x, y = row-scaled lam, s = column-unscaled z. */
+int hn_ipm_kkt(int64_t n, int64_t m, const double* x_dev, const double* lam_dev, const double* b_dev,
+               const double* c_dev, const double* rp_dev, const double* rd_dev, const double* ru_dev,
+               const double* cu_dev, double offset, double* kkt_dev, void* stream);
 /* *result_dev = min(1, 0.99 * min_{d_i<0} -v_i/d_i) (max_step, :134-142). */
 int hn_max_step(int64_t n, const double* v_dev, const double* d_dev, double* result_dev, void* stream);
 
@@ -278,6 +303,30 @@ int hn_batch_residuals(hn_batch* B, const hn_csr* M, const double* x_dev, const 
                        const double* z_dev, const double* b_dev, const double* c_dev, double* mx_dev, double* rp_dev,
                        double* rd_dev, double* D_dev, double* Drd_dev, double* scal_dev, int32_t* status_dev,
                        int32_t* iters_dev, int iter, double tol, double ctol, void* stream);
+/* Relative KKT residual per instance and tightening past the reference's
+ * stop (no reference counterpart). With ru_dev / cu_dev (per packed row /
+ * column, as hn_ipm_kkt) and offset_dev (K) set, every hn_batch_residuals
+ * call measures each instance's residual as hn_ipm_kkt does. With
+ * kkt_tol > 0, an instance that meets the reference's rule has that iterate
+ * saved and keeps iterating until its residual is <= kkt_tol or
+ * extra_iterations more iterations have run; hn_batch_finish then puts the
+ * saved iterate back where the later one is worse or failed. kkt_tol <= 0:
+ * the reference's rule alone (the residual is still measured when ru_dev is
+ * given). The arrays are caller-owned and must stay valid while the batch
+ * iterates. Resets the per-instance records. */
+int hn_batch_set_kkt(hn_batch* B, const double* ru_dev, const double* cu_dev, const double* offset_dev,
+                     double kkt_tol, int extra_iterations);
+/* kkt_host: K x 4 (as hn_ipm_kkt's kkt_dev) at the last hn_batch_residuals
+ * call, or after hn_batch_finish the residual of the returned iterate;
+ * ref_iter_host: K, the iteration at which the reference's rule first held
+ * (-1: never). Either may be NULL. Synchronises the device. */
+int hn_batch_kkt(const hn_batch* B, double* kkt_host, int32_t* ref_iter_host);
+/* Call after the last hn_batch_residuals: every instance that met the
+ * reference's rule becomes status 1; where it then failed (status 7), or its
+ * residual is larger than when the rule first held, it gets that iterate back
+ * (x, z, lam), iters = that iteration and that residual. */
+int hn_batch_finish(hn_batch* B, double* x_dev, double* z_dev, double* lam_dev, int32_t* status_dev,
+                    int32_t* iters_dev, void* stream);
 /* N = A D A^T + dyn_reg_i I per instance (:144-200), then the dense LDL^T of
  * every iterating instance. nval_dev: nnz(P) doubles. */
 int hn_batch_factor(hn_batch* B, const double* D_dev, double reg, double singular_tol, double* nval_dev,
@@ -367,6 +416,15 @@ int hn_gnn_linear(int64_t M, int K1, int K2, const float* X1_dev, const float* X
 int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1_dev, const float* X2_dev, const void* Wt_bf16_dev,
                        const float* bias_dev, int relu, float* Y_dev, void* stream);
 int hn_gnn_check(void* stream);
+/* Test hook of the bounded waits above (no reference counterpart): the
+ * tcgen05 layer's pipeline waits (bulk copies in, MMA done) give up after
+ * `polls` non-blocking mbarrier polls instead of 2^24 blocking ones (0
+ * restores the default). A call with a small limit gives up while its own
+ * copies are in flight; the CTA then
+ * records the timeout, settles those copies and its MMA with the full bound,
+ * frees TMEM and returns, and hn_gnn_check reports the error. Process-wide;
+ * for tests only. */
+int hn_gnn_set_wait_limit(uint32_t polls);
 /* Backward of hn_gnn_linear with N = 64: G = dY * relu'(Y); dX (M x K, may be
  * NULL; K = 64 or 128) = G W^T; dW (K x 64) = [X1 | X2]^T G; db (64) = sum of
  * G's rows. scratch: >= ceil(M / 64) * (64 K + 64) floats. Deterministic. */

@@ -160,7 +160,8 @@ __global__ void __launch_bounds__(kT) ada_fill_kernel(
     const int32_t* __restrict__ wcount, const int64_t* __restrict__ rpN, const int64_t* __restrict__ msrow,
     const int64_t* __restrict__ mqrow, int32_t* __restrict__ ciN, int64_t* __restrict__ diag_pos,
     int64_t* __restrict__ mpos, int32_t* mcnt, int32_t* __restrict__ mbeg, uint2* __restrict__ gmap,
-    uint2* __restrict__ mlist, const int64_t* __restrict__ tq, uint16_t* __restrict__ smap) {
+    uint2* __restrict__ mlist, const int64_t* __restrict__ tq, uint16_t* __restrict__ smap,
+    uint32_t* __restrict__ rmap, int qbits) {
     extern __shared__ uint32_t smem[];
     uint32_t* b1 = smem;
     uint32_t* b2 = smem + Wmax;
@@ -205,6 +206,7 @@ __global__ void __launch_bounds__(kT) ada_fill_kernel(
                     mpos[ms0 + o2] = pos | (k == i ? kDiagFlag : 0);
                     mcnt[ms0 + o2] = 0;
                     if (gmap) gmap[pos] = make_uint2(kMulti | static_cast<uint32_t>(ms0 + o2), 0u);
+                    if (rmap) rmap[pos] = kMulti | static_cast<uint32_t>(o2);
                     ++o2;
                 }
                 ++o1;
@@ -259,6 +261,9 @@ __global__ void __launch_bounds__(kT) ada_fill_kernel(
                     mlist[mbeg[ms] + ord] = pe;
                 } else if (gmap) {
                     gmap[row0 + rank_of(b1, pre1, k, wb)] = pe;
+                } else if (rmap) {
+                    rmap[row0 + rank_of(b1, pre1, k, wb)] =
+                        (static_cast<uint32_t>(e - rp[i]) << qbits) | static_cast<uint32_t>(p - cs);
                 }
                 if (smap) smap[tloc + (p - cs)] = multi ? kSlotMulti : static_cast<uint16_t>(rank_of(b1, pre1, k, wb));
             }
@@ -333,6 +338,88 @@ __global__ void __launch_bounds__(kT, 4) ada_slot_kernel(int64_t nnz, const uint
 #pragma unroll
         for (int u = 0; u < kSlotsPerThread; ++u) g[u] = gn[u];
     }
+}
+
+// Relative map: one warp per row of N at a time (rows handed out longest
+// first), kRmapU slots per lane per trip, the next trip's map words loaded
+// before this trip's gathers. A single-term slot's word gives its A entry
+// within row i (e = rp_A[i] + high bits) and its A^T entry within row j of A^T
+// (ecs[e] + low bits); (A value x A^T value) x d is the slot kernel's
+// arithmetic, so the layouts give the same bits. The row's A entries are
+// read through L1 (a row of A is a few cache lines, reused by every slot of
+// the row); the A^T values come from L2; the map streams from HBM once.
+constexpr int kRmapU = 4;
+__global__ void __launch_bounds__(kT, 4) ada_rmap_kernel(int m, const int32_t* __restrict__ order,
+                                                         unsigned* __restrict__ row_next,
+                                                         const int32_t* __restrict__ rpA,
+                                                         const double2* __restrict__ vd,
+                                                         const int32_t* __restrict__ ecs,
+                                                         const double* __restrict__ valT,
+                                                         const int64_t* __restrict__ rpN,
+                                                         const int64_t* __restrict__ msrow,
+                                                         const uint32_t* __restrict__ rmap, int qbits,
+                                                         const double* __restrict__ mval, double* __restrict__ nval) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t qmask = (1u << qbits) - 1u;
+    constexpr int64_t kStep = 32 * kRmapU;
+    for (;;) {
+        unsigned idx = 0;
+        if (lane == 0) idx = atomicAdd(row_next, 1u);
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (idx >= static_cast<unsigned>(m)) return;
+        const int i = __ldg(order + idx);
+        const int64_t r0 = __ldg(rpN + i), r1 = __ldg(rpN + i + 1);
+        const int e0 = __ldg(rpA + i);
+        const int64_t ms0 = __ldg(msrow + i);
+        uint32_t g[kRmapU];
+#pragma unroll
+        for (int u = 0; u < kRmapU; ++u) {
+            const int64_t t = r0 + lane + u * 32;
+            g[u] = t < r1 ? __ldcs(rmap + t) : kMulti;
+        }
+        for (int64_t t0 = r0 + lane; t0 < r1; t0 += kStep) {
+            uint32_t gn[kRmapU];
+#pragma unroll
+            for (int u = 0; u < kRmapU; ++u) {
+                const int64_t t = t0 + kStep + u * 32;
+                gn[u] = t < r1 ? __ldcs(rmap + t) : kMulti;
+            }
+            double2 q[kRmapU];
+            int32_t cs[kRmapU];
+#pragma unroll
+            for (int u = 0; u < kRmapU; ++u) {
+                const int e = (g[u] & kMulti) ? 0 : e0 + static_cast<int>(g[u] >> qbits);
+                q[u] = __ldg(vd + e);
+                cs[u] = __ldg(ecs + e);
+            }
+            double b[kRmapU];
+#pragma unroll
+            for (int u = 0; u < kRmapU; ++u) {
+                const int64_t t = t0 + u * 32;
+                if (g[u] & kMulti)
+                    b[u] = t < r1 ? __ldcs(mval + ms0 + (g[u] & ~kMulti)) : 0.0;
+                else
+                    b[u] = __ldg(valT + cs[u] + static_cast<int>(g[u] & qmask));
+            }
+#pragma unroll
+            for (int u = 0; u < kRmapU; ++u) {
+                const int64_t t = t0 + u * 32;
+                if (t >= r1) continue;
+                const double v = (g[u] & kMulti) ? b[u]
+                                 : (q[u].y <= 0.0) ? 0.0  // columns with D_j <= 0 skipped
+                                                   : (q[u].x * b[u]) * q[u].y;
+                __stcs(nval + t, v);
+            }
+#pragma unroll
+            for (int u = 0; u < kRmapU; ++u) g[u] = gn[u];
+        }
+    }
+}
+
+__global__ void ada_ecs_kernel(int64_t nnz, const int32_t* __restrict__ ci, const int32_t* __restrict__ rpT,
+                               int32_t* __restrict__ ecs) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x)
+        ecs[e] = rpT[ci[e]];
 }
 
 // The first kBatch terms of a slot are gathered together; longer lists
@@ -471,7 +558,8 @@ void free_pattern(hn_pattern* P) {
     if (!P) return;
     for (void* p : {(void*)P->rp, (void*)P->ci, (void*)P->diag_pos, (void*)P->maxdiag, (void*)P->gmap,
                     (void*)P->mpos, (void*)P->mbeg, (void*)P->mlist, (void*)P->vd, (void*)P->mval, (void*)P->tq,
-                    (void*)P->smap, (void*)P->msrow})
+                    (void*)P->smap, (void*)P->msrow, (void*)P->rmap, (void*)P->ecs, (void*)P->order,
+                    (void*)P->row_next})
         dfree(p);
     delete P;
 }
@@ -503,6 +591,14 @@ void launch_numeric(const hn_pattern* P, const double* d, double* nval, cudaStre
         launched("ada_row_kernel");
         return;
     }
+    if (P->rmap) {
+        check_cuda(cudaMemsetAsync(P->row_next, 0, sizeof(unsigned), s), "memset row counter");
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P->m + 7) / 8, (int64_t)ctx().sm_count * 4));
+        ada_rmap_kernel<<<grid, kT, 0, s>>>((int)P->m, P->order, P->row_next, A->rp, P->vd, P->ecs, A->valT, P->rp,
+                                            P->msrow, P->rmap, P->qbits, P->mval, nval);
+        launched("ada_rmap_kernel");
+        return;
+    }
     const int64_t per_block = (int64_t)kT * kSlotsPerThread;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P->nnz + per_block - 1) / per_block,
                                                                  (int64_t)ctx().sm_count * 4));
@@ -528,7 +624,7 @@ int hn_ada_symbolic(const hn_csr* A, hn_pattern** out) { return hn_ada_symbolic_
 int hn_pattern_mode(const hn_pattern* P, int* row_mode, int64_t* max_row) {
     return guard("hn_pattern_mode", [&] {
         if (!P) fail(HN_ERR_INVALID_ARG, "null pattern");
-        if (row_mode) *row_mode = P->row_mode ? 1 : 0;
+        if (row_mode) *row_mode = P->row_mode ? 1 : (P->rmap ? 2 : 0);
         if (max_row) *max_row = P->max_row;
     });
 }
@@ -613,12 +709,50 @@ int hn_ada_symbolic_ex(const hn_csr* A, unsigned flags, hn_pattern** out) {
             P->row_mode = (flags & HN_ADA_COMPACT) && m > 0 && maxes[1] <= (unsigned)kRowMaxSlots &&
                           maxes[1] < kSlotMulti &&
                           maxes[2] <= (unsigned)kRowMaxEntries && P->nq < (int64_t(1) << 31);
+            // relative map: offsets within a row of A (maxes[2] entries) and
+            // within a row of A^T must share 31 bits
+            int qbits = 0;
+            bool rel = false;
+            if (!P->row_mode && m > 0 && !(flags & HN_ADA_GATHER8)) {
+                std::vector<int32_t> rpT(A->n + 1);
+                check_cuda(cudaMemcpy(rpT.data(), A->rpT, sizeof(int32_t) * (A->n + 1), cudaMemcpyDeviceToHost),
+                           "D2H rpT");
+                int64_t maxcol = 1;
+                for (int64_t j = 0; j < A->n; ++j) maxcol = std::max<int64_t>(maxcol, rpT[j + 1] - rpT[j]);
+                while ((int64_t(1) << qbits) < maxcol) ++qbits;
+                const bool fits = qbits < 31 && (int64_t)std::max(maxes[2], 1u) <= (int64_t(1) << (31 - qbits));
+                const bool long_rows = P->nnz >= 256 * m;  // a warp per row stays busy
+                rel = fits && ((flags & HN_ADA_RELATIVE) || long_rows);
+            }
             P->ci = dmalloc<int32_t>(P->nnz);
             if (P->row_mode) {
                 P->smap = dmalloc<uint16_t>(d2h_i64(tqa + m, s));
                 P->tq = tqa;
                 P->msrow = nms;
                 tqa = nms = nullptr;  // owned by the pattern now
+            } else if (rel) {
+                P->qbits = qbits;
+                P->rmap = dmalloc<uint32_t>(P->nnz);
+                P->ecs = dmalloc<int32_t>(A->nnz > 0 ? A->nnz : 1);
+                P->order = dmalloc<int32_t>(m);
+                P->row_next = dmalloc<unsigned>(1);
+                P->msrow = nms;
+                nms = nullptr;  // owned by the pattern now
+                if (A->nnz > 0) {
+                    const int ge = (int)std::min<int64_t>((A->nnz + kT - 1) / kT, (int64_t)ctx().sm_count * 16);
+                    ada_ecs_kernel<<<ge, kT, 0, s>>>(A->nnz, A->ci, A->rpT, P->ecs);
+                    launched("ada_ecs_kernel");
+                }
+                // rows of N longest first: the counter hands the long rows out early
+                std::vector<int64_t> rpn(m + 1);
+                check_cuda(cudaMemcpy(rpn.data(), P->rp, sizeof(int64_t) * (m + 1), cudaMemcpyDeviceToHost),
+                           "D2H rp");
+                std::vector<int32_t> ord(m);
+                for (int64_t i = 0; i < m; ++i) ord[i] = static_cast<int32_t>(i);
+                std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) {
+                    return rpn[a + 1] - rpn[a] > rpn[b + 1] - rpn[b];
+                });
+                check_cuda(cudaMemcpy(P->order, ord.data(), sizeof(int32_t) * m, cudaMemcpyHostToDevice), "H2D");
             } else {
                 P->gmap = dmalloc<uint2>(P->nnz);
             }
@@ -631,9 +765,9 @@ int hn_ada_symbolic_ex(const hn_csr* A, unsigned flags, hn_pattern** out) {
             check_cuda(cudaMemcpyAsync(P->mbeg + P->nms, &last, sizeof(last), cudaMemcpyHostToDevice, s), "H2D");
             if (m > 0) {
                 ada_fill_kernel<<<grid, kT, smem_fill, s>>>((int)m, A->rp, A->ci, A->val, A->rpT, A->ciT, (int)W,
-                                                            wbase, wcount, P->rp, P->row_mode ? P->msrow : nms, nmq,
+                                                            wbase, wcount, P->rp, P->msrow ? P->msrow : nms, nmq,
                                                             P->ci, P->diag_pos, P->mpos, mcnt, P->mbeg, P->gmap,
-                                                            P->mlist, P->tq, P->smap);
+                                                            P->mlist, P->tq, P->smap, P->rmap, P->qbits);
                 launched("ada_fill_kernel");
             }
             check_cuda(cudaStreamSynchronize(s), "symbolic sync");

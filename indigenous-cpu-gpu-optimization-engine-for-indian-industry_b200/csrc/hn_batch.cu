@@ -63,6 +63,18 @@ struct hn_batch {
     std::vector<int64_t> chunk_off_h;    // host, nsteps+1 offsets into step_chunks
     int64_t* step_chunks = nullptr;      // device, cumulative chunks per (step, instance)
     double* solve_part = nullptr;        // backward-solve partial dot products, 64 per chunk
+    // relative KKT residual per instance and the tightening past the
+    // reference's stop (hn_batch_set_kkt): ru / cu / offset are caller-owned
+    // unscale factors (null = not measured); kkt and kkt_ref hold K x 4
+    // (residual, primal, dual, gap) at the last residual call and at the
+    // iteration the reference's rule first held (ref_iter, -1 = not yet);
+    // xb / zb / lb keep the iterate of that iteration
+    const double *ru = nullptr, *cu = nullptr, *offset = nullptr;
+    double kkt_tol = 0.0;
+    int kkt_extra = 0;
+    double *kkt = nullptr, *kkt_ref = nullptr;
+    int32_t* ref_iter = nullptr;
+    double *xb = nullptr, *zb = nullptr, *lb = nullptr;
 };
 
 namespace hn {
@@ -76,6 +88,18 @@ constexpr int ST_RUN = 0, ST_OPTIMAL = 1, ST_NUMERICAL = 7;
 __device__ __forceinline__ bool fin(double v) { return isfinite(v); }
 
 // ---- per-instance reductions ----
+// What the residual pass needs for the relative KKT residual and the
+// tightening: see hn_batch_set_kkt.
+struct KktArgs {
+    const double *lam, *b, *c, *ru, *cu, *offset;
+    double *kkt, *kkt_ref, *xb, *zb, *lb;
+    int32_t* ref_iter;
+    double tol;
+    int extra;
+};
+
+__device__ __forceinline__ double fin_or_inf(double t) { return t <= 1.7976931348623157e308 ? t : INFINITY; }
+
 __global__ void __launch_bounds__(kT) batch_prep_kernel(const int64_t* __restrict__ row_off,
                                                         const int64_t* __restrict__ col_off,
                                                         const double* __restrict__ x, const double* __restrict__ z,
@@ -83,11 +107,13 @@ __global__ void __launch_bounds__(kT) batch_prep_kernel(const int64_t* __restric
                                                         double* __restrict__ D, double* __restrict__ Drd,
                                                         double* __restrict__ scal, int32_t* __restrict__ status,
                                                         int32_t* __restrict__ iters, int iter, double tol,
-                                                        double ctol) {
+                                                        double ctol, KktArgs k) {
     __shared__ double sh[32];
+    __shared__ int s_save;
     const int64_t i = blockIdx.x;
     const int64_t c0 = col_off[i], c1 = col_off[i + 1], r0 = row_off[i], r1 = row_off[i + 1];
-    double smu = 0.0, mrd = 0.0, mrp = 0.0;
+    const bool measure = k.ru != nullptr;
+    double smu = 0.0, mrd = 0.0, mrp = 0.0, du = 0.0, cn = 0.0, cx = 0.0, pr = 0.0, bn = 0.0, by = 0.0;
     for (int64_t j = c0 + threadIdx.x; j < c1; j += kT) {
         const double xj = x[j], zj = z[j], r = rd[j];
         smu += xj * zj;
@@ -96,22 +122,111 @@ __global__ void __launch_bounds__(kT) batch_prep_kernel(const int64_t* __restric
         if (!(d >= 0.0) || !fin(d) || d > 1e10) d = 1e10;  // interior_point.cpp:532-539
         D[j] = d;
         Drd[j] = d * r;
+        if (measure) {
+            const double u = k.cu[j], cj = k.c[j];
+            du = fmax(du, fin_or_inf(fabs(r) * u));
+            cn = fmax(cn, fabs(cj) * u);
+            cx += cj * xj;
+        }
     }
-    for (int64_t k = r0 + threadIdx.x; k < r1; k += kT) mrp = fmax(mrp, fabs(rp[k]));
+    for (int64_t q = r0 + threadIdx.x; q < r1; q += kT) {
+        const double r = rp[q];
+        mrp = fmax(mrp, fabs(r));
+        if (measure) {
+            const double u = k.ru[q], bq = k.b[q];
+            pr = fmax(pr, fin_or_inf(fabs(r) * u));
+            bn = fmax(bn, fabs(bq) * u);
+            by += bq * k.lam[q];
+        }
+    }
     smu = block_sum<kT>(smu, sh);
     mrd = block_max<kT>(mrd, sh);
     mrp = block_max<kT>(mrp, sh);
+    if (measure) {
+        du = block_max<kT>(du, sh);
+        cn = block_max<kT>(cn, sh);
+        cx = block_sum<kT>(cx, sh);
+        pr = block_max<kT>(pr, sh);
+        bn = block_max<kT>(bn, sh);
+        by = block_sum<kT>(by, sh);
+    }
     if (threadIdx.x == 0) {
         const double mu = smu / static_cast<double>(c1 - c0);
         double* s = scal + i * HN_IPM_NSCAL;
         s[S_MU] = mu;
         s[S_NRD] = mrd;
         s[S_NRP] = mrp;
-        if (status[i] == ST_RUN && mrp < tol && mrd < tol && mu < ctol) {  // :525-530
-            status[i] = ST_OPTIMAL;
-            iters[i] = iter;
+        double kk = 0.0;
+        if (measure) {
+            const double P = pr / (1.0 + bn), Dl = du / (1.0 + cn),
+                         Gp = fabs(cx - by) / (1.0 + fabs(cx + k.offset[i]));
+            kk = (P != P || Dl != Dl || Gp != Gp) ? nan("") : fmax(P, fmax(Dl, Gp));
+            double* o = k.kkt + 4 * i;
+            o[0] = kk;
+            o[1] = P;
+            o[2] = Dl;
+            o[3] = Gp;
+        }
+        int save = 0;
+        if (status[i] == ST_RUN) {
+            int r = k.ref_iter[i];
+            if (r < 0 && mrp < tol && mrd < tol && mu < ctol) {  // the reference's rule, :525-530
+                r = iter;
+                k.ref_iter[i] = iter;
+                save = measure && k.tol > 0.0;
+                if (measure)
+                    for (int q = 0; q < 4; ++q) k.kkt_ref[4 * i + q] = k.kkt[4 * i + q];
+            }
+            // stop at the reference's rule, or past it once the KKT residual
+            // is within tolerance or the extra iterations are spent
+            if (r >= 0 && (!(measure && k.tol > 0.0) || kk <= k.tol || iter - r >= k.extra)) {
+                status[i] = ST_OPTIMAL;
+                iters[i] = iter;
+            }
+        }
+        s_save = save;
+    }
+    __syncthreads();
+    if (s_save) {  // keep the iterate the reference would return
+        for (int64_t j = c0 + threadIdx.x; j < c1; j += kT) {
+            k.xb[j] = x[j];
+            k.zb[j] = z[j];
+        }
+        for (int64_t q = r0 + threadIdx.x; q < r1; q += kT) k.lb[q] = k.lam[q];
+    }
+}
+
+// After the last residual pass: an instance that met the reference's rule
+// and then failed (status 7), was still iterating, or ended with a larger
+// KKT residual than at that point gets the saved iterate back.
+__global__ void __launch_bounds__(kT) batch_finish_kernel(const int64_t* __restrict__ row_off,
+                                                          const int64_t* __restrict__ col_off, double* __restrict__ x,
+                                                          double* __restrict__ z, double* __restrict__ lam,
+                                                          int32_t* __restrict__ status, int32_t* __restrict__ iters,
+                                                          KktArgs k) {
+    __shared__ int s_restore;
+    const int64_t i = blockIdx.x;
+    const int r = k.ref_iter[i];
+    if (r < 0) return;
+    if (threadIdx.x == 0) {
+        const double now = k.kkt[4 * i], then = k.kkt_ref[4 * i];
+        const int st = status[i];
+        const bool worse = !(now <= then);  // NaN now counts as worse
+        s_restore = (st == ST_NUMERICAL || worse) ? 1 : 0;
+        status[i] = ST_OPTIMAL;
+        if (s_restore) {
+            iters[i] = r;
+            for (int q = 0; q < 4; ++q) k.kkt[4 * i + q] = k.kkt_ref[4 * i + q];
         }
     }
+    __syncthreads();
+    if (!s_restore) return;
+    const int64_t c0 = col_off[i], c1 = col_off[i + 1], r0 = row_off[i], r1 = row_off[i + 1];
+    for (int64_t j = c0 + threadIdx.x; j < c1; j += kT) {
+        x[j] = k.xb[j];
+        z[j] = k.zb[j];
+    }
+    for (int64_t q = r0 + threadIdx.x; q < r1; q += kT) lam[q] = k.lb[q];
 }
 
 __global__ void __launch_bounds__(kT) batch_steps_kernel(const int64_t* __restrict__ row_off,
@@ -756,9 +871,15 @@ void free_batch(hn_batch* B) {
                     (void*)B->dense, (void*)B->dD, (void*)B->refine, (void*)B->nref, (void*)B->nrp,
                     (void*)B->tile_row, (void*)B->tile_nz, (void*)B->carry_row, (void*)B->head_row,
                     (void*)B->carry_val, (void*)B->head_val, (void*)B->r, (void*)B->ax, (void*)B->step_pairs, (void*)B->step_chunks,
-                    (void*)B->solve_part})
+                    (void*)B->solve_part, (void*)B->kkt, (void*)B->kkt_ref, (void*)B->ref_iter, (void*)B->xb,
+                    (void*)B->zb, (void*)B->lb})
         dfree(p);
     delete B;
+}
+
+KktArgs kkt_args(const hn_batch* B, const double* lam, const double* b, const double* c) {
+    return KktArgs{lam,    b,      c,      B->ru,  B->cu,       B->offset, B->kkt,
+                   B->kkt_ref, B->xb, B->zb, B->lb, B->ref_iter, B->kkt_tol, B->kkt_extra};
 }
 
 SpmvMat n_mat(const hn_batch* B, const double* nval) {
@@ -842,6 +963,12 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
             B->r = dmalloc<double>(m);
             B->ax = dmalloc<double>(m);
             B->nrp = dmalloc<int32_t>(m + 1);
+            B->ref_iter = dmalloc<int32_t>(K);
+            B->kkt = dmalloc<double>(4 * K);
+            B->kkt_ref = dmalloc<double>(4 * K);
+            check_cuda(cudaMemsetAsync(B->ref_iter, 0xff, sizeof(int32_t) * K, s), "memset");  // -1
+            check_cuda(cudaMemsetAsync(B->kkt, 0, sizeof(double) * 4 * K, s), "memset");
+            check_cuda(cudaMemsetAsync(B->kkt_ref, 0, sizeof(double) * 4 * K, s), "memset");
             check_cuda(cudaMemcpy(B->row_off, row_off_host, sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice), "H2D");
             check_cuda(cudaMemcpy(B->col_off, col_off_host, sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice), "H2D");
             check_cuda(cudaMemcpy(B->dn_off, dn.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice), "H2D");
@@ -918,8 +1045,55 @@ int hn_batch_residuals(hn_batch* B, const hn_csr* M, const double* x, const doub
         spmv_launch(spmv_mat(M, 0), x, EpiResidual{b, mx, rp}, s);
         spmv_launch(spmv_mat(M, 1), lam, EpiDualResidual{z, c, rd}, s);
         batch_prep_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, B->col_off, x, z, rd, rp, D, Drd, scal, status,
-                                                        iters, iter, tol, ctol);
+                                                        iters, iter, tol, ctol, kkt_args(B, lam, b, c));
         launched("batch_prep_kernel");
+    });
+}
+
+int hn_batch_set_kkt(hn_batch* B, const double* ru, const double* cu, const double* offset, double kkt_tol,
+                     int extra_iterations) {
+    return guard("hn_batch_set_kkt", [&] {
+        require_init();
+        if (!B || (ru == nullptr) != (cu == nullptr) || (ru && !offset) || extra_iterations < 0)
+            fail(HN_ERR_INVALID_ARG, "bad arguments");
+        if (kkt_tol > 0.0 && !ru) fail(HN_ERR_INVALID_ARG, "tightening needs the unscale factors");
+        B->ru = ru;
+        B->cu = cu;
+        B->offset = offset;
+        B->kkt_tol = kkt_tol > 0.0 ? kkt_tol : 0.0;
+        B->kkt_extra = extra_iterations;
+        if (B->kkt_tol > 0.0 && !B->xb) {
+            B->xb = dmalloc<double>(B->n);
+            B->zb = dmalloc<double>(B->n);
+            B->lb = dmalloc<double>(B->m);
+        }
+        check_cuda(cudaMemset(B->ref_iter, 0xff, sizeof(int32_t) * B->K), "memset");
+        check_cuda(cudaMemset(B->kkt, 0, sizeof(double) * 4 * B->K), "memset");
+        check_cuda(cudaMemset(B->kkt_ref, 0, sizeof(double) * 4 * B->K), "memset");
+    });
+}
+
+int hn_batch_kkt(const hn_batch* B, double* kkt_host, int32_t* ref_iter_host) {
+    return guard("hn_batch_kkt", [&] {
+        require_init();
+        if (!B) fail(HN_ERR_INVALID_ARG, "null batch");
+        check_cuda(cudaDeviceSynchronize(), "sync");
+        if (kkt_host)
+            check_cuda(cudaMemcpy(kkt_host, B->kkt, sizeof(double) * 4 * B->K, cudaMemcpyDeviceToHost), "D2H kkt");
+        if (ref_iter_host)
+            check_cuda(cudaMemcpy(ref_iter_host, B->ref_iter, sizeof(int32_t) * B->K, cudaMemcpyDeviceToHost),
+                       "D2H ref_iter");
+    });
+}
+
+int hn_batch_finish(hn_batch* B, double* x, double* z, double* lam, int32_t* status, int32_t* iters, void* stream) {
+    return guard("hn_batch_finish", [&] {
+        require_init();
+        if (!B || !x || !z || !lam || !status || !iters) fail(HN_ERR_INVALID_ARG, "bad arguments");
+        cudaStream_t s = as_stream(stream);
+        batch_finish_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, B->col_off, x, z, lam, status, iters,
+                                                          kkt_args(B, lam, nullptr, nullptr));
+        launched("batch_finish_kernel");
     });
 }
 

@@ -13,6 +13,7 @@
 //
 // BF16 rounding is round-to-nearest-even of the FP32 operand
 // (__float2bfloat16_rn), applied when a tile is staged into shared memory.
+#include <atomic>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -203,8 +204,23 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (uint32_t it = 0; it < kUmmaSpin; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit = kUmmaSpin) {
+    if (limit < kUmmaSpin) {
+        // a shortened limit (the test hook) polls without suspending, so a
+        // wait on copies still in flight gives up after `limit` polls
+        for (uint32_t it = 0; it < limit; ++it) {
+            uint32_t done;
+            asm volatile(
+                "{\n\t.reg .pred P1;\n\tmbarrier.test_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                : "=r"(done)
+                : "r"(bar), "r"(parity)
+                : "memory");
+            if (done) return true;
+        }
+        return false;
+    }
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
@@ -237,7 +253,7 @@ __global__ void __launch_bounds__(kUmmaT, 1) gnn_umma_kernel(int64_t M, int K1, 
                                                              const float* __restrict__ X2,
                                                              const __nv_bfloat16* __restrict__ Bt,
                                                              const float* __restrict__ bias, int relu,
-                                                             float* __restrict__ Y, int* err) {
+                                                             float* __restrict__ Y, int* err, uint32_t spin) {
     extern __shared__ __align__(1024) uint8_t umma_smem[];
     uint8_t* sA = umma_smem + kUmmaOffA;
     uint8_t* sB = umma_smem + kUmmaOffB;
@@ -293,7 +309,7 @@ __global__ void __launch_bounds__(kUmmaT, 1) gnn_umma_kernel(int64_t M, int K1, 
     for (; t < ntiles; t += grid, ++i) {
         const int s = (int)(i & 1);
         const int rows = umma_rows(M, t);
-        const bool ok = !bad && mbar_wait(bar_full0 + 8 * s, (uint32_t)((i >> 1) & 1));
+        const bool ok = !bad && mbar_wait(bar_full0 + 8 * s, (uint32_t)((i >> 1) & 1), spin);
         if (ok) {
             const uint8_t* x1 = umma_smem + s * kUmmaStage;
             const uint8_t* x2 = x1 + kUmmaM * 4 * K1;
@@ -340,7 +356,7 @@ __global__ void __launch_bounds__(kUmmaT, 1) gnn_umma_kernel(int64_t M, int K1, 
                          : "memory");
         }
         // warp-uniform outcome: tcgen05.ld below is a .sync.aligned warp instruction
-        if (!__all_sync(0xffffffffu, mbar_wait(bar_mma, (uint32_t)(i & 1)))) {
+        if (!__all_sync(0xffffffffu, mbar_wait(bar_mma, (uint32_t)(i & 1), spin))) {
             bad = true;  // the next iteration's barrier takes every thread to the exit
             continue;
         }
@@ -393,10 +409,13 @@ __global__ void __launch_bounds__(kUmmaT, 1) gnn_umma_kernel(int64_t M, int K1, 
         __syncwarp();
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    if (tid == 0 && bad) {
+    // any warp's timeout counts (one that gave up on the last tile's MMA
+    // leaves the loop without the others noticing)
+    const bool any_bad = __syncthreads_or(bad);
+    if (tid == 0 && any_bad) {
         // a wait timed out in iteration i: settle what is still in flight
         // (the copies of tiles i and i + 1 and the MMA of iteration i - 1)
+        // with the full bound, whatever limit the loop's waits had
         atomicExch(err, 1);
         if (t < ntiles) mbar_wait(bar_full0 + 8 * (int)(i & 1), (uint32_t)((i >> 1) & 1));
         if (t + grid < ntiles) mbar_wait(bar_full0 + 8 * (int)((i + 1) & 1), (uint32_t)(((i + 1) >> 1) & 1));
@@ -566,6 +585,9 @@ int hn_gnn_linear(int64_t M, int K1, int K2, const float* X1, const float* X2, c
 // hn_gnn_check.
 int* umma_flag(cudaStream_t s) { return reinterpret_cast<int*>(workspace(s).select + 7); }
 
+// Poll limit of the tcgen05 layer's pipeline waits (hn_gnn_set_wait_limit).
+std::atomic<uint32_t> g_umma_spin{kUmmaSpin};
+
 int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1, const float* X2, const void* Wt_bf16,
                        const float* bias, int relu, float* Y, void* stream) {
     return guard("hn_gnn_linear_umma", [&] {
@@ -586,9 +608,15 @@ int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1, const float* 
         }
         const int64_t tiles = (M + kUmmaM - 1) / kUmmaM;
         gnn_umma_kernel<<<(unsigned)std::min<int64_t>(tiles, ctx().sm_count), kUmmaT, kUmmaSmem, s>>>(
-            M, K1, K2, X1, X2, static_cast<const __nv_bfloat16*>(Wt_bf16), bias, relu, Y, umma_flag(s));
+            M, K1, K2, X1, X2, static_cast<const __nv_bfloat16*>(Wt_bf16), bias, relu, Y, umma_flag(s),
+            g_umma_spin.load());
         launched("gnn_umma_kernel");
     });
+}
+
+int hn_gnn_set_wait_limit(uint32_t polls) {
+    g_umma_spin.store(polls == 0 ? kUmmaSpin : polls);
+    return HN_OK;
 }
 
 int hn_gnn_check(void* stream) {

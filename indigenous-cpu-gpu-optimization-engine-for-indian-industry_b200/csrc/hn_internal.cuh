@@ -345,5 +345,15 @@ struct hn_pattern {
     int32_t max_row = 0;             // longest row of N (slots)
     int64_t* tq = nullptr;           // m+1: term offsets per row
     uint16_t* smap = nullptr;        // nq
-    int64_t* msrow = nullptr;        // m+1: multi-slot offsets per row
+    int64_t* msrow = nullptr;        // m+1: multi-slot offsets per row (row mode and relative map)
+    // relative map (rows of N long enough to keep a warp busy): instead of
+    // gmap, 4 bytes per slot -- ((e - rp_A[i]) << qbits) | (p - rp_AT[j]) for
+    // the single term of A entry e (column j) and A^T entry p, or kMulti |
+    // (index of the slot among row i's multi slots); ecs[e] = rp_AT[ci[e]].
+    // Rows are handed out longest first (order) from a counter (row_next).
+    uint32_t* rmap = nullptr;        // nnz
+    int32_t* ecs = nullptr;          // nnz(A)
+    int32_t* order = nullptr;        // m
+    unsigned* row_next = nullptr;    // 1
+    int qbits = 0;
 };

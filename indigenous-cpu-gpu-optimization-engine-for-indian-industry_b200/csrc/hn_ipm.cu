@@ -219,6 +219,73 @@ __global__ void __launch_bounds__(kT) max_step_kernel(int64_t n, const double* _
     }
 }
 
+// Relative KKT residual of the iterate with the scaling undone: per block the
+// maxima of |rp| ru, |b| ru, |rd| cu, |c| cu and the sums c^T x, b^T lam; the
+// last block folds the partials in block order (deterministic).
+constexpr int kKktMaxBlocks = 592;  // 6 partial arrays fit the workspace's 4 x kMaxReduceBlocks
+static_assert(6 * kKktMaxBlocks <= 4 * kMaxReduceBlocks, "kkt partials exceed the workspace");
+
+__global__ void __launch_bounds__(kT) kkt_kernel(int64_t n, int64_t m, const double* __restrict__ x,
+                                                 const double* __restrict__ lam, const double* __restrict__ b,
+                                                 const double* __restrict__ c, const double* __restrict__ rp,
+                                                 const double* __restrict__ rd, const double* __restrict__ ru,
+                                                 const double* __restrict__ cu, double offset, double* partials,
+                                                 unsigned* counter, double* out) {
+    __shared__ double sh[32];
+    double pr = 0.0, bn = 0.0, du = 0.0, cn = 0.0, cx = 0.0, by = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * kT;
+    for (int64_t j = blockIdx.x * (int64_t)kT + threadIdx.x; j < n; j += stride) {
+        const double u = cu[j], cj = c[j];
+        const double t = fabs(rd[j]) * u;
+        du = fmax(du, t <= 1.7976931348623157e308 ? t : INFINITY);  // NaN or inf counts as infinite
+        cn = fmax(cn, fabs(cj) * u);
+        cx += cj * x[j];
+    }
+    for (int64_t i = blockIdx.x * (int64_t)kT + threadIdx.x; i < m; i += stride) {
+        const double u = ru[i], bi = b[i];
+        const double t = fabs(rp[i]) * u;
+        pr = fmax(pr, t <= 1.7976931348623157e308 ? t : INFINITY);
+        bn = fmax(bn, fabs(bi) * u);
+        by += bi * lam[i];
+    }
+    const int G = gridDim.x;
+    const double v0 = block_max<kT>(pr, sh), v1 = block_max<kT>(bn, sh), v2 = block_max<kT>(du, sh),
+                 v3 = block_max<kT>(cn, sh), v4 = block_sum<kT>(cx, sh), v5 = block_sum<kT>(by, sh);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = v0;
+        partials[G + blockIdx.x] = v1;
+        partials[2 * G + blockIdx.x] = v2;
+        partials[3 * G + blockIdx.x] = v3;
+        partials[4 * G + blockIdx.x] = v4;
+        partials[5 * G + blockIdx.x] = v5;
+    }
+    if (!last_block(counter)) return;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a5 = 0.0;
+    for (int k = threadIdx.x; k < G; k += kT) {
+        a0 = fmax(a0, __ldcg(partials + k));
+        a1 = fmax(a1, __ldcg(partials + G + k));
+        a2 = fmax(a2, __ldcg(partials + 2 * G + k));
+        a3 = fmax(a3, __ldcg(partials + 3 * G + k));
+        a4 += __ldcg(partials + 4 * G + k);
+        a5 += __ldcg(partials + 5 * G + k);
+    }
+    a0 = block_max<kT>(a0, sh);
+    a1 = block_max<kT>(a1, sh);
+    a2 = block_max<kT>(a2, sh);
+    a3 = block_max<kT>(a3, sh);
+    a4 = block_sum<kT>(a4, sh);
+    a5 = block_sum<kT>(a5, sh);
+    if (threadIdx.x == 0) {
+        const double P = a0 / (1.0 + a1), Dl = a2 / (1.0 + a3), Gp = fabs(a4 - a5) / (1.0 + fabs(a4 + offset));
+        // NaN in any part makes the whole residual NaN (never "converged")
+        out[0] = (P != P || Dl != Dl || Gp != Gp) ? nan("") : fmax(P, fmax(Dl, Gp));
+        out[1] = P;
+        out[2] = Dl;
+        out[3] = Gp;
+        *counter = 0u;
+    }
+}
+
 int red_grid(int64_t n) { return grid_for(n, kT * 4, kMaxReduceBlocks); }
 
 void need_t(const hn_csr* A) {
@@ -302,6 +369,21 @@ int hn_ipm_update(int64_t n, int64_t m, double* x, const double* dx, double* z, 
         update_kernel<<<grid_for(n > m ? n : m, kT, ctx().sm_count * 16), kT, 0, s>>>(n, m, x, dx, z, dz, lam,
                                                                                      dlam, scal);
         launched("update_kernel");
+    });
+}
+
+int hn_ipm_kkt(int64_t n, int64_t m, const double* x, const double* lam, const double* b, const double* c,
+               const double* rp, const double* rd, const double* ru, const double* cu, double offset, double* kkt,
+               void* stream) {
+    return guard("hn_ipm_kkt", [&] {
+        require_init();
+        if (n < 1 || m < 0 || !x || !c || !rd || !cu || !kkt || (m > 0 && (!lam || !b || !rp || !ru)))
+            fail(HN_ERR_INVALID_ARG, "bad arguments");
+        cudaStream_t s = as_stream(stream);
+        Workspace& w = workspace(s);
+        kkt_kernel<<<grid_for(n > m ? n : m, kT * 4, kKktMaxBlocks), kT, 0, s>>>(n, m, x, lam, b, c, rp, rd, ru, cu,
+                                                                                  offset, w.partials, w.counter, kkt);
+        launched("kkt_kernel");
     });
 }
 

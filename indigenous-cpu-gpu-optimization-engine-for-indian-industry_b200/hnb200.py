@@ -91,6 +91,7 @@ SIGNATURES = {
     "hn_ipm_corrector": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "hn_ipm_update": [_i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "hn_max_step": [_i64, _vp, _vp, _vp, _vp],
+    "hn_ipm_kkt": [_i64, _i64] + [_vp] * 8 + [C.c_double, _vp, _vp],
     "hn_spmv_noalloc": [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp],
     "hn_csr_spmv_kind": [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "hn_spmv_residual": [_vp, C.c_int, _vp, _vp, _vp, _vp],
@@ -104,6 +105,7 @@ SIGNATURES = {
     "hn_gnn_linear": [_i64, C.c_int, C.c_int, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp],
     "hn_gnn_linear_umma": [_i64, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp],
     "hn_gnn_check": [_vp],
+    "hn_gnn_set_wait_limit": [C.c_uint32],
     "hn_gnn_linear_bwd": [_i64, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _i64,
                           _vp],
     "hn_gnn_split_grad": [_i64, _vp, _vp, _vp, _vp],
@@ -117,6 +119,9 @@ SIGNATURES = {
     "hn_batch_steps": [_vp] + [_vp] * 7 + [_vp],
     "hn_batch_corrector": [_vp, _vp] + [_vp] * 9 + [_vp],
     "hn_batch_update": [_vp] + [_vp] * 9 + [C.c_int, _vp],
+    "hn_batch_set_kkt": [_vp, _vp, _vp, _vp, C.c_double, C.c_int],
+    "hn_batch_kkt": [_vp, _f64p, _i32p],
+    "hn_batch_finish": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
 }
 _RESTYPE = {"hn_last_error": C.c_char_p}
 
@@ -298,9 +303,17 @@ class Csr:
 class Pattern:
     """Fixed pattern of A diag(d) A^T + reg I (hn_pattern)."""
 
-    def __init__(self, A: Csr, compact: bool = False):
+    # numeric layouts (hn_ada_symbolic_ex flags; hn_pattern_mode numbers)
+    GATHER, ROW, RELATIVE = 0, 1, 2
+
+    def __init__(self, A: Csr, compact: bool = False, layout: int | None = None):
+        """layout: None = the library's choice, or GATHER / RELATIVE / ROW
+        (ROW is also what compact=True asks for)."""
+        flags = 1 if compact else 0
+        if layout is not None:
+            flags = {self.GATHER: 2, self.ROW: 1, self.RELATIVE: 4}[layout]
         h = C.c_void_p()
-        check(load().hn_ada_symbolic_ex(A.h, 1 if compact else 0, C.byref(h)))
+        check(load().hn_ada_symbolic_ex(A.h, flags, C.byref(h)))
         self.h = h
         self.A = A
         m, nnz = C.c_int64(), C.c_int64()
@@ -308,10 +321,10 @@ class Pattern:
         self.m, self.nnz = m.value, nnz.value
 
     def mode(self):
-        """(row_mode, longest row of N)."""
+        """(layout: GATHER / ROW / RELATIVE, longest row of N)."""
         rm, mr = C.c_int(), C.c_int64()
         check(load().hn_pattern_mode(self.h, C.byref(rm), C.byref(mr)))
-        return bool(rm.value), mr.value
+        return rm.value, mr.value
 
     def export(self):
         rp = np.empty(self.m + 1, dtype=np.uint64)
@@ -396,14 +409,16 @@ class IpmOptions(C.Structure):
                 ("complementarity_tol", C.c_double), ("regularization", C.c_double), ("device", C.c_int),
                 ("verbose", C.c_int), ("interrupt_cb", INTERRUPT_CB), ("interrupt_user", C.c_void_p),
                 ("initial_x", _f64p), ("initial_y", _f64p), ("initial_s", _f64p), ("warm_start_floor", C.c_double),
-                ("factorization", C.c_int)]
+                ("factorization", C.c_int), ("kkt_tol", C.c_double), ("kkt_extra_iterations", C.c_int)]
 
 
 class IpmResult(C.Structure):
     _fields_ = [("status", C.c_int), ("iterations", C.c_int64), ("objective", C.c_double),
                 ("solve_time_ms", C.c_double), ("device_ms", C.c_double), ("factor_ms", C.c_double),
                 ("solve_ms", C.c_double), ("nnz_normal", C.c_int64), ("warm_start_used", C.c_int),
-                ("kkt_default", C.c_double), ("kkt_warm", C.c_double)]
+                ("kkt_default", C.c_double), ("kkt_warm", C.c_double), ("kkt", C.c_double),
+                ("kkt_primal", C.c_double), ("kkt_dual", C.c_double), ("kkt_gap", C.c_double),
+                ("reference_iterations", C.c_int64)]
 
 
 class SparseLdltStats(C.Structure):
@@ -420,7 +435,7 @@ HOST_SIGNATURES = {
     "hn_lp_solve_batch": (C.c_int, [_i64, _i64p, _i64p, _i64p, _u64p, _u64p, _f64p, _f64p, _f64p,
                                     C.POINTER(C.c_int), _f64p, _f64p, C.POINTER(C.c_int), _f64p,
                                     C.POINTER(IpmOptions), C.POINTER(C.c_int), _f64p, _i64p, _f64p, _vp,
-                                    C.POINTER(C.c_int), _f64p, _f64p]),
+                                    C.POINTER(C.c_int), _f64p, _f64p, _f64p, _i64p]),
     "hn_mps_read_file": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),
     "hn_mps_read_string": (C.c_int, [C.c_char_p, _i64, C.c_int, C.POINTER(_vp)]),
     "hn_lp_read_file": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
@@ -599,9 +614,11 @@ def crossover_basis(x, lb, ub) -> np.ndarray:
 
 def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=0.0, max_iter=100,
              time_limit=0.0, device=0, interrupt=None, verbose=False, x0=None, y0=None, s0=None, warm_floor=None,
-             factorization=0):
+             factorization=0, kkt_tol=1e-8, kkt_extra=10):
     """GPU IPM on an LP given as CSR (rows EQ and x >= 0 unless told otherwise);
-    x0/y0/s0: optional warm start in the original space."""
+    x0/y0/s0: optional warm start in the original space. kkt_tol / kkt_extra:
+    tightening past the reference's stop (kkt_tol <= 0: the reference's rule
+    alone); the result's `kkt` is the relative KKT residual on the unscaled LP."""
     m, n = int(lp["m"]), int(lp["n"])
     rp, ci, val = u64(lp["rp"]), u64(lp["ci"]), f64(lp["val"])
     c, b = f64(lp["c"]), f64(lp["b"])
@@ -620,6 +637,8 @@ def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=
     if warm_floor is not None:
         opt.warm_start_floor = warm_floor
     opt.factorization = int(factorization)  # 0 auto, 1 dense, 2 sparse (host normal-matrix factorisation)
+    opt.kkt_tol = float(kkt_tol)
+    opt.kkt_extra_iterations = int(kkt_extra)
     res = IpmResult()
     x = np.zeros(n)
     y = np.full(m, np.nan)
@@ -634,7 +653,8 @@ def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=
             "iterations": res.iterations, "time_ms": res.solve_time_ms, "device_ms": res.device_ms,
             "factor_ms": res.factor_ms, "solve_ms": res.solve_ms, "nnz_normal": res.nnz_normal, "x": x,
             "y": y, "s": s, "warm_start_used": bool(res.warm_start_used), "kkt_default": res.kkt_default,
-            "kkt_warm": res.kkt_warm, "error": err}
+            "kkt_warm": res.kkt_warm, "kkt": res.kkt, "kkt_parts": (res.kkt_primal, res.kkt_dual, res.kkt_gap),
+            "reference_iterations": res.reference_iterations, "error": err}
 
 
 class BatchStats(C.Structure):
@@ -644,9 +664,11 @@ class BatchStats(C.Structure):
 
 
 def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs=None, x0s=None, y0s=None,
-                   s0s=None, warm_floor=None):
+                   s0s=None, warm_floor=None, kkt_tol=1e-8, kkt_extra=10):
     """Batched GPU IPM over a list of LP dicts (rows EQ, x >= 0 unless given);
-    x0s/y0s/s0s: optional per-instance warm starts (lists of arrays)."""
+    x0s/y0s/s0s: optional per-instance warm starts (lists of arrays);
+    kkt_tol / kkt_extra as in lp_solve (per instance). The result's `kkt` is
+    K x 4: relative KKT residual, primal, dual and gap parts."""
     K = len(lps)
     row_off = np.zeros(K + 1, np.int64)
     col_off = np.zeros(K + 1, np.int64)
@@ -669,6 +691,8 @@ def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs
     host().hn_ipm_default_options(C.byref(opt))
     opt.max_iterations = max_iter
     opt.device = device
+    opt.kkt_tol = float(kkt_tol)
+    opt.kkt_extra_iterations = int(kkt_extra)
     keep = _warm_arrays(opt, None if x0s is None else np.concatenate(x0s),  # noqa: F841
                         None if y0s is None else np.concatenate(y0s), None if s0s is None else np.concatenate(s0s))
     if warm_floor is not None:
@@ -681,6 +705,8 @@ def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs
     y = np.full(row_off[-1], np.nan)
     s = np.full(col_off[-1], np.nan)
     st = BatchStats()
+    kkt = np.full((K, 4), np.nan)
+    ref_it = np.zeros(K, np.int64)
     P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
     host_check(host().hn_lp_solve_batch(K, P(row_off, C.c_int64), P(col_off, C.c_int64), P(nnz_off, C.c_int64),
                                         P(rp, C.c_uint64), P(ci, C.c_uint64), P(val, C.c_double), P(c, C.c_double),
@@ -688,9 +714,9 @@ def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs
                                         P(maxi, C.c_int), P(off, C.c_double), C.byref(opt), P(status, C.c_int),
                                         P(obj, C.c_double), P(iters, C.c_int64), P(x, C.c_double),
                                         C.cast(C.pointer(st), C.c_void_p), P(warm_used, C.c_int), P(y, C.c_double),
-                                        P(s, C.c_double)))
+                                        P(s, C.c_double), P(kkt, C.c_double), P(ref_it, C.c_int64)))
     return {"status": status, "objective": obj, "iterations": iters, "x": x, "y": y, "s": s, "col_off": col_off,
-            "row_off": row_off,
+            "row_off": row_off, "kkt": kkt, "reference_iterations": ref_it,
             "warm_used": warm_used.astype(bool),
             "stats": {k: getattr(st, k) for k, _ in BatchStats._fields_}}
 

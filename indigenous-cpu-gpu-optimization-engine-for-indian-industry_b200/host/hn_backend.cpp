@@ -14,19 +14,48 @@ uint64_t mix(uint64_t h, uint64_t v) {
     return h;
 }
 
+// 64-bit finaliser (splitmix64's): every input bit affects every output bit.
+inline uint64_t avalanche(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+// Hash of n 64-bit words, in chunks of 2^16 words hashed in parallel and
+// combined in chunk order (the result does not depend on the thread count).
+uint64_t hash_words(const void* data, std::size_t n, uint64_t seed) {
+    const auto* w = static_cast<const uint64_t*>(data);
+    constexpr std::size_t kChunk = std::size_t(1) << 16;
+    const std::size_t chunks = (n + kChunk - 1) / kChunk;
+    std::vector<uint64_t> part(chunks);
+#pragma omp parallel for schedule(static) if (chunks > 4)
+    for (std::size_t c = 0; c < chunks; ++c) {
+        const std::size_t e = (c + 1) * kChunk < n ? (c + 1) * kChunk : n;
+        uint64_t a = seed ^ (c * 0x9e3779b97f4a7c15ull), b = ~seed;
+        std::size_t k = c * kChunk;
+        for (; k + 1 < e; k += 2) {  // two independent lanes
+            a = avalanche(a ^ w[k]) + 0x632be59bd9b4e019ull;
+            b = avalanche(b ^ w[k + 1]) + 0x8cb92ba72f3d8dd7ull;
+        }
+        if (k < e) a = avalanche(a ^ w[k]);
+        part[c] = avalanche(a ^ (b << 1) ^ (b >> 63));
+    }
+    uint64_t h = avalanche(seed ^ n);
+    for (uint64_t v : part) h = avalanche(h ^ v);
+    return h;
+}
+
+// Hash of every value, column index and row pointer: a caller that rewrites
+// any entry of a matrix whose buffers it reuses gets a new device copy (the
+// reference's cache checks only the pointer and the sizes,
+// gpu_backend.cpp:289-306).
 uint64_t fingerprint(const std::vector<double>& values, const std::vector<std::size_t>& col_indices,
                      const std::vector<std::size_t>& row_ptr) {
+    static_assert(sizeof(double) == 8 && sizeof(std::size_t) == 8, "64-bit words expected");
     uint64_t h = mix(values.size(), row_ptr.size());
-    const std::size_t nnz = values.size();
-    const std::size_t samples = nnz < 64 ? nnz : 64;
-    for (std::size_t s = 0; s < samples; ++s) {
-        const std::size_t k = samples == nnz ? s : (s * (nnz - 1)) / (samples - 1);
-        uint64_t bits;
-        std::memcpy(&bits, &values[k], 8);
-        h = mix(mix(h, bits), col_indices[k]);
-    }
-    const std::size_t rs = row_ptr.size() < 64 ? row_ptr.size() : 64;
-    for (std::size_t s = 0; s < rs; ++s) h = mix(h, row_ptr[(s * (row_ptr.size() - 1)) / (rs > 1 ? rs - 1 : 1)]);
+    h = mix(h, hash_words(values.data(), values.size(), 0x51ed270b27f1e5a1ull));
+    h = mix(h, hash_words(col_indices.data(), col_indices.size(), 0x2545f4914f6cdd1dull));
+    h = mix(h, hash_words(row_ptr.data(), row_ptr.size(), 0x9fb21c651e98df25ull));
     return h;
 }
 

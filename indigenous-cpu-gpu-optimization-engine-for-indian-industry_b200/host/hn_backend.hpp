@@ -89,7 +89,7 @@ private:
     };
     // Device copy of a matrix, keyed by the host values pointer like the
     // reference's cache (gpu_backend.cpp:289-306) but also checked against
-    // sizes and a sampled fingerprint of the three arrays, so a reused buffer
+    // sizes and a hash of every entry of the three arrays, so a reused buffer
     // with new contents is uploaded again instead of returning stale data.
     Resident& resident(const std::vector<double>& values, const std::vector<std::size_t>& col_indices,
                        const std::vector<std::size_t>& row_ptr, std::size_t ncols);

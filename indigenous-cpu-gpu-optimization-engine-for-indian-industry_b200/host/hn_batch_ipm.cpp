@@ -84,6 +84,12 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
         ck(hn_memset(status.p, 0, 4 * K, st), "memset");
         ck(hn_memset(iters.p, 0, 4 * K, st), "memset");
         ck(hn_memset(scal.p, 0, 8 * HN_IPM_NSCAL * K, st), "memset");
+        // relative KKT residual per instance and tightening past the reference's rule
+        DevBuf ru(8 * m), cu(8 * n), koff(8 * K);
+        ck(hn_memcpy_h2d(ru.p, pf.ru.data(), 8 * m, st), "H2D");
+        ck(hn_memcpy_h2d(cu.p, pf.cu.data(), 8 * n, st), "H2D");
+        ck(hn_memcpy_h2d(koff.p, pf.offset.data(), 8 * K, st), "H2D");
+        ck(hn_batch_set_kkt(B, ru.d(), cu.d(), koff.d(), O.kkt_tol, O.kkt_extra_iterations), "hn_batch_set_kkt");
         std::vector<int32_t> hstatus(K), hiters(K);
         auto read_status = [&]() {
             ck(hn_memcpy_d2h(hstatus.data(), status.p, 4 * K, st), "D2H status");
@@ -135,7 +141,10 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
         ck(hn_batch_residuals(B, M, x.d(), lam.d(), z.d(), b.d(), c.d(), mx.d(), rp.d(), rd.d(), D.d(), Drd.d(),
                               scal.d(), st_copy.i(), iters.i(), iter, O.convergence_tol, O.complementarity_tol, st),
            "hn_batch_residuals");
-        std::vector<double> hscal(HN_IPM_NSCAL * K), hx(n), hl(m);
+        ck(hn_batch_finish(B, x.d(), z.d(), lam.d(), status.i(), iters.i(), st), "hn_batch_finish");
+        std::vector<double> hscal(HN_IPM_NSCAL * K), hx(n), hl(m), hkkt(4 * K);
+        std::vector<int32_t> href(K);
+        ck(hn_batch_kkt(B, hkkt.data(), href.data()), "hn_batch_kkt");
         ck(hn_memcpy_d2h(hl.data(), lam.p, 8 * m, st), "D2H lam");
         ck(hn_memcpy_d2h(hscal.data(), scal.p, 8 * HN_IPM_NSCAL * K, st), "D2H scal");
         ck(hn_memcpy_d2h(hstatus.data(), status.p, 4 * K, st), "D2H status");
@@ -168,6 +177,11 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
             r.warm_start_used = pf.warm_used[i] != 0;
             r.kkt_default = pf.kkt_default[i];
             r.kkt_warm = pf.kkt_warm[i];
+            r.kkt = hkkt[4 * i];
+            r.kkt_primal = hkkt[4 * i + 1];
+            r.kkt_dual = hkkt[4 * i + 2];
+            r.kkt_gap = hkkt[4 * i + 3];
+            r.reference_iterations = href[i];
             r.solve_time_ms = total_ms;
             const bool feasible_incumbent = s[HN_IPM_NRP] <= O.feasibility_tol;
             r.status = numerical_error ? model::ProblemStatus::NUMERICAL_ERROR

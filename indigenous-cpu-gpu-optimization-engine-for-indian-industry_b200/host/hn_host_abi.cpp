@@ -58,6 +58,8 @@ void hn_ipm_default_options(hn_ipm_options* o) {
     o->initial_s = nullptr;
     o->warm_start_floor = 1e-2;
     o->factorization = 0;
+    o->kkt_tol = 1e-8;
+    o->kkt_extra_iterations = 10;
 }
 
 const char* hn_host_last_error(void) { return g_err.c_str(); }
@@ -169,6 +171,8 @@ int hn_lp_solve(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, co
             }
             o.warm_start_floor = opt->warm_start_floor;
             o.factorization = opt->factorization;
+            o.kkt_tol = opt->kkt_tol;
+            o.kkt_extra_iterations = opt->kkt_extra_iterations;
             if (opt->initial_x) {
                 o.initial_point.x = vec(opt->initial_x, n);
                 if (opt->initial_y) o.initial_point.y = vec(opt->initial_y, m);
@@ -188,6 +192,11 @@ int hn_lp_solve(int64_t m, int64_t n, const uint64_t* rp, const uint64_t* ci, co
         res->warm_start_used = r.warm_start_used ? 1 : 0;
         res->kkt_default = r.kkt_default;
         res->kkt_warm = r.kkt_warm;
+        res->kkt = r.kkt;
+        res->kkt_primal = r.kkt_primal;
+        res->kkt_dual = r.kkt_dual;
+        res->kkt_gap = r.kkt_gap;
+        res->reference_iterations = (int64_t)r.reference_iterations;
         if (x_out && r.primal.size() == (std::size_t)n) std::memcpy(x_out, r.primal.data(), 8 * n);
         if (y_out && r.dual_estimate.size() == (std::size_t)m) std::memcpy(y_out, r.dual_estimate.data(), 8 * m);
         if (s_out && r.reduced_cost_estimate.size() == (std::size_t)n)
@@ -201,7 +210,7 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
                       const int* sense, const double* lb, const double* ub, const int* maximize,
                       const double* obj_offset, const hn_ipm_options* opt, int* status, double* objective,
                       int64_t* iterations, double* x_out, hn_batch_stats* stats, int* warm_used, double* y_out,
-                      double* s_out) {
+                      double* s_out, double* kkt_out, int64_t* reference_iterations) {
     return wrap([&] {
         if (K < 0 || !row_off || !col_off || !nnz_off || !status || !objective || !iterations)
             throw std::invalid_argument("bad arguments");
@@ -238,6 +247,8 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
             o.device = opt->device;
             o.warm_start_floor = opt->warm_start_floor;
             o.factorization = opt->factorization;
+            o.kkt_tol = opt->kkt_tol;
+            o.kkt_extra_iterations = opt->kkt_extra_iterations;
         }
         std::vector<hn::lp::WarmStart> warm;
         if (opt && opt->initial_x) {
@@ -257,6 +268,13 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
             objective[i] = r.objective_value;
             iterations[i] = (int64_t)r.iterations;
             if (warm_used) warm_used[i] = r.warm_start_used ? 1 : 0;
+            if (kkt_out) {
+                kkt_out[4 * i] = r.kkt;
+                kkt_out[4 * i + 1] = r.kkt_primal;
+                kkt_out[4 * i + 2] = r.kkt_dual;
+                kkt_out[4 * i + 3] = r.kkt_gap;
+            }
+            if (reference_iterations) reference_iterations[i] = (int64_t)r.reference_iterations;
             const auto& pi = probs[(std::size_t)i];
             if (y_out && r.dual_estimate.size() == pi.num_rows)
                 std::memcpy(y_out + row_off[i], r.dual_estimate.data(), 8 * pi.num_rows);

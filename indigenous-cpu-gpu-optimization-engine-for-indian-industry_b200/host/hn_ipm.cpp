@@ -407,6 +407,18 @@ std::vector<double> to_original_primal(const StandardForm& f, const std::vector<
     return primal;
 }
 
+// Unscale factors for the relative KKT residual (hn_ipm_kkt): row i of the
+// standard form is the original row times row_mult[i] (+-gamma_i) -- the
+// upper-bound rows are unscaled -- and column j carries col_scale[j]; offset
+// is the minimisation form's objective constant (shifts plus obj_offset).
+void unscale_factors(const StandardForm& f, const model::LpProblem& p, double* ru, double* cu, double* offset) {
+    for (std::size_t i = 0; i < f.m; ++i)
+        ru[i] = i < f.row_mult.size() && f.row_mult[i] != 0.0 ? 1.0 / std::abs(f.row_mult[i]) : 1.0;
+    for (std::size_t j = 0; j < f.n; ++j) cu[j] = 1.0 / f.col_scale[j];
+    const bool negate = p.obj_sense == model::ObjectiveSense::MAXIMIZE;
+    *offset = f.offset + (negate ? -p.obj_offset : p.obj_offset);
+}
+
 // Device buffer owning helper.
 struct DevBuf {
     void* p = nullptr;
@@ -531,6 +543,13 @@ void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol,
         std::copy(z.begin(), z.end(), out.z0.begin() + out.col_off[i]);
         std::copy(lam.begin(), lam.end(), out.lam0.begin() + out.row_off[i]);
     }
+    out.ru.resize(out.row_off.back());
+    out.cu.resize(out.col_off.back());
+    out.offset.resize(K);
+#pragma omp parallel for schedule(dynamic, 8)
+    for (std::size_t i = 0; i < K; ++i)
+        unscale_factors(*forms[i], problems[i], out.ru.data() + out.row_off[i], out.cu.data() + out.col_off[i],
+                        &out.offset[i]);
     out.forms = std::move(forms);
 }
 
@@ -614,6 +633,24 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
         ck(hn_memset(scal.p, 0, 8 * HN_IPM_NSCAL, st), "memset");
         double sc[HN_IPM_NSCAL];
         auto read_scal = [&]() { ck(hn_memcpy_d2h(sc, scal.p, sizeof(sc), st), "D2H scal"); };
+        // relative KKT residual of the unscaled LP, and the iterate the
+        // reference's rule accepted (kept while the solve tightens past it)
+        const bool tighten = O.kkt_tol > 0.0;
+        std::vector<double> hru(m), hcu(n);
+        double koff = 0.0;
+        unscale_factors(f, cleaned, hru.data(), hcu.data(), &koff);
+        DevBuf ru(8 * m), cu(8 * n), kkt(8 * 4), xb(tighten ? 8 * n : 8), zb(tighten ? 8 * n : 8),
+            lb(tighten ? 8 * m : 8);
+        ck(hn_memcpy_h2d(ru.p, hru.data(), 8 * m, st), "H2D");
+        ck(hn_memcpy_h2d(cu.p, hcu.data(), 8 * n, st), "H2D");
+        double kv[4] = {0, 0, 0, 0}, kref[4] = {0, 0, 0, 0};
+        long ref_iter = -1;
+        auto measure = [&]() {
+            ck(hn_ipm_kkt((int64_t)n, (int64_t)m, x.d(), lam.d(), b.d(), c.d(), rp.d(), rd.d(), ru.d(), cu.d(), koff,
+                          kkt.d(), st),
+               "hn_ipm_kkt");
+            ck(hn_memcpy_d2h(kv, kkt.p, sizeof(kv), st), "D2H kkt");
+        };
         auto flags = [&]() {
             std::uint64_t fl;
             std::memcpy(&fl, &sc[HN_IPM_FLAGS], 8);
@@ -663,8 +700,20 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
                                 scal.d(), st),
                "hn_ipm_residuals");
             read_scal();
+            measure();
             const double mu = sc[HN_IPM_MU];
-            if (sc[HN_IPM_NRP] < O.convergence_tol && sc[HN_IPM_NRD] < O.convergence_tol && mu < O.complementarity_tol) {
+            if (ref_iter < 0 && sc[HN_IPM_NRP] < O.convergence_tol && sc[HN_IPM_NRD] < O.convergence_tol &&
+                mu < O.complementarity_tol) {  // the reference's rule (:525-530)
+                ref_iter = (long)iter;
+                std::memcpy(kref, kv, sizeof(kv));
+                if (tighten) {
+                    ck(hn_memcpy_d2d(xb.p, x.p, 8 * n, st), "save x");
+                    ck(hn_memcpy_d2d(zb.p, z.p, 8 * n, st), "save z");
+                    ck(hn_memcpy_d2d(lb.p, lam.p, 8 * m, st), "save lam");
+                }
+            }
+            if (ref_iter >= 0 &&
+                (!tighten || kv[0] <= O.kkt_tol || (long)iter - ref_iter >= O.kkt_extra_iterations)) {
                 done = true;
                 result.device_ms += ms_since(t0);
                 break;
@@ -733,11 +782,30 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
                                 scal.d(), st),
                "hn_ipm_residuals");
             read_scal();
+            measure();
             last_nrp = sc[HN_IPM_NRP];
+            if (ref_iter >= 0) {
+                // the reference stopped here as OPTIMAL; whatever the
+                // tightening met afterwards, return the better iterate
+                if (tighten && (numerical_error || !(kv[0] <= kref[0]))) {
+                    ck(hn_memcpy_d2d(x.p, xb.p, 8 * n, st), "restore x");
+                    ck(hn_memcpy_d2d(z.p, zb.p, 8 * n, st), "restore z");
+                    ck(hn_memcpy_d2d(lam.p, lb.p, 8 * m, st), "restore lam");
+                    std::memcpy(kv, kref, sizeof(kv));
+                    result.iterations = (std::size_t)ref_iter;
+                }
+                done = true;
+                numerical_error = interrupted = time_up = false;
+            }
             // relaxed acceptance after the loop (:727-753); crossover is not
             // part of this solver, so the strict 1e-4 primal threshold applies
             if (!done && !interrupted && sc[HN_IPM_NRP] < 1e-4 && sc[HN_IPM_NRD] < 1e-4 && sc[HN_IPM_MU] < 1e-4)
                 done = true;
+            result.kkt = kv[0];
+            result.kkt_primal = kv[1];
+            result.kkt_dual = kv[2];
+            result.kkt_gap = kv[3];
+            result.reference_iterations = ref_iter;
         }
         ck(hn_memcpy_d2h(hx.data(), x.p, 8 * n, st), "D2H x");
         std::vector<double> primal = to_original_primal(f, hx);

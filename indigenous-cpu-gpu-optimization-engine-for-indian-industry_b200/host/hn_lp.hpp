@@ -87,6 +87,15 @@ struct InteriorPointOptions {
     // Normal-matrix factorisation on the host: 0 auto (dense LDL^T up to
     // 12,000 rows, sparse LDL^T above), 1 dense, 2 sparse (SparseLDLT).
     int factorization = 0;
+    // Tightening past the reference's stop (no counterpart in the reference,
+    // whose absolute tests on the scaled form can leave a relative duality
+    // gap above 1e-8): once those tests hold, the solve keeps iterating until
+    // the relative KKT residual of the unscaled LP (hn_ipm_kkt) is <= kkt_tol
+    // or kkt_extra_iterations more iterations have run, and returns the
+    // better of that iterate and the one the reference's rule accepted. The
+    // status is the reference rule's. kkt_tol <= 0: the reference's rule alone.
+    double kkt_tol = 1e-8;
+    int kkt_extra_iterations = 10;
 };
 
 struct InteriorPointResult {
@@ -110,6 +119,14 @@ struct InteriorPointResult {
     // fills it only through crossover, so `dual` stays zero here and the
     // estimate is reported beside it (a WarmStart for a related LP)
     std::vector<double> dual_estimate, reduced_cost_estimate;
+    // relative KKT residual of the returned iterate on the unscaled LP:
+    // max of the primal, dual and gap parts (hn_ipm_kkt), NaN if unmeasured;
+    // reference_iterations: the iteration at which the reference's stopping
+    // rule first held (-1: never; iterations - reference_iterations extra
+    // iterations tightened the result)
+    double kkt = std::numeric_limits<double>::quiet_NaN();
+    double kkt_primal = kkt, kkt_dual = kkt, kkt_gap = kkt;
+    long reference_iterations = -1;
     std::string error;
 };
 
@@ -140,6 +157,9 @@ struct PackedForm {
     std::vector<std::shared_ptr<detail::StandardForm>> forms;
     std::vector<char> warm_used;
     std::vector<double> kkt_default, kkt_warm;
+    // unscale factors of the packed rows / columns and each instance's
+    // objective constant, for the relative KKT residual (hn_ipm_kkt)
+    std::vector<double> ru, cu, offset;
 };
 // warm: empty, or one (possibly empty) WarmStart per problem
 void build_forms(const std::vector<model::LpProblem>& problems, double feas_tol, PackedForm& out,

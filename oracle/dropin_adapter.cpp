@@ -1,4 +1,5 @@
-// The HyperNova-side adapter of INTEGRATION.md, compiled against the
+// The HyperNova-side adapter a maintainer adds (hn::execution::B200Backend
+// behind the reference's IComputeBackend), compiled against the
 // reference's own headers -- TEST INFRASTRUCTURE ONLY (built into
 // oracle/_ref/libhnref_dropin.so with the reference objects). It lets a GPU
 // test run the reference's unchanged InteriorPointSolver::solve

@@ -139,6 +139,11 @@ typedef struct {
     double value;
 } trip_t;
 
+static int i64_cmp_fwd(const void* a, const void* b) {
+    const int64_t x = *(const int64_t*)a, y = *(const int64_t*)b;
+    return x < y ? -1 : (x > y);
+}
+
 static int trip_cmp(const void* a, const void* b) {
     const trip_t* x = (const trip_t*)a;
     const trip_t* y = (const trip_t*)b;
@@ -238,6 +243,94 @@ int64_t hno_normal_equations(int64_t m, int64_t n, const int64_t* rp, const int6
     free(cvals);
     free(t);
     free(diag);
+    return out;
+}
+
+/* Selected rows of the same N (interior_point.cpp:144-200), for matrices
+ * whose full triplet list does not fit: row i of N gathers, for every column
+ * j of row i with D_j > 0 (j ascending, the emission order of :176-186), the
+ * terms (a_ij * a_kj) * D_j of column j's rows k; each entry sums its terms in
+ * that order (as the stable sort of the full restatement does), exact zero
+ * sums are dropped, and the diagonal gains dyn_reg = max(reg, 1e-12 * max over
+ * ALL rows of sum_j a_ij^2 D_j) last (:188-196). absS (may be NULL) receives
+ * the same sums over |terms| (with dyn_reg on the diagonal), the scale of the
+ * 1e-12 normwise bar. With ciS == NULL only rpS (nsel + 1 offsets) is filled.
+ * Returns the entry count. */
+int64_t hno_normal_rows(int64_t m, int64_t n, const int64_t* rp, const int64_t* ci, const double* val,
+                        const double* D, double reg, int64_t nsel, const int64_t* rows, int64_t* rpS,
+                        int64_t* ciS, double* valS, double* absS, double* dyn_out) {
+    const int64_t nnz = rp[m];
+    int64_t* cs = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));
+    int64_t* crows = (int64_t*)malloc(sizeof(int64_t) * (size_t)(nnz ? nnz : 1));
+    double* cvals = (double*)malloc(sizeof(double) * (size_t)(nnz ? nnz : 1));
+    csc_of(m, n, rp, ci, val, cs, crows, cvals);
+    double max_diag = 0.0;
+    for (int64_t i = 0; i < m; ++i) {
+        double dsum = 0.0;
+        for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+            const int64_t j = ci[k];
+            if (D[j] <= 0.0) continue;
+            dsum += val[k] * val[k] * D[j];
+        }
+        max_diag = (max_diag < dsum) ? dsum : max_diag;
+    }
+    double dyn = 1e-12 * max_diag;
+    dyn = (reg < dyn) ? dyn : reg;
+    double* acc = (double*)calloc((size_t)(m ? m : 1), sizeof(double));
+    double* aab = (double*)calloc((size_t)(m ? m : 1), sizeof(double));
+    char* seen = (char*)calloc((size_t)(m ? m : 1), 1);
+    int64_t* touched = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m ? m : 1));
+    int64_t out = 0;
+    rpS[0] = 0;
+    for (int64_t s = 0; s < nsel; ++s) {
+        const int64_t i = rows[s];
+        int64_t nt = 0;
+        for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+            const int64_t j = ci[k];
+            if (D[j] <= 0.0) continue;
+            const double d = D[j], aij = val[k];
+            for (int64_t q = cs[j]; q < cs[j + 1]; ++q) {
+                const int64_t r = crows[q];
+                const double t = aij * cvals[q] * d;
+                if (!seen[r]) {
+                    seen[r] = 1;
+                    touched[nt++] = r;
+                }
+                acc[r] += t;
+                aab[r] += fabs(t);
+            }
+        }
+        if (!seen[i]) {
+            seen[i] = 1;
+            touched[nt++] = i;
+        }
+        acc[i] += dyn;
+        aab[i] += dyn;
+        qsort(touched, (size_t)nt, sizeof(int64_t), i64_cmp_fwd);
+        for (int64_t t = 0; t < nt; ++t) {
+            const int64_t r = touched[t];
+            if (acc[r] != 0.0) {
+                if (ciS) {
+                    ciS[out] = r;
+                    valS[out] = acc[r];
+                    if (absS) absS[out] = aab[r];
+                }
+                ++out;
+            }
+            acc[r] = 0.0;
+            aab[r] = 0.0;
+            seen[r] = 0;
+        }
+        rpS[s + 1] = out;
+    }
+    if (dyn_out) *dyn_out = dyn;
+    free(cs);
+    free(crows);
+    free(cvals);
+    free(acc);
+    free(aab);
+    free(seen);
+    free(touched);
     return out;
 }
 

@@ -56,6 +56,10 @@ int64_t hno_normal_equations_triplets(int64_t m, int64_t n, const int64_t* rp,
 int64_t hno_normal_equations(int64_t m, int64_t n, const int64_t* rp, const int64_t* ci,
                              const double* val, const double* D, double reg, int64_t* rpN,
                              int64_t* ciN, double* valN, double* dyn_reg_out);
+/* selected rows of the same N, with |term| sums (see hn_oracle.c) */
+int64_t hno_normal_rows(int64_t m, int64_t n, const int64_t* rp, const int64_t* ci, const double* val,
+                        const double* D, double reg, int64_t nsel, const int64_t* rows, int64_t* rpS,
+                        int64_t* ciS, double* valS, double* absS, double* dyn_out);
 
 /* Structural pattern of M M^T plus the full diagonal, rows sorted, no values
  * (the pattern build_normal_equations produces when every D_j > 0 and no sum

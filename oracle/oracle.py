@@ -31,11 +31,13 @@ _port = None
 _ref = None
 
 
-def build(ref: bool = True) -> None:
-    """make the port (always) and the reference build (when its sources exist)."""
+def build(ref_dir: str | None = None) -> None:
+    """make the port (always) and, given the reference's source root (or the
+    REF environment variable), the reference build."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if ref and os.path.isdir(os.environ.get("REF", "/root/reference")):
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+    ref_dir = ref_dir or os.environ.get("REF")
+    if ref_dir and os.path.isdir(os.path.join(ref_dir, "core")):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={ref_dir}"], check=True)
 
 
 def _p(a, ct):
@@ -46,7 +48,7 @@ def port():
     global _port
     if _port is None:
         if not os.path.exists(PORT_LIB):
-            build(ref=False)
+            build()
         lib = C.CDLL(PORT_LIB)
         sig = {
             "hno_csr_multiply": (None, [_i64, _i64p, _i64p, _f64p, _f64p, _f64p]),
@@ -63,6 +65,8 @@ def port():
             "hno_normal_equations": (_i64, [_i64, _i64, _i64p, _i64p, _f64p, _f64p, C.c_double, _i64p,
                                             _i64p, _f64p, _f64p]),
             "hno_ada_pattern": (_i64, [_i64, _i64, _i64p, _i64p, _i64p, _i32p]),
+            "hno_normal_rows": (_i64, [_i64, _i64, _i64p, _i64p, _f64p, _f64p, C.c_double, _i64, _i64p, _i64p,
+                                       _i64p, _f64p, _f64p, _f64p]),
             "hno_merge_tiles": (None, [_i64, _i64, _i32p, _i64, _i64, _i32p, _i32p]),
             "hno_price_reduced_costs": (None, [_i64, _i64, _i64p, _i64p, _f64p, _f64p, _f64p, _f64p]),
             "hno_price_devex_update": (None, [_i64, _i64, _i64p, _i64p, _f64p, _f64p, _i32p, _f64p, _f64p]),
@@ -225,6 +229,23 @@ def normal_equations(rp, ci, val, D, reg, n):
                                     _p(D, C.c_double), reg, _p(rpN, C.c_int64), _p(ciN, C.c_int64),
                                     _p(valN, C.c_double), C.byref(dyn))
     return rpN, ciN[:w], valN[:w], dyn.value
+
+
+def normal_rows(rp, ci, val, D, reg, n, rows):
+    """Rows `rows` of build_normal_equations' N: (rpS, ciS, valS, absS, dyn)
+    with rpS the offsets of the selected rows (hno_normal_rows)."""
+    rp, ci, val, D, rows = i64(rp), i64(ci), f64(val), f64(D), i64(rows)
+    m = rp.shape[0] - 1
+    rpS = np.empty(rows.shape[0] + 1, dtype=np.int64)
+    args = (m, n, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(val, C.c_double), _p(D, C.c_double), reg,
+            rows.shape[0], _p(rows, C.c_int64), _p(rpS, C.c_int64))
+    total = port().hno_normal_rows(*args, None, None, None, None)
+    ciS = np.empty(max(total, 1), dtype=np.int64)
+    valS = np.empty(max(total, 1))
+    absS = np.empty(max(total, 1))
+    dyn = C.c_double()
+    port().hno_normal_rows(*args, _p(ciS, C.c_int64), _p(valS, C.c_double), _p(absS, C.c_double), C.byref(dyn))
+    return rpS, ciS[:total], valS[:total], absS[:total], dyn.value
 
 
 def ada_pattern(rp, ci, n):

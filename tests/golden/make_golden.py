@@ -1,7 +1,7 @@
 """Generates the golden fixtures in this folder from the reference itself.
 
-Run in a checkout that has the reference sources (oracle/Makefile builds
-oracle/_ref/libhnref.so from them): `python tests/golden/make_golden.py`.
+Run with the reference's source root in REF (oracle/Makefile builds
+oracle/_ref/libhnref.so from it): `REF=<dir> python tests/golden/make_golden.py`.
 Every output array below is produced by the reference's own code through
 oracle/ref_shim.cpp; inputs are rebuilt from their seeds by tests/refcases.py
 (the reference tests' mt19937 generators) and the package's lpgen.py.
@@ -68,7 +68,7 @@ def normal_eq_triplets(rp, ci, val, D, reg):
 
 
 def main():
-    O.build(ref=True)
+    O.build(os.environ.get("REF"))
     assert O.ref() is not None, "reference build missing"
     out = {}
     # CpuBackendTest.SpmvMatchesReference (test_gpu_backend.cpp:90-98) and the

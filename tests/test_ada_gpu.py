@@ -130,10 +130,50 @@ def test_large_zipf_pattern_properties(hn, torch_cuda):
     assert torch.equal(row_cnt, col_cnt)
 
 
-@pytest.mark.parametrize("shape", [(2000, 5000, 8, 0), (529, 1322, 6, 7)])
-def test_row_and_gather_modes_bit_identical(hn, torch_cuda, shape):
-    """The two numeric layouts give the same bits (gather mode is the
-    default; row mode is asked for)."""
+def test_large_zipf_sampled_rows_match_oracle(hn, torch_cuda):
+    """The benchmarked size (m 200k, n 500k, 5.16M nonzeros, nnz(N) 9.7e8):
+    4,096 rows of N -- the 64 longest and a seeded sample of the rest --
+    against the row-restricted oracle restatement of build_normal_equations.
+    Pattern bit-exact, values within 1e-12 normwise, dyn_reg equal."""
+    import ctypes as C
+
+    torch = torch_cuda
+    lp = lpgen.scaled_problem(lpgen.lp_zipf(seed=1000))
+    m, n = lp["m"], lp["n"]
+    A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
+    P = hn.Pattern(A)
+    D = np.random.default_rng(17).uniform(0.5, 1.5, n)
+    nval = torch.empty(P.nnz, dtype=torch.float64, device="cuda")
+    dyn = torch.empty(1, dtype=torch.float64, device="cuda")
+    P.numeric(torch.as_tensor(D, device="cuda"), 1e-8, nval, dyn)
+    torch.cuda.synchronize()
+    rp_d, ci_d, _ = P.device_arrays()
+    lib = hn.load()
+    rpN = np.empty(m + 1, dtype=np.int64)
+    hn.check(lib.hn_memcpy_d2h(rpN.ctypes.data, rp_d, 8 * (m + 1), None))
+    lens = np.diff(rpN)
+    longest = np.argsort(-lens, kind="stable")[:64]
+    rest = np.setdiff1d(np.arange(m), longest)
+    rows = np.sort(np.concatenate([longest, np.random.default_rng(5).choice(rest, 4096 - 64, replace=False)]))
+    rpS, ciS, vS, aS, dynS = O.normal_rows(lp["rp"], lp["ci"], lp["val"], D, 1e-8, n, rows)
+    assert float(dyn.item()) == dynS
+    for s, i in enumerate(rows):
+        a, b = int(rpN[i]), int(rpN[i + 1])
+        assert b - a == rpS[s + 1] - rpS[s], (i, b - a, rpS[s + 1] - rpS[s])
+        cols = np.empty(b - a, dtype=np.int32)
+        hn.check(lib.hn_memcpy_d2h(cols.ctypes.data, C.c_void_p(ci_d + 4 * a), 4 * (b - a), None))
+        assert np.array_equal(cols.astype(np.int64), ciS[rpS[s]:rpS[s + 1]]), i
+        got = nval[a:b].cpu().numpy()
+        ref, scale = vS[rpS[s]:rpS[s + 1]], aS[rpS[s]:rpS[s + 1]]
+        assert np.all(np.abs(got - ref) <= 1e-12 * scale), (i, np.max(np.abs(got - ref) / scale))
+
+
+@pytest.mark.parametrize("shape", [(2000, 5000, 8, 0), (529, 1322, 6, 7), (3000, 6000, 40, 3)])
+def test_numeric_layouts_bit_identical(hn, torch_cuda, shape):
+    """The three numeric layouts (row mode, gather mode, relative map) give
+    the same bits, with inactive columns (d_j = 0) and three or more terms in
+    some slots; the last shape has rows of N long enough (>= 256 slots on
+    average) for the relative map to be the library's own choice."""
     m, n, k, seed = shape
     lp = lpgen.scaled_problem(lpgen.lp_uniform(m, n, k, seed))
     D = np.random.default_rng(seed).uniform(1e-3, 1e3, n)
@@ -141,17 +181,21 @@ def test_row_and_gather_modes_bit_identical(hn, torch_cuda, shape):
     A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
     Dd = torch_cuda.as_tensor(D, device="cuda")
     out = []
-    for compact in (True, False):
-        P = hn.Pattern(A, compact=compact)
-        assert P.mode()[0] == compact
+    for layout in (hn.Pattern.ROW, hn.Pattern.GATHER, hn.Pattern.RELATIVE):
+        P = hn.Pattern(A, layout=layout)
+        assert P.mode()[0] == layout
         nval = torch_cuda.empty(P.nnz, dtype=torch_cuda.float64, device="cuda")
         dyn = torch_cuda.empty(1, dtype=torch_cuda.float64, device="cuda")
         P.numeric(Dd, 1e-8, nval, dyn)
         torch_cuda.cuda.synchronize()
         out.append((P.export(), nval.cpu().numpy(), dyn.item()))
-    (p0, v0, d0), (p1, v1, d1) = out
-    assert np.array_equal(p0[0], p1[0]) and np.array_equal(p0[1], p1[1])
-    assert np.array_equal(v0, v1) and d0 == d1
+    (p0, v0, d0) = out[0]
+    for (p1, v1, d1) in out[1:]:
+        assert np.array_equal(p0[0], p1[0]) and np.array_equal(p0[1], p1[1])
+        assert np.array_equal(v0, v1) and d0 == d1
+    auto = hn.Pattern(A)
+    assert auto.mode()[0] == (hn.Pattern.RELATIVE if auto.nnz >= 256 * m else hn.Pattern.GATHER)
+    check_values(lp, D, 1e-8, p0[0].astype(np.int64), p0[1].astype(np.int64), v0, d0)
 
 
 def test_long_row_of_a_selects_gather_mode(hn, torch_cuda):
@@ -168,5 +212,5 @@ def test_long_row_of_a_selects_gather_mode(hn, torch_cuda):
     lp2 = dict(lp, rp=rp, ci=np.concatenate(rows).astype(np.int64), val=np.concatenate(vals))
     D = np.random.default_rng(5).uniform(0.1, 10, n)
     A, P, rp_, ci_, vals_, dyn = assemble(hn, torch_cuda, lp2, D, compact=True)
-    assert P.mode()[0] is False
+    assert P.mode()[0] != hn.Pattern.ROW
     check_values(lp2, D, 1e-8, rp_, ci_, vals_, dyn)

@@ -1,6 +1,6 @@
 """GPU: the drop-in at the reference's own seam. The reference's unchanged
 InteriorPointSolver::solve runs with InteriorPointOptions::compute_backend set
-to the B200 backend through the INTEGRATION.md adapter (oracle/dropin_adapter.cpp
+to the B200 backend through the maintainer-side adapter (oracle/dropin_adapter.cpp
 compiled against the reference sources). It must reach the reference's status
 and objective (golden, CPU backend) while its products run as GPU kernels."""
 import ctypes as C

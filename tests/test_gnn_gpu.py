@@ -134,3 +134,46 @@ def test_tcgen05_layer_matches_mma_sync_layer(hn, torch_cuda, K1, K2, relu, M):
     assert np.all(np.isfinite(ys[1]))
     scale = np.abs(ys[0]).max() + 1.0
     assert np.max(np.abs(ys[1] - ys[0])) <= 1e-5 * scale
+
+
+@pytest.mark.parametrize("polls", [1, 8])
+def test_tcgen05_wait_timeout_is_reported_and_the_context_recovers(hn, torch_cuda, polls):
+    """The tcgen05 layer's pipeline waits are bounded. With the test hook's
+    limit of a few polls, the first waits give up while the CTA's own bulk
+    copies are still in flight: the kernel records the timeout, settles those
+    copies (and any MMA it issued) with the full bound, frees TMEM and
+    returns; hn_gnn_check reports the error and clears it. Afterwards the
+    same call with the normal limit succeeds and matches the mma.sync layer:
+    nothing hung, nothing faulted, the context is usable."""
+    torch = torch_cuda
+    M, K1, K2 = 148 * 128 * 2 + 5, 64, 64
+    g = torch.Generator(device="cuda").manual_seed(7)
+    X1 = torch.randn((M, K1), generator=g, device="cuda")
+    X2 = torch.randn((M, K2), generator=g, device="cuda")
+    W = torch.randn(128 * 64, generator=g, device="cuda") / 128 ** 0.5
+    b = torch.randn(64, generator=g, device="cuda")
+    Wt = torch.empty(128 * 64, dtype=torch.bfloat16, device="cuda")
+    Wb = torch.empty(128 * 64, dtype=torch.bfloat16, device="cuda")
+    lib = hn.load()
+    hn.check(lib.hn_gnn_cast_weights(128, W.data_ptr(), Wt.data_ptr(), Wb.data_ptr(), None))
+    Y = torch.empty((M, 64), device="cuda")
+    hn.check(lib.hn_gnn_check(None))  # no stale flag
+    try:
+        hn.check(lib.hn_gnn_set_wait_limit(polls))
+        hn.check(lib.hn_gnn_linear_umma(M, K1, K2, X1.data_ptr(), X2.data_ptr(), Wt.data_ptr(), b.data_ptr(), 1,
+                                        Y.data_ptr(), None))
+        st = lib.hn_gnn_check(None)
+        assert st == hn.HN_ERR_CUDA, st
+        assert b"timed out" in lib.hn_last_error()
+    finally:
+        hn.check(lib.hn_gnn_set_wait_limit(0))
+    assert lib.hn_gnn_check(None) == hn.HN_OK  # the flag was cleared
+    ref = torch.empty((M, 64), device="cuda")
+    hn.check(lib.hn_gnn_linear(M, K1, K2, X1.data_ptr(), X2.data_ptr(), Wt.data_ptr(), 64, b.data_ptr(), 1,
+                               ref.data_ptr(), None))
+    hn.check(lib.hn_gnn_linear_umma(M, K1, K2, X1.data_ptr(), X2.data_ptr(), Wt.data_ptr(), b.data_ptr(), 1,
+                                    Y.data_ptr(), None))
+    hn.check(lib.hn_gnn_check(None))
+    torch.cuda.synchronize()
+    y, r = Y.cpu().numpy().astype(np.float64), ref.cpu().numpy().astype(np.float64)
+    assert np.max(np.abs(y - r)) <= 1e-5 * (np.abs(r).max() + 1.0)

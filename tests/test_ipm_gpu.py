@@ -300,4 +300,14 @@ def test_backend_residency_reused(hn):
     R.expect_close(y3, 2.0 * y1, 1e-12)
     t = be.spmv_t(rp, ci, val, np.ones(2000), 1500)
     R.expect_close(t, O.tmultiply(rp, ci, val, np.ones(2000), 1500), 1e-12)
+    # one entry rewritten, everything else identical (the C ABI copies into
+    # vectors the allocator hands back at the same address): still a new
+    # upload, for a value and for a column index alike
+    for k in (1, len(val) // 2 + 1, len(val) - 2):
+        v2 = val.copy()
+        v2[k] += 1.0
+        R.expect_close(be.spmv(rp, ci, v2, x), O.multiply(rp, ci, v2, x), 1e-12)
+        c2 = ci.copy()
+        c2[k] = (ci[k] + 7) % 1500
+        R.expect_close(be.spmv(rp, c2, val, x), O.multiply(rp, c2, val, x), 1e-12)
     be.close()

@@ -197,3 +197,20 @@ def test_port_matvec_t_and_max_step_match_reference_functions():
     v, d = rng.uniform(0.1, 2, 1000), rng.standard_normal(1000)
     assert O.max_step(v, d) == O.ref_max_step(v, d)
     assert O.max_step(v, np.abs(d)) == O.ref_max_step(v, np.abs(d)) == 0.99  # 0.99 * 1 when nothing blocks
+
+
+def test_port_normal_rows_equal_full_restatement():
+    """The row-restricted restatement (used at sizes whose triplet list does
+    not fit) gives the full restatement's rows bit for bit, including dyn_reg
+    taken over all rows and repeated / unordered row requests."""
+    lp = lpgen.scaled_problem(lpgen.lp_uniform(300, 750, 8, 3))
+    D = np.random.default_rng(1).uniform(0.1, 10, 750)
+    D[::13] = 0.0
+    rpN, ciN, vN, dyn = O.normal_equations(lp["rp"], lp["ci"], lp["val"], D, 1e-8, 750)
+    rows = np.array([5, 0, 299, 17, 17, 150])
+    rpS, ciS, vS, aS, dynS = O.normal_rows(lp["rp"], lp["ci"], lp["val"], D, 1e-8, 750, rows)
+    assert dynS == dyn
+    for s, i in enumerate(rows):
+        a, b, c, d = rpN[i], rpN[i + 1], rpS[s], rpS[s + 1]
+        assert np.array_equal(ciN[a:b], ciS[c:d]) and np.array_equal(vN[a:b], vS[c:d])
+        assert np.all(aS[c:d] >= np.abs(vS[c:d]))

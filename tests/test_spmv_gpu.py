@@ -166,3 +166,23 @@ def test_large_zipf_lp_parity(hn, torch_cuda, big_lp):
     at1 = run_spmv(hn, torch_cuda, A, ones, trans=1)
     lhs, rhs = y.sum(), at1 @ lp["x0"]
     assert abs(lhs - rhs) <= 1e-10 * (np.abs(val).sum() * 2.0)
+
+
+@pytest.mark.parametrize("kind,t", [(None, None), (0, 0), (1, 4), (1, 16)])
+def test_spec_literal_zipf_lp_parity(hn, torch_cuda, kind, t):
+    """The spec-literal large LP: m 200k, n 500k, Zipf(1.5) column counts on
+    [1, 2000] without rescaling (about 17M nonzeros). y = A x and A^T y on the
+    autotuned path and on each path pinned, normwise 1e-12 against the
+    oracle's multiply / matvec_t."""
+    lp = lpgen.lp_zipf(seed=1000, target_nnz=None)
+    rp, ci, val = lp["rp"], lp["ci"], lp["val"]
+    A = hn.Csr(lp["m"], lp["n"], rp, ci, val)
+    assert A.nnz > 15_000_000
+    if kind is not None:
+        A.set_spmv_kind(kind, t, trans=0)
+        A.set_spmv_kind(kind, t, trans=1)
+    y = run_spmv(hn, torch_cuda, A, lp["x0"])
+    R.normwise_close(y, O.multiply(rp, ci, val, lp["x0"]), rp, ci, val, lp["x0"])
+    yt = run_spmv(hn, torch_cuda, A, lp["y0"], trans=1)
+    rpT, ciT, valT = O.transposed(rp, ci, val, lp["n"])
+    R.normwise_close(yt, O.matvec_t(rp, ci, val, lp["y0"], lp["n"]), rpT, ciT, valT, lp["y0"])
