@@ -312,10 +312,15 @@ int hn_batch_residuals(hn_batch* B, const hn_csr* M, const double* x_dev, const 
  * extra_iterations more iterations have run; hn_batch_finish then puts the
  * saved iterate back where the later one is worse or failed. kkt_tol <= 0:
  * the reference's rule alone (the residual is still measured when ru_dev is
- * given). The arrays are caller-owned and must stay valid while the batch
- * iterates. Resets the per-instance records. */
+ * given). max_iterations > 0: the reference's iteration limit; at iteration
+ * max_iterations an instance its strict rule has not accepted is accepted
+ * by the relaxed rule of interior_point.cpp:727-753 (residuals and mu below
+ * 1e-4) -- and then tightened like the others -- or stops there with status
+ * 6 (the loop may then run up to extra_iterations past the limit). The
+ * arrays are caller-owned and must stay valid while the batch iterates.
+ * Resets the per-instance records. */
 int hn_batch_set_kkt(hn_batch* B, const double* ru_dev, const double* cu_dev, const double* offset_dev,
-                     double kkt_tol, int extra_iterations);
+                     double kkt_tol, int extra_iterations, int max_iterations);
 /* kkt_host: K x 4 (as hn_ipm_kkt's kkt_dev) at the last hn_batch_residuals
  * call, or after hn_batch_finish the residual of the returned iterate;
  * ref_iter_host: K, the iteration at which the reference's rule first held

@@ -72,6 +72,7 @@ struct hn_batch {
     const double *ru = nullptr, *cu = nullptr, *offset = nullptr;
     double kkt_tol = 0.0;
     int kkt_extra = 0;
+    int kkt_max_it = 0x7fffffff;  // the reference's iteration limit (its relaxed acceptance applies there)
     double *kkt = nullptr, *kkt_ref = nullptr;
     int32_t* ref_iter = nullptr;
     double *xb = nullptr, *zb = nullptr, *lb = nullptr;
@@ -96,7 +97,9 @@ struct KktArgs {
     int32_t* ref_iter;
     double tol;
     int extra;
+    int max_it;
 };
+constexpr int ST_LIMIT = 6;  // stopped at the reference's iteration limit without its acceptance
 
 __device__ __forceinline__ double fin_or_inf(double t) { return t <= 1.7976931348623157e308 ? t : INFINITY; }
 
@@ -170,7 +173,11 @@ __global__ void __launch_bounds__(kT) batch_prep_kernel(const int64_t* __restric
         int save = 0;
         if (status[i] == ST_RUN) {
             int r = k.ref_iter[i];
-            if (r < 0 && mrp < tol && mrd < tol && mu < ctol) {  // the reference's rule, :525-530
+            // the reference's rule (:525-530), or at its iteration limit its
+            // relaxed acceptance (:727-753)
+            const bool strict = mrp < tol && mrd < tol && mu < ctol;
+            const bool relaxed = iter >= k.max_it && mrp < 1e-4 && mrd < 1e-4 && mu < 1e-4;
+            if (r < 0 && (strict || relaxed)) {
                 r = iter;
                 k.ref_iter[i] = iter;
                 save = measure && k.tol > 0.0;
@@ -182,6 +189,8 @@ __global__ void __launch_bounds__(kT) batch_prep_kernel(const int64_t* __restric
             if (r >= 0 && (!(measure && k.tol > 0.0) || kk <= k.tol || iter - r >= k.extra)) {
                 status[i] = ST_OPTIMAL;
                 iters[i] = iter;
+            } else if (r < 0 && iter >= k.max_it) {
+                status[i] = ST_LIMIT;  // where the reference stops unaccepted
             }
         }
         s_save = save;
@@ -879,7 +888,7 @@ void free_batch(hn_batch* B) {
 
 KktArgs kkt_args(const hn_batch* B, const double* lam, const double* b, const double* c) {
     return KktArgs{lam,    b,      c,      B->ru,  B->cu,       B->offset, B->kkt,
-                   B->kkt_ref, B->xb, B->zb, B->lb, B->ref_iter, B->kkt_tol, B->kkt_extra};
+                   B->kkt_ref, B->xb, B->zb, B->lb, B->ref_iter, B->kkt_tol, B->kkt_extra, B->kkt_max_it};
 }
 
 SpmvMat n_mat(const hn_batch* B, const double* nval) {
@@ -1051,7 +1060,7 @@ int hn_batch_residuals(hn_batch* B, const hn_csr* M, const double* x, const doub
 }
 
 int hn_batch_set_kkt(hn_batch* B, const double* ru, const double* cu, const double* offset, double kkt_tol,
-                     int extra_iterations) {
+                     int extra_iterations, int max_iterations) {
     return guard("hn_batch_set_kkt", [&] {
         require_init();
         if (!B || (ru == nullptr) != (cu == nullptr) || (ru && !offset) || extra_iterations < 0)
@@ -1062,6 +1071,7 @@ int hn_batch_set_kkt(hn_batch* B, const double* ru, const double* cu, const doub
         B->offset = offset;
         B->kkt_tol = kkt_tol > 0.0 ? kkt_tol : 0.0;
         B->kkt_extra = extra_iterations;
+        B->kkt_max_it = max_iterations > 0 ? max_iterations : 0x7fffffff;
         if (B->kkt_tol > 0.0 && !B->xb) {
             B->xb = dmalloc<double>(B->n);
             B->zb = dmalloc<double>(B->n);

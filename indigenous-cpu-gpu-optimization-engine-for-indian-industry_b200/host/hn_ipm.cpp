@@ -684,7 +684,9 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
             result.solve_ms += ms_since(t);
         };
 
-        const std::size_t max_it = static_cast<std::size_t>(O.max_iterations);
+        // past the reference's limit the loop runs only while tightening
+        const std::size_t ref_max_it = static_cast<std::size_t>(std::max(O.max_iterations, 0));
+        const std::size_t max_it = ref_max_it + (tighten ? static_cast<std::size_t>(O.kkt_extra_iterations) : 0);
         std::size_t iter = 0;
         for (iter = 0; iter < max_it; ++iter) {
             if (O.interrupt_callback && O.interrupt_callback()) {
@@ -702,8 +704,13 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
             read_scal();
             measure();
             const double mu = sc[HN_IPM_MU];
-            if (ref_iter < 0 && sc[HN_IPM_NRP] < O.convergence_tol && sc[HN_IPM_NRD] < O.convergence_tol &&
-                mu < O.complementarity_tol) {  // the reference's rule (:525-530)
+            const bool strict =
+                sc[HN_IPM_NRP] < O.convergence_tol && sc[HN_IPM_NRD] < O.convergence_tol && mu < O.complementarity_tol;
+            // at the reference's limit its relaxed acceptance (:727-753)
+            const bool relaxed =
+                iter >= ref_max_it && sc[HN_IPM_NRP] < 1e-4 && sc[HN_IPM_NRD] < 1e-4 && mu < 1e-4;
+            if (ref_iter < 0 && iter >= ref_max_it && !relaxed) break;  // the reference stops here unaccepted
+            if (ref_iter < 0 && (strict || relaxed)) {  // the reference's rule (:525-530)
                 ref_iter = (long)iter;
                 std::memcpy(kref, kv, sizeof(kv));
                 if (tighten) {

@@ -20,6 +20,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -200,6 +201,10 @@ std::vector<int> amd_order(int n, const std::vector<int>& rp, const std::vector<
 
 // ---- symbolic analysis ----
 void SparseLDLT::analyze(std::size_t m, const uint64_t* rp, const uint64_t* ci) {
+    // the ordering and the symbolic analysis index rows and entries with int
+    if (m > static_cast<std::size_t>(INT_MAX) || rp[m] > static_cast<uint64_t>(INT_MAX))
+        throw std::invalid_argument("SparseLDLT: " + std::to_string(m) + " rows / " + std::to_string(rp[m]) +
+                                    " entries exceed the 2^31 - 1 index range");
     m_ = m;
     const int n = static_cast<int>(m);
     std::vector<int> rp32(m + 1), ci32(rp[m]);
@@ -358,22 +363,32 @@ namespace {
 // of a front are never read.
 void trailing_update(double* F, std::size_t nf, std::size_t kb, std::size_t ke, const double* D) {
     const std::size_t nbk = ke - kb, t = nf - ke, tp = (t + 7) & ~std::size_t(7);
-    std::vector<double> LT(nbk * tp, 0.0), C(tp * nbk, 0.0);  // LT[k][i] = L(ke+i, kb+k), C[j][k] = L(ke+j, kb+k) D_k
+    // LT[k][i] = L(ke+i, kb+k), C[j][k] = L(ke+j, kb+k) D_k, padded to tp rows
+    // with zeros; per-thread buffers reused across panels and fronts
+    thread_local std::vector<double> LT, C;
+    if (LT.size() < nbk * tp) LT.resize(nbk * tp);
+    if (C.size() < tp * nbk) C.resize(tp * nbk);
     for (std::size_t k = 0; k < nbk; ++k) {
         const double* lk = F + (kb + k) * nf + ke;
         std::memcpy(LT.data() + k * tp, lk, sizeof(double) * t);
+        std::fill(LT.data() + k * tp + t, LT.data() + (k + 1) * tp, 0.0);
         for (std::size_t j = 0; j < t; ++j) C[j * nbk + k] = lk[j] * D[kb + k];
     }
+    std::fill(C.data() + t * nbk, C.data() + tp * nbk, 0.0);
+    // the parallel loop reads the calling thread's buffers through these
+    // (a thread_local name inside the region would be each worker's own)
+    const double* const LTp = LT.data();
+    const double* const Cp = C.data();
     const std::size_t nj = (t + 3) / 4;
     const bool par = t * t * nbk > (std::size_t(1) << 21);
 #pragma omp parallel for schedule(dynamic, 2) if (par)
     for (std::size_t jb = 0; jb < nj; ++jb) {
         const std::size_t j0 = jb * 4, nc = std::min<std::size_t>(4, t - j0);
-        const double* c0 = C.data() + j0 * nbk;
+        const double* c0 = Cp + j0 * nbk;
         for (std::size_t i0 = j0 & ~std::size_t(7); i0 < t; i0 += 8) {
             double acc[4][8] = {};
             for (std::size_t k = 0; k < nbk; ++k) {
-                const double* l = LT.data() + k * tp + i0;
+                const double* l = LTp + k * tp + i0;
                 for (std::size_t jj = 0; jj < 4; ++jj) {
                     const double c = c0[jj * nbk + k];
 #pragma omp simd

@@ -143,3 +143,24 @@ def test_tiny_sizes(hn, m):
     rp, ci, v = csr(M)
     x, st = hn.sparse_ldlt_solve(rp, ci, v, np.ones(m))
     assert np.allclose(x, 0.5)
+
+
+@pytest.mark.parametrize("name,build", [("normal3000", lambda: normal_matrix(3000, 7500, 11)),
+                                        ("grid150", lambda: grid(150))])
+def test_parallel_front_and_subtree_paths(hn, name, build):
+    """Matrices large enough for the multithreaded paths: fronts wider than
+    ~256 columns (the parallel trailing update of a front, here the
+    3,000-row normal matrix of a random LP, which fills almost densely) and
+    many independent subtrees (the 150 x 150 grid). Residuals as the smaller
+    cases; the host library runs with the process's OpenMP threads (all cores
+    unless OMP_NUM_THREADS says otherwise)."""
+    M = build()
+    rp, ci, v = csr(M)
+    rng = np.random.default_rng(1)
+    B = rng.standard_normal((2, M.shape[0]))
+    X, st = hn.sparse_ldlt_solve(rp, ci, v, B)
+    assert not st["singular"]
+    for b, x in zip(B, X):
+        assert np.linalg.norm(M @ x - b) <= 1e-10 * np.linalg.norm(b) * max(1.0, np.abs(M).max())
+    if name == "grid150":
+        assert st["supernodes"] > 1000
