@@ -347,9 +347,10 @@ __global__ void __launch_bounds__(kT, 4) ada_slot_kernel(int64_t nnz, const uint
 // (ecs[e] + low bits); (A value x A^T value) x d is the slot kernel's
 // arithmetic, so the layouts give the same bits. The row's A entries are
 // read through L1 (a row of A is a few cache lines, reused by every slot of
-// the row); the A^T values come from L2; the map streams from HBM once.
-constexpr int kRmapU = 4;
-__global__ void __launch_bounds__(kT, 4) ada_rmap_kernel(int m, const int32_t* __restrict__ order,
+// the row); the A^T values are gathered from L2 without allocating in L1
+// (they would evict the row's entries); the map streams from HBM once.
+constexpr int kRmapU = 8;
+__global__ void __launch_bounds__(kT, 3) ada_rmap_kernel(int m, const int32_t* __restrict__ order,
                                                          unsigned* __restrict__ row_next,
                                                          const int32_t* __restrict__ rpA,
                                                          const double2* __restrict__ vd,
@@ -399,7 +400,7 @@ __global__ void __launch_bounds__(kT, 4) ada_rmap_kernel(int m, const int32_t* _
                 if (g[u] & kMulti)
                     b[u] = t < r1 ? __ldcs(mval + ms0 + (g[u] & ~kMulti)) : 0.0;
                 else
-                    b[u] = __ldg(valT + cs[u] + static_cast<int>(g[u] & qmask));
+                    b[u] = __ldcg(valT + cs[u] + static_cast<int>(g[u] & qmask));
             }
 #pragma unroll
             for (int u = 0; u < kRmapU; ++u) {
@@ -593,7 +594,7 @@ void launch_numeric(const hn_pattern* P, const double* d, double* nval, cudaStre
     }
     if (P->rmap) {
         check_cuda(cudaMemsetAsync(P->row_next, 0, sizeof(unsigned), s), "memset row counter");
-        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P->m + 7) / 8, (int64_t)ctx().sm_count * 4));
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P->m + 7) / 8, (int64_t)ctx().sm_count * 3));
         ada_rmap_kernel<<<grid, kT, 0, s>>>((int)P->m, P->order, P->row_next, A->rp, P->vd, P->ecs, A->valT, P->rp,
                                             P->msrow, P->rmap, P->qbits, P->mval, nval);
         launched("ada_rmap_kernel");

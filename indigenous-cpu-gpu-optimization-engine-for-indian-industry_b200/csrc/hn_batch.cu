@@ -76,6 +76,7 @@ struct hn_batch {
     double *kkt = nullptr, *kkt_ref = nullptr;
     int32_t* ref_iter = nullptr;
     double *xb = nullptr, *zb = nullptr, *lb = nullptr;
+    double* dyn = nullptr;  // K: each instance's dyn_reg of the current factorisation
 };
 
 namespace hn {
@@ -85,6 +86,10 @@ constexpr int kT = 256;
 constexpr int S_NRP = HN_IPM_NRP, S_NRD = HN_IPM_NRD, S_MU = HN_IPM_MU, S_AP = HN_IPM_AP, S_AD = HN_IPM_AD,
               S_MUAFF = HN_IPM_MUAFF, S_SIGMA = HN_IPM_SIGMA;
 constexpr int ST_RUN = 0, ST_OPTIMAL = 1, ST_NUMERICAL = 7;
+
+// Row stride of an instance's dense block: m rounded up to even, so every row
+// starts on a 16-byte boundary (16-byte asynchronous copies of the panels).
+__host__ __device__ __forceinline__ int dense_ld(int m) { return (m + 1) & ~1; }
 
 __device__ __forceinline__ bool fin(double v) { return isfinite(v); }
 
@@ -350,7 +355,8 @@ __global__ void __launch_bounds__(kT) batch_update_kernel(const int64_t* __restr
 // ---- normal equations per instance ----
 __global__ void __launch_bounds__(kT) batch_reg_kernel(const int64_t* __restrict__ row_off,
                                                        const int64_t* __restrict__ diag_pos, double reg,
-                                                       const int32_t* __restrict__ status, double* __restrict__ nval) {
+                                                       const int32_t* __restrict__ status, double* __restrict__ nval,
+                                                       double* __restrict__ dyn_out) {
     __shared__ double sh[32];
     __shared__ double s_dyn;
     const int64_t i = blockIdx.x;
@@ -362,6 +368,7 @@ __global__ void __launch_bounds__(kT) batch_reg_kernel(const int64_t* __restrict
     if (threadIdx.x == 0) {
         const double dyn = 1e-12 * md;
         s_dyn = (reg < dyn) ? dyn : reg;  // std::max(regularization, 1e-12 * max_diag)
+        dyn_out[i] = s_dyn;
     }
     __syncthreads();
     const double dyn = s_dyn;
@@ -379,7 +386,7 @@ __global__ void batch_dense_kernel(int64_t m, const int64_t* __restrict__ row_of
     const int inst = row_inst[r];
     if (status[inst] != ST_RUN) return;
     const int64_t b0 = row_off[inst], mi = row_off[inst + 1] - b0, lr = r - b0;
-    double* row = dense + dn_off[inst] + lr * mi;
+    double* row = dense + dn_off[inst] + lr * dense_ld(static_cast<int>(mi));
     for (int64_t c = lane; c <= lr; c += 32) row[c] = 0.0;
     __syncwarp();
     for (int64_t p = rpN[r] + lane; p < rpN[r + 1]; p += 32) {
@@ -424,13 +431,14 @@ __global__ void __launch_bounds__(kT) batch_ldlt_diag_kernel(int s, const int64_
     if (status[inst] != ST_RUN) return;
     const int64_t r0 = row_off[inst];
     const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int ld = dense_ld(m);
     const int k0 = s * kFb;
     if (k0 >= m) return;
     const int nb = min(kFb, m - k0);
     double* A = dense + dn_off[inst];
     for (int idx = tid; idx < kFb * kFb; idx += kT) {
         const int r = idx / kFb, c = idx % kFb;
-        sA[r][c] = (r < nb && c <= r) ? A[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
+        sA[r][c] = (r < nb && c <= r) ? A[(int64_t)(k0 + r) * ld + k0 + c] : 0.0;
     }
     __syncthreads();
     for (int j = 0; j < nb; ++j) {
@@ -451,7 +459,7 @@ __global__ void __launch_bounds__(kT) batch_ldlt_diag_kernel(int s, const int64_
     }
     for (int idx = tid; idx < nb * nb; idx += kT) {
         const int r = idx / nb, c = idx % nb;
-        if (c < r) A[(int64_t)(k0 + r) * m + k0 + c] = sA[r][c];
+        if (c < r) A[(int64_t)(k0 + r) * ld + k0 + c] = sA[r][c];
     }
     if (tid < nb) dD[r0 + k0 + tid] = sD[tid];
 }
@@ -482,19 +490,20 @@ __global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, int cnt, co
     const int64_t local = chunk - (lo > 0 ? chunks[lo - 1] : 0);
     const int64_t r0 = row_off[inst];
     const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int ld = dense_ld(m);
     const int k0 = s * kFb;
     const int nb = min(kFb, m - k0), k1 = k0 + nb;
     double* A = dense + dn_off[inst];
     for (int idx = tid; idx < kFb * kFb; idx += kT) {
         const int r = idx / kFb, c = idx % kFb;
-        sL[r][c] = (r < nb && c < r) ? A[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
+        sL[r][c] = (r < nb && c < r) ? A[(int64_t)(k0 + r) * ld + k0 + c] : 0.0;
     }
     if (tid < kFb) sD[tid] = tid < nb ? dD[r0 + k0 + tid] : 1.0;
     __syncthreads();
     const int r = k1 + static_cast<int>(local) * kT + tid;
     if (r >= m) return;
     double lv[kFb];
-    double* Ar = A + (int64_t)r * m + k0;
+    double* Ar = A + (int64_t)r * ld + k0;
 #pragma unroll
     for (int c = 0; c < kFb; ++c) lv[c] = (c < nb) ? Ar[c] : 0.0;
 #pragma unroll
@@ -511,7 +520,23 @@ __global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, int cnt, co
         if (c < nb) Ar[c] = lv[c];
 }
 
-__global__ void __launch_bounds__(kT, 4) batch_ldlt_update_kernel(int s, int cnt, int64_t npairs,
+// Trailing update of one 64 x 64 tile pair per CTA iteration. Both 64-column
+// panel slices arrive by 16-byte asynchronous copies (rows start on 16-byte
+// boundaries: even row stride), in two commit groups of 32 columns, so the
+// second half is in flight while the first is multiplied. D is applied at the
+// fragment load: a = L[r, k] D_k rounds once, as a staged product would, and
+// every output fragment takes the same DMMA sequence (k ascending in steps of
+// 4), so the result does not depend on the staging.
+constexpr int kUpdP = kFb + 4;  // smem row stride: a half-warp's fragment loads hit 16 distinct bank pairs
+constexpr size_t kUpdSmem = sizeof(double) * (2 * kFb * kUpdP + kFb);
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(kT, 3) batch_ldlt_update_kernel(int s, int cnt, int64_t npairs,
                                                                const int64_t* __restrict__ pairs,
                                                                const int64_t* __restrict__ row_off,
                                                                const int64_t* __restrict__ dn_off,
@@ -519,14 +544,10 @@ __global__ void __launch_bounds__(kT, 4) batch_ldlt_update_kernel(int s, int cnt
                                                                const int32_t* __restrict__ status,
                                                                double* __restrict__ dense,
                                                                const double* __restrict__ dD) {
-    // row-major copies of the two panel slices, kFb / 2 columns at a time:
-    // sW[r][q] = L[rb+r, k0+kh+q] D_(kh+q), sL[c][q] = L[cb+c, k0+kh+q].
-    // A warp stages one row (32 consecutive doubles: conflict-free stores);
-    // the row stride of 36 doubles puts a half-warp's fragment loads (row
-    // l/4, k = l%4) on 16 distinct bank pairs.
-    constexpr int kUP = kFb / 2 + 4;
-    __shared__ double sW[kFb][kUP];
-    __shared__ double sL[kFb][kUP];
+    extern __shared__ __align__(16) double upd_smem[];
+    double(*sW)[kUpdP] = reinterpret_cast<double(*)[kUpdP]>(upd_smem);                // L[rb + r, k0 + k]
+    double(*sL)[kUpdP] = reinterpret_cast<double(*)[kUpdP]>(upd_smem + kFb * kUpdP);  // L[cb + c, k0 + k]
+    double* sD = upd_smem + 2 * kFb * kUpdP;
     const int tid = threadIdx.x;
     const int k0 = s * kFb;
     int lo = 0;  // the instance of the previous pair: pairs arrive in increasing order
@@ -554,14 +575,30 @@ __global__ void __launch_bounds__(kT, 4) batch_ldlt_update_kernel(int s, int cnt
         const int64_t local = pidx - (lo > 0 ? pairs[lo - 1] : 0);
         const int64_t r0 = row_off[inst];
         const int m = static_cast<int>(row_off[inst + 1] - r0);
-        const int nb = min(kFb, m - k0), k1 = k0 + nb;
+        const int ld = dense_ld(m);
+        // a trailing part exists only below a full block: nb = kFb here
+        const int k1 = k0 + kFb;
         int ti = static_cast<int>((sqrt(8.0 * (double)local + 1.0) - 1.0) * 0.5);
         while ((int64_t)(ti + 1) * (ti + 2) / 2 <= local) ++ti;
         while ((int64_t)ti * (ti + 1) / 2 > local) --ti;
         const int tj = static_cast<int>(local - (int64_t)ti * (ti + 1) / 2);
         const int rb = k1 + ti * kFb, cb = k1 + tj * kFb;
         double* A = dense + dn_off[inst];
-        const double* Dv = dD + r0 + k0;
+        __syncthreads();  // the previous pair's fragment loads are done with the buffers
+        // 2 slices x 64 rows x 16 chunks of 16 bytes per half; rows past m are zero-filled
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            for (int idx = tid; idx < 2 * kFb * 16; idx += kT) {
+                const int side = idx >> 10, rr = (idx >> 4) & (kFb - 1), q2 = idx & 15;
+                const int row = (side ? cb : rb) + rr;
+                const bool ok = row < m;
+                const double* src = A + (int64_t)(ok ? row : rb) * ld + k0 + h * 32 + 2 * q2;
+                double* dst = (side ? sL[rr] : sW[rr]) + h * 32 + 2 * q2;
+                cp_async16(dst, src, ok);
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+        }
+        if (tid < kFb) sD[tid] = dD[r0 + k0 + tid];
         // warp w: rows 16 (w >> 1) .. + 16 (two 8-row tiles), columns
         // 32 (w & 1) .. + 32 (four 8-column tiles) of the 64 x 64 output
         const int lane = tid & 31, warp = tid >> 5;
@@ -572,20 +609,19 @@ __global__ void __launch_bounds__(kT, 4) batch_ldlt_update_kernel(int s, int cnt
         for (int i = 0; i < 2; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-        for (int kh = 0; kh < kFb; kh += kFb / 2) {
-            __syncthreads();
-            for (int idx = tid; idx < kFb * (kFb / 2); idx += kT) {
-                const int rr = idx / (kFb / 2), q = idx % (kFb / 2);
-                const bool okr = rb + rr < m && kh + q < nb, okc = cb + rr < m && kh + q < nb;
-                sW[rr][q] = okr ? A[(int64_t)(rb + rr) * m + k0 + kh + q] * Dv[kh + q] : 0.0;
-                sL[rr][q] = okc ? A[(int64_t)(cb + rr) * m + k0 + kh + q] : 0.0;
-            }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (h == 0)
+                asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+            else
+                asm volatile("cp.async.wait_group 0;\n" ::: "memory");
             __syncthreads();
 #pragma unroll
-            for (int kq = 0; kq < kFb / 2; kq += 4) {
+            for (int kq = h * 32; kq < h * 32 + 32; kq += 4) {
+                const double dk = sD[kq + fk];
                 double a[2], b[4];
 #pragma unroll
-                for (int i = 0; i < 2; ++i) a[i] = sW[wr + 8 * i + fr][kq + fk];  // A(8x4)[fr][fk]
+                for (int i = 0; i < 2; ++i) a[i] = sW[wr + 8 * i + fr][kq + fk] * dk;  // A(8x4)[fr][fk]
 #pragma unroll
                 for (int j = 0; j < 4; ++j) b[j] = sL[wc + 8 * j + fr][kq + fk];  // B(4x8)[fk][fr]
 #pragma unroll
@@ -594,7 +630,6 @@ __global__ void __launch_bounds__(kT, 4) batch_ldlt_update_kernel(int s, int cnt
                     for (int j = 0; j < 4; ++j) dmma_m8n8k4(acc[i][j], a[i], b[j]);
             }
         }
-        // D(8x8)[fr][2 fk + t]
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
             const int gr = rb + wr + 8 * i + fr;
@@ -604,7 +639,7 @@ __global__ void __launch_bounds__(kT, 4) batch_ldlt_update_kernel(int s, int cnt
 #pragma unroll
                 for (int t = 0; t < 2; ++t) {
                     const int gc = cb + wc + 8 * j + 2 * fk + t;
-                    if (gc <= gr) A[(int64_t)gr * m + gc] -= acc[i][j][t];
+                    if (gc <= gr) A[(int64_t)gr * ld + gc] -= acc[i][j][t];
                 }
             }
         }
@@ -650,6 +685,7 @@ __global__ void __launch_bounds__(kFb) batch_fwd_diag_kernel(int s, const int64_
     if (!solving(status, refine, inst)) return;
     const int64_t r0 = row_off[inst];
     const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int ld = dense_ld(m);
     const int k0 = s * kFb;
     if (k0 >= m) return;
     const int nb = min(kFb, m - k0);
@@ -658,7 +694,7 @@ __global__ void __launch_bounds__(kFb) batch_fwd_diag_kernel(int s, const int64_
     const int i = threadIdx.x;
     for (int idx = i; idx < kFb * kFb; idx += kFb) {
         const int r = idx / kFb, c = idx % kFb;
-        sL[r][c] = (r < nb && c < r) ? L[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
+        sL[r][c] = (r < nb && c < r) ? L[(int64_t)(k0 + r) * ld + k0 + c] : 0.0;
     }
     double v = i < nb ? x[k0 + i] : 0.0;
     __syncthreads();
@@ -685,6 +721,7 @@ __global__ void __launch_bounds__(kT) batch_fwd_gemv_kernel(int s, int cnt, cons
     const int64_t local = blockIdx.x - (b > 0 ? chunks[b - 1] : 0);
     const int64_t r0 = row_off[inst];
     const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int ld = dense_ld(m);
     const int k0 = s * kFb;
     const int nb = min(kFb, m - k0), k1 = k0 + nb;
     const double* L = dense + dn_off[inst];
@@ -699,7 +736,7 @@ __global__ void __launch_bounds__(kT) batch_fwd_gemv_kernel(int s, int cnt, cons
             const int r = rw + u;
             double a = 0.0;
             if (r < re) {
-                const double* Lr = L + (int64_t)r * m + k0;
+                const double* Lr = L + (int64_t)r * ld + k0;
                 const double p0 = lane < nb ? Lr[lane] * sx[lane] : 0.0;
                 const double p1 = lane + 32 < nb ? Lr[lane + 32] * sx[lane + 32] : 0.0;
                 a = p0 + p1;
@@ -744,6 +781,7 @@ __global__ void __launch_bounds__(kT) batch_bwd_gemv_kernel(int s, int cnt, cons
     const int64_t local = blockIdx.x - (b > 0 ? chunks[b - 1] : 0);
     const int64_t r0 = row_off[inst];
     const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int ld = dense_ld(m);
     const int k0 = s * kFb;
     const int nb = min(kFb, m - k0), k1 = k0 + nb;
     const double* L = dense + dn_off[inst];
@@ -751,7 +789,7 @@ __global__ void __launch_bounds__(kT) batch_bwd_gemv_kernel(int s, int cnt, cons
     const int rb = k1 + static_cast<int>(local) * kT, re = min(m, rb + kT);
     double a0 = 0.0, a1 = 0.0;
     for (int c = rb + warp; c < re; c += kT / 32) {
-        const double* Lc = L + (int64_t)c * m + k0;
+        const double* Lc = L + (int64_t)c * ld + k0;
         const double xc = x[c];
         if (lane < nb) a0 += Lc[lane] * xc;
         if (lane + 32 < nb) a1 += Lc[lane + 32] * xc;
@@ -782,6 +820,7 @@ __global__ void __launch_bounds__(kFb) batch_bwd_diag_kernel(int s, const int64_
     if (!solving(status, refine, inst)) return;
     const int64_t r0 = row_off[inst];
     const int m = static_cast<int>(row_off[inst + 1] - r0);
+    const int ld = dense_ld(m);
     const int k0 = s * kFb;
     if (k0 >= m) return;
     const int nb = min(kFb, m - k0);
@@ -790,7 +829,7 @@ __global__ void __launch_bounds__(kFb) batch_bwd_diag_kernel(int s, const int64_
     const int q = threadIdx.x;
     for (int idx = q; idx < kFb * kFb; idx += kFb) {
         const int r = idx / kFb, c = idx % kFb;
-        sL[r][c] = (r < nb && c < r) ? L[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
+        sL[r][c] = (r < nb && c < r) ? L[(int64_t)(k0 + r) * ld + k0 + c] : 0.0;
     }
     const int64_t c0 = b > 0 ? chunks[b - 1] : 0, c1 = chunks[b];
     double t = 0.0;
@@ -809,18 +848,27 @@ __global__ void __launch_bounds__(kFb) batch_bwd_diag_kernel(int s, const int64_
 // Refinement bookkeeping per instance (refinement.cpp:15-30): with r = rhs - N x,
 // rel = max|r| / max|rhs|; an instance keeps sweeping while rel > 1e-10 and
 // sweeps remain; a sweeping instance's r is then solved and added to x.
+// In the tightening phase (an instance the reference's rule has accepted,
+// unreg != 0) the residual is taken against N without its dyn_reg: the
+// regularised system leaves M dx = -rp - dyn_reg dlam, a floor of about
+// dyn_reg |dlam| under the primal residual, which refinement against the
+// unregularised N (the regularised factor as its preconditioner) removes.
 __global__ void __launch_bounds__(kT) batch_refine_check_kernel(const int64_t* __restrict__ row_off,
                                                                 const int32_t* __restrict__ status,
                                                                 const double* __restrict__ rhs,
                                                                 const double* __restrict__ ax, double* __restrict__ r,
-                                                                int32_t* __restrict__ refine, int32_t* nref) {
+                                                                int32_t* __restrict__ refine, int32_t* nref,
+                                                                const double* __restrict__ x,
+                                                                const double* __restrict__ dyn,
+                                                                const int32_t* __restrict__ ref_iter, int unreg) {
     __shared__ double sh[32];
     const int64_t i = blockIdx.x;
     if (status[i] != ST_RUN || !refine[i]) return;
     const int64_t r0 = row_off[i], r1 = row_off[i + 1];
+    const double shift = (unreg && ref_iter[i] >= 0) ? dyn[i] : 0.0;
     double nb = 0.0, nr = 0.0;
     for (int64_t k = r0 + threadIdx.x; k < r1; k += kT) {
-        const double b = rhs[k], d = b - ax[k];
+        const double b = rhs[k], d = shift != 0.0 ? b - (ax[k] - shift * x[k]) : b - ax[k];
         nb = fmax(nb, fabs(b));
         nr = fmax(nr, fabs(d));
         r[k] = d;
@@ -881,7 +929,7 @@ void free_batch(hn_batch* B) {
                     (void*)B->tile_row, (void*)B->tile_nz, (void*)B->carry_row, (void*)B->head_row,
                     (void*)B->carry_val, (void*)B->head_val, (void*)B->r, (void*)B->ax, (void*)B->step_pairs, (void*)B->step_chunks,
                     (void*)B->solve_part, (void*)B->kkt, (void*)B->kkt_ref, (void*)B->ref_iter, (void*)B->xb,
-                    (void*)B->zb, (void*)B->lb})
+                    (void*)B->zb, (void*)B->lb, (void*)B->dyn})
         dfree(p);
     delete B;
 }
@@ -947,7 +995,7 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
             const int64_t mi = row_off_host[i + 1] - row_off_host[i];
             const int64_t ni = col_off_host[i + 1] - col_off_host[i];
             if (mi < 1 || ni < 1) fail(HN_ERR_INVALID_ARG, "every instance needs a row and a column");
-            dn[i + 1] = dn[i] + mi * mi;
+            dn[i + 1] = dn[i] + mi * dense_ld(static_cast<int>(mi));
             order[i] = static_cast<int32_t>(i);
         }
         std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
@@ -972,7 +1020,12 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
             B->r = dmalloc<double>(m);
             B->ax = dmalloc<double>(m);
             B->nrp = dmalloc<int32_t>(m + 1);
+            check_cuda(cudaFuncSetAttribute(batch_ldlt_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kUpdSmem),
+                       "update smem attribute");
             B->ref_iter = dmalloc<int32_t>(K);
+            B->dyn = dmalloc<double>(K);
+            check_cuda(cudaMemsetAsync(B->dyn, 0, sizeof(double) * K, s), "memset");
             B->kkt = dmalloc<double>(4 * K);
             B->kkt_ref = dmalloc<double>(4 * K);
             check_cuda(cudaMemsetAsync(B->ref_iter, 0xff, sizeof(int32_t) * K, s), "memset");  // -1
@@ -1114,7 +1167,7 @@ int hn_batch_factor(hn_batch* B, const double* D, double reg, double singular_to
         if (!B || !D || !nval || !status) fail(HN_ERR_INVALID_ARG, "bad arguments");
         cudaStream_t s = as_stream(stream);
         ada_numeric_unregularised(B->P, D, nval, s);
-        batch_reg_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, B->P->diag_pos, reg, status, nval);
+        batch_reg_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, B->P->diag_pos, reg, status, nval, B->dyn);
         launched("batch_reg_kernel");
         batch_dense_kernel<<<(unsigned)((B->m * 32 + 255) / 256), 256, 0, s>>>(
             B->m, B->row_off, B->row_inst, B->dn_off, status, B->P->rp, B->P->ci, nval, B->dense);
@@ -1134,7 +1187,7 @@ int hn_batch_factor(hn_batch* B, const double* D, double reg, double singular_to
             const int64_t np = B->step_pairs_h[st];
             if (np > 0) {
                 const int grid = (int)std::min<int64_t>(np, (int64_t)ctx().sm_count * 8);
-                batch_ldlt_update_kernel<<<grid, kT, 0, s>>>((int)st, cnt, np, B->step_pairs + B->pair_off_h[st],
+                batch_ldlt_update_kernel<<<grid, kT, kUpdSmem, s>>>((int)st, cnt, np, B->step_pairs + B->pair_off_h[st],
                                                              B->row_off, B->dn_off, B->order, status, B->dense,
                                                              B->dD);
                 launched("batch_ldlt_update_kernel");
@@ -1158,7 +1211,8 @@ int hn_batch_solve(hn_batch* B, const double* nval, const double* rhs, double* x
             spmv_launch(N, x, EpiAxpby{1.0, 0.0, B->ax}, s);
             check_cuda(cudaMemsetAsync(B->nref, 0, sizeof(int32_t), s), "memset");
             batch_refine_check_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, status, rhs, B->ax, B->r, B->refine,
-                                                                    B->nref);
+                                                                    B->nref, x, B->dyn, B->ref_iter,
+                                                                    B->kkt_tol > 0.0 ? 1 : 0);
             launched("batch_refine_check_kernel");
             int32_t left = 0;
             check_cuda(cudaMemcpyAsync(&left, B->nref, sizeof(left), cudaMemcpyDeviceToHost, s), "D2H");

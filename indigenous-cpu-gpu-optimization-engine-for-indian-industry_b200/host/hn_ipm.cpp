@@ -460,9 +460,12 @@ struct HostNormal {
 };
 
 // iterative_refinement(fac, N, x, rhs) with its defaults 1e-10 / 5 sweeps
-// (core/numerical/refinement.cpp:7-37).
+// (core/numerical/refinement.cpp:7-37). With shift != 0 the residual is taken
+// against N - shift I (the tightening phase refines against N without its
+// dyn_reg, whose M dx = -rp - dyn_reg dlam would floor the primal residual).
 template <class Fac>
-void refine(const Fac& fac, const HostNormal& N, std::vector<double>& x, const std::vector<double>& rhs) {
+void refine(const Fac& fac, const HostNormal& N, std::vector<double>& x, const std::vector<double>& rhs,
+            double shift = 0.0) {
     const std::size_t n = x.size();
     double norm_rhs = 0.0;
     for (double v : rhs) norm_rhs = std::max(norm_rhs, std::abs(v));
@@ -470,6 +473,8 @@ void refine(const Fac& fac, const HostNormal& N, std::vector<double>& x, const s
     std::vector<double> ax, r(n);
     for (int it = 0; it < 5; ++it) {
         N.multiply(x, ax);
+        if (shift != 0.0)
+            for (std::size_t i = 0; i < n; ++i) ax[i] -= shift * x[i];
         double rel = 0.0;
         for (std::size_t i = 0; i < n; ++i) rel = std::max(rel, std::abs(rhs[i] - ax[i]));
         rel /= norm_rhs;
@@ -669,16 +674,17 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
             result.factor_ms += ms_since(ta);
         }
         std::vector<double> hrhs(m), hdlam(m);
+        double unreg = 0.0;  // dyn_reg removed from the refinement's N while tightening
         auto solve_normal = [&](const DevBuf& rhs_dev) {
             auto t = Clock::now();
             ck(hn_memcpy_d2h(hrhs.data(), rhs_dev.p, 8 * m, st), "D2H rhs");
             hdlam = hrhs;
             if (sparse_fac) {
                 sfac.solve(hdlam);
-                refine(sfac, N, hdlam, hrhs);
+                refine(sfac, N, hdlam, hrhs, unreg);
             } else {
                 fac.solve(hdlam);
-                refine(fac, N, hdlam, hrhs);
+                refine(fac, N, hdlam, hrhs, unreg);
             }
             ck(hn_memcpy_h2d(dlam.p, hdlam.data(), 8 * m, st), "H2D dlam");
             result.solve_ms += ms_since(t);
@@ -727,6 +733,7 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
             }
             ck(hn_ada_numeric(P, D.d(), O.regularization, nval.d(), dyn.d(), st), "hn_ada_numeric");
             ck(hn_memcpy_d2h(N.val.data(), nval.p, 8 * (std::size_t)pnnz, st), "D2H N");
+            if (tighten && ref_iter >= 0) ck(hn_memcpy_d2h(&unreg, dyn.p, 8, st), "D2H dyn_reg");
             result.device_ms += ms_since(t0);
             if (deadline_passed()) {
                 time_up = true;

@@ -261,8 +261,17 @@ def test_bounded_and_ge_rows_match_reference(hn):
     ub = np.where(rng.random(400) < 0.3, lp["x0"] + 1.0, np.inf)
     lp2 = dict(lp, b=b)
     g = O.ref_ipm_solve(lp2, sense=sense, ub=ub)
+    # the reference's stopping rule alone: the reference's status and objective
+    r0 = hn.lp_solve(lp2, sense=sense, ub=ub, kkt_tol=0.0)
+    assert r0["status"] == g["status"] and rel(r0["objective"], g["objective"]) <= 1e-8, (r0["objective"], g)
+    # tightened past it (the default): same status; the objective stays within
+    # 1e-8 of the reference's or lands nearer the vertex optimum (the
+    # reference's crossover) than the reference's barrier endpoint does
     r = hn.lp_solve(lp2, sense=sense, ub=ub)
-    assert r["status"] == g["status"] and rel(r["objective"], g["objective"]) <= 1e-8, (r["objective"], g)
+    assert r["status"] == g["status"]
+    if rel(r["objective"], g["objective"]) > 1e-8:
+        vx = O.ref_ipm_solve(lp2, sense=sense, ub=ub, crossover=True)["objective"]
+        assert abs(r["objective"] - vx) < abs(g["objective"] - vx), (r["objective"], g["objective"], vx)
 
 
 # ---------------------------------------------------------------- IComputeBackend contract

@@ -59,3 +59,29 @@ def test_batch_warm_matches_plain_warm(hn):
         p = hn.lp_solve(lp, x0=x0s[k], y0=y0s[k], s0=s0s[k])
         assert r["warm_used"][k] == p["warm_start_used"]
         assert r["status"][k] == p["status"] == 1 and rel(r["objective"][k], p["objective"]) <= 1e-8
+
+
+def test_branch_and_bound_node_batch_warm_from_the_parent(hn):
+    """Branch-and-bound style nodes of one base LP (each tightens 1-8
+    variable bounds: ub = floor or lb = ceil of a perturbed x0_j, so the
+    standard forms gain upper-bound rows of their own and differ in shape),
+    solved in one batch warm-started from the parent's barrier solution
+    (x and the dual estimate y): every node ends with the status and
+    objective of its own cold plain solve (1e-8), at relative KKT <= 1e-8,
+    and the parent's point is taken as the start for most nodes."""
+    base = lpgen.lp_uniform(300, 720, 8, 31)
+    parent = hn.lp_solve(base)
+    assert parent["status"] == 1
+    nodes = lpgen.bb_nodes(base, 12, kmax=8, seed=77)
+    lbs, ubs = [lb for lb, _ in nodes], [ub for _, ub in nodes]
+    r = hn.lp_solve_batch([base] * len(nodes), lbs=lbs, ubs=ubs, x0s=[parent["x"]] * len(nodes),
+                          y0s=[parent["y"]] * len(nodes))
+    assert int(r["warm_used"].sum()) >= len(nodes) // 2
+    for k, (lb, ub) in enumerate(nodes):
+        cold = hn.lp_solve(base, lb=lb, ub=ub)
+        assert r["status"][k] == cold["status"], (k, r["status"][k], cold["status"])
+        if cold["status"] == 1:
+            assert rel(r["objective"][k], cold["objective"]) <= 1e-8, (k, r["objective"][k], cold["objective"])
+            assert r["kkt"][k, 0] <= 1e-8, (k, r["kkt"][k])
+            # a tightened bound can only raise the minimum
+            assert r["objective"][k] >= parent["objective"] - 1e-8 * (1 + abs(parent["objective"]))
