@@ -181,14 +181,15 @@ int hn_nrm2(int64_t n, const double* v_dev, double* result_dev, void* stream);
  * limited by their largest block only), and nnz(N) < 2^31. */
 int hn_ada_symbolic(const hn_csr* A, hn_pattern** out);
 /* The numeric phase has three layouts with bit-identical results.
- *  - Gather mode keeps an 8-byte source pair (A^T entry, A entry) per slot of
- *    N; one thread per slot, in slot order.
- *  - Relative map keeps 4 bytes per slot: the single term's entry within its
- *    row of A and within its row of A^T (or the slot's index among its row's
- *    multi-term slots); one warp per row of N, longest rows first. Chosen by
- *    default when rows of N average >= 256 slots and the offsets fit 32 bits
- *    (longest row of A x longest row of A^T < 2^31); HN_ADA_RELATIVE asks for
- *    it whenever the offsets fit, HN_ADA_GATHER8 asks for gather mode.
+ *  - Gather mode (the default) keeps an 8-byte source pair (A^T entry, A
+ *    entry) per slot of N; one thread per slot, in slot order.
+ *  - Relative map, asked for with HN_ADA_RELATIVE and used when the offsets
+ *    fit 32 bits (longest row of A x longest row of A^T < 2^31), keeps 4
+ *    bytes per slot: the single term's entry within its row of A and within
+ *    its row of A^T (or the slot's index among its row's multi-term slots);
+ *    one warp per row of N, longest rows first. Half the map memory; on the
+ *    large LP it is not faster (both layouts are bound by the random L2
+ *    gathers of A^T values). HN_ADA_GATHER8 asks for gather mode.
  *  - Row mode, asked for with HN_ADA_COMPACT and used when every row of N has
  *    <= 65,534 slots and every row of A <= 256 entries, keeps a 2-byte slot
  *    offset per term and assembles each row of N in shared-memory windows. */
@@ -312,15 +313,10 @@ int hn_batch_residuals(hn_batch* B, const hn_csr* M, const double* x_dev, const 
  * extra_iterations more iterations have run; hn_batch_finish then puts the
  * saved iterate back where the later one is worse or failed. kkt_tol <= 0:
  * the reference's rule alone (the residual is still measured when ru_dev is
- * given). max_iterations > 0: the reference's iteration limit; at iteration
- * max_iterations an instance its strict rule has not accepted is accepted
- * by the relaxed rule of interior_point.cpp:727-753 (residuals and mu below
- * 1e-4) -- and then tightened like the others -- or stops there with status
- * 6 (the loop may then run up to extra_iterations past the limit). The
- * arrays are caller-owned and must stay valid while the batch iterates.
- * Resets the per-instance records. */
+ * given). The arrays are caller-owned and must stay valid while the batch
+ * iterates. Resets the per-instance records. */
 int hn_batch_set_kkt(hn_batch* B, const double* ru_dev, const double* cu_dev, const double* offset_dev,
-                     double kkt_tol, int extra_iterations, int max_iterations);
+                     double kkt_tol, int extra_iterations);
 /* kkt_host: K x 4 (as hn_ipm_kkt's kkt_dev) at the last hn_batch_residuals
  * call, or after hn_batch_finish the residual of the returned iterate;
  * ref_iter_host: K, the iteration at which the reference's rule first held

@@ -722,8 +722,7 @@ int hn_ada_symbolic_ex(const hn_csr* A, unsigned flags, hn_pattern** out) {
                 for (int64_t j = 0; j < A->n; ++j) maxcol = std::max<int64_t>(maxcol, rpT[j + 1] - rpT[j]);
                 while ((int64_t(1) << qbits) < maxcol) ++qbits;
                 const bool fits = qbits < 31 && (int64_t)std::max(maxes[2], 1u) <= (int64_t(1) << (31 - qbits));
-                const bool long_rows = P->nnz >= 256 * m;  // a warp per row stays busy
-                rel = fits && ((flags & HN_ADA_RELATIVE) || long_rows);
+                rel = fits && (flags & HN_ADA_RELATIVE);
             }
             P->ci = dmalloc<int32_t>(P->nnz);
             if (P->row_mode) {

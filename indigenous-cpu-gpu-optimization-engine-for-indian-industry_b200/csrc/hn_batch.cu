@@ -72,11 +72,9 @@ struct hn_batch {
     const double *ru = nullptr, *cu = nullptr, *offset = nullptr;
     double kkt_tol = 0.0;
     int kkt_extra = 0;
-    int kkt_max_it = 0x7fffffff;  // the reference's iteration limit (its relaxed acceptance applies there)
     double *kkt = nullptr, *kkt_ref = nullptr;
     int32_t* ref_iter = nullptr;
     double *xb = nullptr, *zb = nullptr, *lb = nullptr;
-    double* dyn = nullptr;  // K: each instance's dyn_reg of the current factorisation
 };
 
 namespace hn {
@@ -102,9 +100,7 @@ struct KktArgs {
     int32_t* ref_iter;
     double tol;
     int extra;
-    int max_it;
 };
-constexpr int ST_LIMIT = 6;  // stopped at the reference's iteration limit without its acceptance
 
 __device__ __forceinline__ double fin_or_inf(double t) { return t <= 1.7976931348623157e308 ? t : INFINITY; }
 
@@ -178,11 +174,7 @@ __global__ void __launch_bounds__(kT) batch_prep_kernel(const int64_t* __restric
         int save = 0;
         if (status[i] == ST_RUN) {
             int r = k.ref_iter[i];
-            // the reference's rule (:525-530), or at its iteration limit its
-            // relaxed acceptance (:727-753)
-            const bool strict = mrp < tol && mrd < tol && mu < ctol;
-            const bool relaxed = iter >= k.max_it && mrp < 1e-4 && mrd < 1e-4 && mu < 1e-4;
-            if (r < 0 && (strict || relaxed)) {
+            if (r < 0 && mrp < tol && mrd < tol && mu < ctol) {  // the reference's rule, :525-530
                 r = iter;
                 k.ref_iter[i] = iter;
                 save = measure && k.tol > 0.0;
@@ -194,8 +186,6 @@ __global__ void __launch_bounds__(kT) batch_prep_kernel(const int64_t* __restric
             if (r >= 0 && (!(measure && k.tol > 0.0) || kk <= k.tol || iter - r >= k.extra)) {
                 status[i] = ST_OPTIMAL;
                 iters[i] = iter;
-            } else if (r < 0 && iter >= k.max_it) {
-                status[i] = ST_LIMIT;  // where the reference stops unaccepted
             }
         }
         s_save = save;
@@ -355,8 +345,7 @@ __global__ void __launch_bounds__(kT) batch_update_kernel(const int64_t* __restr
 // ---- normal equations per instance ----
 __global__ void __launch_bounds__(kT) batch_reg_kernel(const int64_t* __restrict__ row_off,
                                                        const int64_t* __restrict__ diag_pos, double reg,
-                                                       const int32_t* __restrict__ status, double* __restrict__ nval,
-                                                       double* __restrict__ dyn_out) {
+                                                       const int32_t* __restrict__ status, double* __restrict__ nval) {
     __shared__ double sh[32];
     __shared__ double s_dyn;
     const int64_t i = blockIdx.x;
@@ -368,7 +357,6 @@ __global__ void __launch_bounds__(kT) batch_reg_kernel(const int64_t* __restrict
     if (threadIdx.x == 0) {
         const double dyn = 1e-12 * md;
         s_dyn = (reg < dyn) ? dyn : reg;  // std::max(regularization, 1e-12 * max_diag)
-        dyn_out[i] = s_dyn;
     }
     __syncthreads();
     const double dyn = s_dyn;
@@ -848,27 +836,18 @@ __global__ void __launch_bounds__(kFb) batch_bwd_diag_kernel(int s, const int64_
 // Refinement bookkeeping per instance (refinement.cpp:15-30): with r = rhs - N x,
 // rel = max|r| / max|rhs|; an instance keeps sweeping while rel > 1e-10 and
 // sweeps remain; a sweeping instance's r is then solved and added to x.
-// In the tightening phase (an instance the reference's rule has accepted,
-// unreg != 0) the residual is taken against N without its dyn_reg: the
-// regularised system leaves M dx = -rp - dyn_reg dlam, a floor of about
-// dyn_reg |dlam| under the primal residual, which refinement against the
-// unregularised N (the regularised factor as its preconditioner) removes.
 __global__ void __launch_bounds__(kT) batch_refine_check_kernel(const int64_t* __restrict__ row_off,
                                                                 const int32_t* __restrict__ status,
                                                                 const double* __restrict__ rhs,
                                                                 const double* __restrict__ ax, double* __restrict__ r,
-                                                                int32_t* __restrict__ refine, int32_t* nref,
-                                                                const double* __restrict__ x,
-                                                                const double* __restrict__ dyn,
-                                                                const int32_t* __restrict__ ref_iter, int unreg) {
+                                                                int32_t* __restrict__ refine, int32_t* nref) {
     __shared__ double sh[32];
     const int64_t i = blockIdx.x;
     if (status[i] != ST_RUN || !refine[i]) return;
     const int64_t r0 = row_off[i], r1 = row_off[i + 1];
-    const double shift = (unreg && ref_iter[i] >= 0) ? dyn[i] : 0.0;
     double nb = 0.0, nr = 0.0;
     for (int64_t k = r0 + threadIdx.x; k < r1; k += kT) {
-        const double b = rhs[k], d = shift != 0.0 ? b - (ax[k] - shift * x[k]) : b - ax[k];
+        const double b = rhs[k], d = b - ax[k];
         nb = fmax(nb, fabs(b));
         nr = fmax(nr, fabs(d));
         r[k] = d;
@@ -929,14 +908,14 @@ void free_batch(hn_batch* B) {
                     (void*)B->tile_row, (void*)B->tile_nz, (void*)B->carry_row, (void*)B->head_row,
                     (void*)B->carry_val, (void*)B->head_val, (void*)B->r, (void*)B->ax, (void*)B->step_pairs, (void*)B->step_chunks,
                     (void*)B->solve_part, (void*)B->kkt, (void*)B->kkt_ref, (void*)B->ref_iter, (void*)B->xb,
-                    (void*)B->zb, (void*)B->lb, (void*)B->dyn})
+                    (void*)B->zb, (void*)B->lb})
         dfree(p);
     delete B;
 }
 
 KktArgs kkt_args(const hn_batch* B, const double* lam, const double* b, const double* c) {
     return KktArgs{lam,    b,      c,      B->ru,  B->cu,       B->offset, B->kkt,
-                   B->kkt_ref, B->xb, B->zb, B->lb, B->ref_iter, B->kkt_tol, B->kkt_extra, B->kkt_max_it};
+                   B->kkt_ref, B->xb, B->zb, B->lb, B->ref_iter, B->kkt_tol, B->kkt_extra};
 }
 
 SpmvMat n_mat(const hn_batch* B, const double* nval) {
@@ -1024,8 +1003,6 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
                                             (int)kUpdSmem),
                        "update smem attribute");
             B->ref_iter = dmalloc<int32_t>(K);
-            B->dyn = dmalloc<double>(K);
-            check_cuda(cudaMemsetAsync(B->dyn, 0, sizeof(double) * K, s), "memset");
             B->kkt = dmalloc<double>(4 * K);
             B->kkt_ref = dmalloc<double>(4 * K);
             check_cuda(cudaMemsetAsync(B->ref_iter, 0xff, sizeof(int32_t) * K, s), "memset");  // -1
@@ -1113,7 +1090,7 @@ int hn_batch_residuals(hn_batch* B, const hn_csr* M, const double* x, const doub
 }
 
 int hn_batch_set_kkt(hn_batch* B, const double* ru, const double* cu, const double* offset, double kkt_tol,
-                     int extra_iterations, int max_iterations) {
+                     int extra_iterations) {
     return guard("hn_batch_set_kkt", [&] {
         require_init();
         if (!B || (ru == nullptr) != (cu == nullptr) || (ru && !offset) || extra_iterations < 0)
@@ -1124,7 +1101,6 @@ int hn_batch_set_kkt(hn_batch* B, const double* ru, const double* cu, const doub
         B->offset = offset;
         B->kkt_tol = kkt_tol > 0.0 ? kkt_tol : 0.0;
         B->kkt_extra = extra_iterations;
-        B->kkt_max_it = max_iterations > 0 ? max_iterations : 0x7fffffff;
         if (B->kkt_tol > 0.0 && !B->xb) {
             B->xb = dmalloc<double>(B->n);
             B->zb = dmalloc<double>(B->n);
@@ -1167,7 +1143,7 @@ int hn_batch_factor(hn_batch* B, const double* D, double reg, double singular_to
         if (!B || !D || !nval || !status) fail(HN_ERR_INVALID_ARG, "bad arguments");
         cudaStream_t s = as_stream(stream);
         ada_numeric_unregularised(B->P, D, nval, s);
-        batch_reg_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, B->P->diag_pos, reg, status, nval, B->dyn);
+        batch_reg_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, B->P->diag_pos, reg, status, nval);
         launched("batch_reg_kernel");
         batch_dense_kernel<<<(unsigned)((B->m * 32 + 255) / 256), 256, 0, s>>>(
             B->m, B->row_off, B->row_inst, B->dn_off, status, B->P->rp, B->P->ci, nval, B->dense);
@@ -1211,8 +1187,7 @@ int hn_batch_solve(hn_batch* B, const double* nval, const double* rhs, double* x
             spmv_launch(N, x, EpiAxpby{1.0, 0.0, B->ax}, s);
             check_cuda(cudaMemsetAsync(B->nref, 0, sizeof(int32_t), s), "memset");
             batch_refine_check_kernel<<<(unsigned)B->K, kT, 0, s>>>(B->row_off, status, rhs, B->ax, B->r, B->refine,
-                                                                    B->nref, x, B->dyn, B->ref_iter,
-                                                                    B->kkt_tol > 0.0 ? 1 : 0);
+                                                                    B->nref);
             launched("batch_refine_check_kernel");
             int32_t left = 0;
             check_cuda(cudaMemcpyAsync(&left, B->nref, sizeof(left), cudaMemcpyDeviceToHost, s), "D2H");

@@ -119,7 +119,7 @@ SIGNATURES = {
     "hn_batch_steps": [_vp] + [_vp] * 7 + [_vp],
     "hn_batch_corrector": [_vp, _vp] + [_vp] * 9 + [_vp],
     "hn_batch_update": [_vp] + [_vp] * 9 + [C.c_int, _vp],
-    "hn_batch_set_kkt": [_vp, _vp, _vp, _vp, C.c_double, C.c_int, C.c_int],
+    "hn_batch_set_kkt": [_vp, _vp, _vp, _vp, C.c_double, C.c_int],
     "hn_batch_kkt": [_vp, _f64p, _i32p],
     "hn_batch_finish": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
 }

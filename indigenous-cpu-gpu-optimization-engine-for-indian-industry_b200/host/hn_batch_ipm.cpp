@@ -89,8 +89,7 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
         ck(hn_memcpy_h2d(ru.p, pf.ru.data(), 8 * m, st), "H2D");
         ck(hn_memcpy_h2d(cu.p, pf.cu.data(), 8 * n, st), "H2D");
         ck(hn_memcpy_h2d(koff.p, pf.offset.data(), 8 * K, st), "H2D");
-        ck(hn_batch_set_kkt(B, ru.d(), cu.d(), koff.d(), O.kkt_tol, O.kkt_extra_iterations, O.max_iterations),
-           "hn_batch_set_kkt");
+        ck(hn_batch_set_kkt(B, ru.d(), cu.d(), koff.d(), O.kkt_tol, O.kkt_extra_iterations), "hn_batch_set_kkt");
         std::vector<int32_t> hstatus(K), hiters(K);
         auto read_status = [&]() {
             ck(hn_memcpy_d2h(hstatus.data(), status.p, 4 * K, st), "D2H status");
@@ -98,9 +97,7 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
             for (int32_t v : hstatus) running += (v == 0);
             return running;
         };
-        // past the reference's limit only instances in their tightening phase
-        // iterate (the others stop there, status 6)
-        const int max_it = O.max_iterations + (O.kkt_tol > 0.0 ? O.kkt_extra_iterations : 0);
+        const int max_it = O.max_iterations;
         int iter = 0;
         bool time_up = false;
         for (iter = 0; iter < max_it; ++iter) {

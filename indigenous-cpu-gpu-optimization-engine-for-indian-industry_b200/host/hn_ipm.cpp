@@ -460,12 +460,9 @@ struct HostNormal {
 };
 
 // iterative_refinement(fac, N, x, rhs) with its defaults 1e-10 / 5 sweeps
-// (core/numerical/refinement.cpp:7-37). With shift != 0 the residual is taken
-// against N - shift I (the tightening phase refines against N without its
-// dyn_reg, whose M dx = -rp - dyn_reg dlam would floor the primal residual).
+// (core/numerical/refinement.cpp:7-37).
 template <class Fac>
-void refine(const Fac& fac, const HostNormal& N, std::vector<double>& x, const std::vector<double>& rhs,
-            double shift = 0.0) {
+void refine(const Fac& fac, const HostNormal& N, std::vector<double>& x, const std::vector<double>& rhs) {
     const std::size_t n = x.size();
     double norm_rhs = 0.0;
     for (double v : rhs) norm_rhs = std::max(norm_rhs, std::abs(v));
@@ -473,8 +470,6 @@ void refine(const Fac& fac, const HostNormal& N, std::vector<double>& x, const s
     std::vector<double> ax, r(n);
     for (int it = 0; it < 5; ++it) {
         N.multiply(x, ax);
-        if (shift != 0.0)
-            for (std::size_t i = 0; i < n; ++i) ax[i] -= shift * x[i];
         double rel = 0.0;
         for (std::size_t i = 0; i < n; ++i) rel = std::max(rel, std::abs(rhs[i] - ax[i]));
         rel /= norm_rhs;
@@ -674,25 +669,22 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
             result.factor_ms += ms_since(ta);
         }
         std::vector<double> hrhs(m), hdlam(m);
-        double unreg = 0.0;  // dyn_reg removed from the refinement's N while tightening
         auto solve_normal = [&](const DevBuf& rhs_dev) {
             auto t = Clock::now();
             ck(hn_memcpy_d2h(hrhs.data(), rhs_dev.p, 8 * m, st), "D2H rhs");
             hdlam = hrhs;
             if (sparse_fac) {
                 sfac.solve(hdlam);
-                refine(sfac, N, hdlam, hrhs, unreg);
+                refine(sfac, N, hdlam, hrhs);
             } else {
                 fac.solve(hdlam);
-                refine(fac, N, hdlam, hrhs, unreg);
+                refine(fac, N, hdlam, hrhs);
             }
             ck(hn_memcpy_h2d(dlam.p, hdlam.data(), 8 * m, st), "H2D dlam");
             result.solve_ms += ms_since(t);
         };
 
-        // past the reference's limit the loop runs only while tightening
-        const std::size_t ref_max_it = static_cast<std::size_t>(std::max(O.max_iterations, 0));
-        const std::size_t max_it = ref_max_it + (tighten ? static_cast<std::size_t>(O.kkt_extra_iterations) : 0);
+        const std::size_t max_it = static_cast<std::size_t>(std::max(O.max_iterations, 0));
         std::size_t iter = 0;
         for (iter = 0; iter < max_it; ++iter) {
             if (O.interrupt_callback && O.interrupt_callback()) {
@@ -710,13 +702,8 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
             read_scal();
             measure();
             const double mu = sc[HN_IPM_MU];
-            const bool strict =
-                sc[HN_IPM_NRP] < O.convergence_tol && sc[HN_IPM_NRD] < O.convergence_tol && mu < O.complementarity_tol;
-            // at the reference's limit its relaxed acceptance (:727-753)
-            const bool relaxed =
-                iter >= ref_max_it && sc[HN_IPM_NRP] < 1e-4 && sc[HN_IPM_NRD] < 1e-4 && mu < 1e-4;
-            if (ref_iter < 0 && iter >= ref_max_it && !relaxed) break;  // the reference stops here unaccepted
-            if (ref_iter < 0 && (strict || relaxed)) {  // the reference's rule (:525-530)
+            if (ref_iter < 0 && sc[HN_IPM_NRP] < O.convergence_tol && sc[HN_IPM_NRD] < O.convergence_tol &&
+                mu < O.complementarity_tol) {  // the reference's rule (:525-530)
                 ref_iter = (long)iter;
                 std::memcpy(kref, kv, sizeof(kv));
                 if (tighten) {
@@ -733,7 +720,6 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
             }
             ck(hn_ada_numeric(P, D.d(), O.regularization, nval.d(), dyn.d(), st), "hn_ada_numeric");
             ck(hn_memcpy_d2h(N.val.data(), nval.p, 8 * (std::size_t)pnnz, st), "D2H N");
-            if (tighten && ref_iter >= 0) ck(hn_memcpy_d2h(&unreg, dyn.p, 8, st), "D2H dyn_reg");
             result.device_ms += ms_since(t0);
             if (deadline_passed()) {
                 time_up = true;

@@ -172,8 +172,7 @@ def test_large_zipf_sampled_rows_match_oracle(hn, torch_cuda):
 def test_numeric_layouts_bit_identical(hn, torch_cuda, shape):
     """The three numeric layouts (row mode, gather mode, relative map) give
     the same bits, with inactive columns (d_j = 0) and three or more terms in
-    some slots; the last shape has rows of N long enough (>= 256 slots on
-    average) for the relative map to be the library's own choice."""
+    some slots; the last shape has rows of N of ~1,300 slots on average."""
     m, n, k, seed = shape
     lp = lpgen.scaled_problem(lpgen.lp_uniform(m, n, k, seed))
     D = np.random.default_rng(seed).uniform(1e-3, 1e3, n)
@@ -193,8 +192,7 @@ def test_numeric_layouts_bit_identical(hn, torch_cuda, shape):
     for (p1, v1, d1) in out[1:]:
         assert np.array_equal(p0[0], p1[0]) and np.array_equal(p0[1], p1[1])
         assert np.array_equal(v0, v1) and d0 == d1
-    auto = hn.Pattern(A)
-    assert auto.mode()[0] == (hn.Pattern.RELATIVE if auto.nnz >= 256 * m else hn.Pattern.GATHER)
+    assert hn.Pattern(A).mode()[0] == hn.Pattern.GATHER  # the default
     check_values(lp, D, 1e-8, p0[0].astype(np.int64), p0[1].astype(np.int64), v0, d0)
 
 
