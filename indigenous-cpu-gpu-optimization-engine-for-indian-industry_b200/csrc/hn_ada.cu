@@ -41,7 +41,7 @@ constexpr int64_t kDiagFlag = int64_t(1) << 62;
 constexpr int kSlotsPerThread = 4;  // slots per thread per trip of the numeric kernel
 constexpr uint16_t kSlotMulti = 0xFFFFu;
 constexpr int kRowThreads = 256;     // row-mode numeric kernel
-constexpr int kRowWindow = 4096;     // row mode: slots of a row of N assembled per pass (32 KB)
+constexpr int kRowWindow = 8192;     // row mode: slots of a row of N assembled per pass (64 KB)
 constexpr int kRowMaxSlots = 65534;  // row mode: slot offsets fit 16 bits
 constexpr int kRowMaxEntries = 256;  // row mode: entries of a row of A staged in shared memory
 
@@ -453,28 +453,34 @@ __global__ void ada_combine_kernel(int64_t nms, const int64_t* __restrict__ mpos
         atomicMax(maxdiag, static_cast<unsigned long long>(__double_as_longlong(s)));
 }
 
-// Row mode: one CTA per row of N at a time, in windows of kRowWindow slots.
-// The row's A entries (value, d, A^T row start, term offset) are staged in
-// shared memory; the row's terms (e, p) are cut into chunks of 8 -- one
-// 16-byte load of the slot map (each row's terms start on a 16-byte
-// boundary) -- and each thread walks its chunk, moving to the next entry as
-// the term offsets pass. A single-slot term in the current window writes
-// (A value x A^T value) x d into the shared window at its slot offset, the
-// window's multi slots take their combined sums from mval, and the window
-// leaves in one coalesced streaming store; a row longer than the window
-// walks its terms once per window. The arithmetic of each slot is the slot
-// kernel's, so both modes give the same bits.
-__global__ void __launch_bounds__(kRowThreads) ada_row_kernel(
+// Row mode: one CTA per row of N at a time, the row assembled in shared
+// memory in windows of kRowWindow slots. The row's A entries (value, d,
+// A^T row start, term offset) are staged in shared memory; then each warp
+// takes whole entries e (column j) and its lanes walk the entry's terms --
+// row j of A^T and the matching run of 2-byte slot offsets -- contiguously,
+// kRowU terms per lane in flight, so A^T values and offsets arrive in
+// coalesced lines instead of one random 32-byte sector per slot. A
+// single-term slot in the window gets (A value x A^T value) x d at its
+// offset, the window's multi slots take their combined sums from mval, and
+// the window leaves in one coalesced streaming store; a row longer than the
+// window walks its terms once per window. The arithmetic of each slot is the
+// slot kernel's, so every layout gives the same bits.
+constexpr int kRowU = 4;
+constexpr size_t kRowSmem = sizeof(double) * kRowWindow + sizeof(double2) * kRowMaxEntries +
+                            sizeof(int32_t) * (2 * kRowMaxEntries + 1);
+__global__ void __launch_bounds__(kRowThreads, 3) ada_row_kernel(
     int m, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double2* __restrict__ vd,
     const int32_t* __restrict__ rpT, const double* __restrict__ valT, const int64_t* __restrict__ tq,
     const uint16_t* __restrict__ smap, const int64_t* __restrict__ rpN, const int64_t* __restrict__ msrow,
     const int64_t* __restrict__ mpos, const double* __restrict__ mval, double* __restrict__ nval) {
-    __shared__ double srow[kRowWindow];
-    __shared__ double2 s_vd[kRowMaxEntries];
-    __shared__ int32_t s_cs[kRowMaxEntries];
-    __shared__ int32_t s_to[kRowMaxEntries + 1];
+    extern __shared__ __align__(16) double row_smem[];
+    double* srow = row_smem;
+    double2* s_vd = reinterpret_cast<double2*>(row_smem + kRowWindow);
+    int32_t* s_cs = reinterpret_cast<int32_t*>(s_vd + kRowMaxEntries);
+    int32_t* s_to = s_cs + kRowMaxEntries;
     __shared__ int64_t sh[32];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int kWarps = kRowThreads / 32;
     for (int i = blockIdx.x; i < m; i += gridDim.x) {
         const int e0 = rp[i], ne = rp[i + 1] - e0;
         // term counts per entry (0 for an explicit zero of A), exclusive scan
@@ -492,38 +498,32 @@ __global__ void __launch_bounds__(kRowThreads) ada_row_kernel(
         if (tid < ne) s_to[tid] = static_cast<int32_t>(ex);
         if (tid == 0) s_to[ne] = static_cast<int32_t>(tot);
         __syncthreads();
-        const int T = static_cast<int>(tot);
-        const uint4* sm = reinterpret_cast<const uint4*>(smap + tq[i]);
-        const int nch = (T + 7) >> 3;
+        const uint16_t* sm = smap + tq[i];
         const int64_t r0 = rpN[i];
         const int L = static_cast<int>(rpN[i + 1] - r0);
         const int64_t ms0 = msrow[i], ms1 = msrow[i + 1];
         for (int w0 = 0; w0 < L; w0 += kRowWindow) {
             const int w1 = min(L, w0 + kRowWindow);
-            for (int c = tid; c < nch; c += kRowThreads) {
-                const uint4 raw = __ldcs(sm + c);
-                const uint32_t w[4] = {raw.x, raw.y, raw.z, raw.w};
-                const int t0 = c << 3;
-                int lo = 0, hi = ne - 1;  // entry of term t0: last e with s_to[e] <= t0
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (s_to[mid] <= t0)
-                        lo = mid;
-                    else
-                        hi = mid - 1;
-                }
-                int e = lo, next = s_to[lo + 1];
+            for (int e = warp; e < ne; e += kWarps) {
+                const int t0 = s_to[e], c = s_to[e + 1] - t0;
+                if (c == 0) continue;
+                const double2 q = s_vd[e];
+                const double* vT = valT + s_cs[e];
+                const uint16_t* se = sm + t0;
+                for (int p0 = lane; p0 < c; p0 += 32 * kRowU) {
+                    uint16_t slot[kRowU];
+                    double b[kRowU];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int t = t0 + u;
-                    if (t < T) {
-                        while (t >= next) next = s_to[++e + 1];
-                        const int slot = static_cast<int>((w[u >> 1] >> ((u & 1) * 16)) & 0xFFFFu);
-                        if (slot != kSlotMulti && slot >= w0 && slot < w1) {
-                            const double2 q = s_vd[e];
-                            const double b = __ldg(valT + s_cs[e] + (t - s_to[e]));
-                            srow[slot - w0] = (q.y <= 0.0) ? 0.0 : (q.x * b) * q.y;  // columns with D_j <= 0 skipped
-                        }
+                    for (int u = 0; u < kRowU; ++u) {
+                        const int p = p0 + 32 * u;
+                        slot[u] = p < c ? __ldcs(se + p) : kSlotMulti;
+                        b[u] = p < c ? __ldcg(vT + p) : 0.0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < kRowU; ++u) {
+                        const int sl = slot[u];
+                        if (sl != kSlotMulti && sl >= w0 && sl < w1)
+                            srow[sl - w0] = (q.y <= 0.0) ? 0.0 : (q.x * b[u]) * q.y;  // columns with D_j <= 0 skipped
                     }
                 }
             }
@@ -586,8 +586,15 @@ void launch_numeric(const hn_pattern* P, const double* d, double* nval, cudaStre
         launched("ada_combine_kernel");
     }
     if (P->row_mode) {
-        const int grid = (int)std::min<int64_t>(P->m, (int64_t)ctx().sm_count * 5);
-        ada_row_kernel<<<grid, kRowThreads, 0, s>>>((int)P->m, A->rp, A->ci, P->vd, A->rpT, A->valT, P->tq,
+        static int row_attr_device = -1;
+        if (row_attr_device != ctx().device) {
+            check_cuda(cudaFuncSetAttribute(ada_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kRowSmem),
+                       "row kernel smem attribute");
+            row_attr_device = ctx().device;
+        }
+        const int grid = (int)std::min<int64_t>(P->m, (int64_t)ctx().sm_count * 3);
+        ada_row_kernel<<<grid, kRowThreads, kRowSmem, s>>>((int)P->m, A->rp, A->ci, P->vd, A->rpT, A->valT, P->tq,
                                                        P->smap, P->rp, P->msrow, P->mpos, P->mval, nval);
         launched("ada_row_kernel");
         return;

@@ -212,3 +212,32 @@ def test_long_row_of_a_selects_gather_mode(hn, torch_cuda):
     A, P, rp_, ci_, vals_, dyn = assemble(hn, torch_cuda, lp2, D, compact=True)
     assert P.mode()[0] != hn.Pattern.ROW
     check_values(lp2, D, 1e-8, rp_, ci_, vals_, dyn)
+
+
+def test_row_layout_long_rows_bit_identical_to_gather(hn, torch_cuda):
+    """Rows of N longer than the row layout's 8,192-slot shared-memory window
+    (m 30,000, n 90,000, 60 nonzeros per column: ~9,000 slots per row, rows of
+    A 180 entries on average, 236 at most): the row layout assembles each row
+    in several windows and
+    must give the gather layout's bits (the gather layout is pinned to the
+    oracle by the tests above)."""
+    torch = torch_cuda
+    lp = lpgen.scaled_problem(lpgen.lp_uniform(30000, 90000, 60, 5))
+    m, n = lp["m"], lp["n"]
+    D = np.random.default_rng(8).uniform(1e-3, 1e3, n)
+    D[::29] = 0.0
+    A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
+    Dd = torch.as_tensor(D, device="cuda")
+    out = []
+    for layout in (hn.Pattern.ROW, hn.Pattern.GATHER):
+        P = hn.Pattern(A, layout=layout)
+        assert P.mode()[0] == layout
+        if layout == hn.Pattern.ROW:
+            assert P.mode()[1] > 8192
+        nval = torch.empty(P.nnz, dtype=torch.float64, device="cuda")
+        dyn = torch.empty(1, dtype=torch.float64, device="cuda")
+        P.numeric(Dd, 1e-8, nval, dyn)
+        torch.cuda.synchronize()
+        out.append((nval.cpu().numpy(), dyn.item()))
+        del P, nval
+    assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
