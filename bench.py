@@ -284,6 +284,10 @@ def run_ours(args, rank, world, local):
             result["plain_ipm"] = plain_ipm()
         if batch_result is not None:
             result["batched_ipm"] = batch_result
+        if not args.no_gnn:
+            # the GNN warm start at reduced scale (the config's 20,000 training
+            # and 4,096 evaluation LPs are the --only gnn mode)
+            result["gnn_warm_small"] = gnn_warm(args.small_gnn, args.small_gnn, 500, 5000, 20, 256, plain_sample=2)
         if not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(lp, vec, threads=os.cpu_count() or 1, reps=1)
     return result
@@ -491,6 +495,7 @@ def bb_batch(K: int, chunk: int, sample: int = 2):
 
 
 def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: int, plain_sample: int = 8):
+    # n_eval LPs: cold and warm batched solves; plain_sample of them by the plain GPU IPM
     """GNN warm start: LPs of the m=2000 generator with m log-uniform in
     [mlo, mhi] and n = round(2.5 m), 8 nonzeros per column. Training LPs
     (seeds 4,000,000 + i) are labelled by the batched GPU IPM (its primal
@@ -510,7 +515,7 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
         return [lpgen.lp_uniform(int(m), int(round(2.5 * m)), 8, seed0 + i) for i, m in enumerate(sizes)]
 
     def batched(lps, warm=None):
-        out = {"status": [], "objective": [], "iterations": [], "warm_used": [], "x": [], "y": [], "s": []}
+        out = {"status": [], "objective": [], "iterations": [], "warm_used": [], "kkt": [], "x": [], "y": [], "s": []}
         for c0 in range(0, len(lps), chunk):
             part = lps[c0:c0 + chunk]
             kw = {}
@@ -521,13 +526,14 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
             r = hn.lp_solve_batch(part, **kw)
             for k in ("status", "objective", "iterations", "warm_used"):
                 out[k].append(r[k])
+            out["kkt"].append(r["kkt"][:, 0])
             for k, lp in enumerate(part):
                 c0_, c1_ = r["col_off"][k], r["col_off"][k + 1]
                 r0_, r1_ = r["row_off"][k], r["row_off"][k + 1]
                 out["x"].append(r["x"][c0_:c1_])
                 out["y"].append(r["y"][r0_:r1_])
                 out["s"].append(r["s"][c0_:c1_])
-        for k in ("status", "objective", "iterations", "warm_used"):
+        for k in ("status", "objective", "iterations", "warm_used", "kkt"):
             out[k] = np.concatenate(out[k])
         return out
 
@@ -577,6 +583,8 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
             "iterations_mean_warm": round(float(warm["iterations"].mean()), 2),
             "warm_used": int(warm["warm_used"].sum()), "optimal_cold": int((cold["status"] == 1).sum()),
             "optimal_warm": int((warm["status"] == 1).sum()),
+            "kkt_le_1e-8_cold": int(((cold["status"] == 1) & (cold["kkt"] <= 1e-8)).sum()),
+            "kkt_le_1e-8_warm": int(((warm["status"] == 1) & (warm["kkt"] <= 1e-8)).sum()),
             "same_status_and_objective_1e-8": int(same.sum()),
             "plain_gpu_solves_per_s_extrapolated": round(n_eval / plain_est, 3),
             "warm_batched_vs_plain_gpu": round(plain_est / warm_s, 2)}
@@ -901,6 +909,8 @@ def main():
     ap.add_argument("--scale", type=int, default=1, help="--only modes: shrink the LP by this factor (profiling)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-IPM key")
     ap.add_argument("--no-literal", action="store_true", help="skip the spec-literal (17M nonzeros) SpMV lines")
+    ap.add_argument("--no-gnn", action="store_true", help="skip the reduced GNN warm-start key")
+    ap.add_argument("--small-gnn", type=int, default=256, help="training and evaluation LPs of the reduced GNN key")
     ap.add_argument("--literal", action="store_true", help="--only spmv / spmv_t: the spec-literal LP")
     ap.add_argument("--spmv-kind", type=int, default=-1, help="--only spmv / spmv_t: pin a path (0 merge, 1 binned)")
     ap.add_argument("--spmv-t", type=int, default=8, help="--only spmv / spmv_t: nonzeros per lane of the binned path")
