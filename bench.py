@@ -287,7 +287,7 @@ def run_ours(args, rank, world, local):
         if not args.no_gnn:
             # the GNN warm start at reduced scale (the config's 20,000 training
             # and 4,096 evaluation LPs are the --only gnn mode)
-            result["gnn_warm_small"] = gnn_warm(args.small_gnn, args.small_gnn, 500, 5000, 20, 256, plain_sample=2)
+            result["gnn_warm_small"] = gnn_warm(args.small_gnn, args.small_gnn, 500, 5000, 20, 256, plain_sample=6)
         if not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(lp, vec, threads=os.cpu_count() or 1, reps=1)
     return result
@@ -514,13 +514,18 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
         sizes = np.round(np.exp(rng.uniform(np.log(mlo), np.log(mhi), count))).astype(int)
         return [lpgen.lp_uniform(int(m), int(round(2.5 * m)), 8, seed0 + i) for i, m in enumerate(sizes)]
 
+    infer = [0.0]
+
     def batched(lps, warm=None):
         out = {"status": [], "objective": [], "iterations": [], "warm_used": [], "kkt": [], "x": [], "y": [], "s": []}
         for c0 in range(0, len(lps), chunk):
             part = lps[c0:c0 + chunk]
             kw = {}
             if warm is not None:
+                ti = time.perf_counter()
                 preds = gnn.predict(warm, gnn.Batch(part))
+                torch.cuda.synchronize()
+                infer[0] += time.perf_counter() - ti
                 kw = {"x0s": [p[0] for p in preds], "y0s": [p[1] for p in preds], "s0s": [p[2] for p in preds],
                       "warm_floor": gnn.WARM_FLOOR}
             r = hn.lp_solve_batch(part, **kw)
@@ -579,6 +584,7 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
             "loss_first_last": [round(losses[0], 4), round(losses[-1], 4)],
             "cold_batched_s": round(cold_s, 2), "cold_batched_solves_per_s": round(n_eval / cold_s, 2),
             "warm_batched_s": round(warm_s, 2), "warm_batched_solves_per_s": round(n_eval / warm_s, 2),
+            "warm_inference_s": round(infer[0], 2),
             "iterations_mean_cold": round(float(cold["iterations"].mean()), 2),
             "iterations_mean_warm": round(float(warm["iterations"].mean()), 2),
             "warm_used": int(warm["warm_used"].sum()), "optimal_cold": int((cold["status"] == 1).sum()),

@@ -511,12 +511,14 @@ __global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, int cnt, co
 // Trailing update of one 64 x 64 tile pair per CTA iteration. Both 64-column
 // panel slices arrive by 16-byte asynchronous copies (rows start on 16-byte
 // boundaries: even row stride), in two commit groups of 32 columns, so the
-// second half is in flight while the first is multiplied. D is applied at the
+// second half is in flight while the first is multiplied; the output tile
+// arrives the same way (a third group) and is read back from shared memory in
+// the epilogue. D is applied at the
 // fragment load: a = L[r, k] D_k rounds once, as a staged product would, and
 // every output fragment takes the same DMMA sequence (k ascending in steps of
 // 4), so the result does not depend on the staging.
 constexpr int kUpdP = kFb + 4;  // smem row stride: a half-warp's fragment loads hit 16 distinct bank pairs
-constexpr size_t kUpdSmem = sizeof(double) * (2 * kFb * kUpdP + kFb);
+constexpr size_t kUpdSmem = sizeof(double) * (3 * kFb * kUpdP + kFb);
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
@@ -524,7 +526,7 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool vali
                  : "memory");
 }
 
-__global__ void __launch_bounds__(kT, 3) batch_ldlt_update_kernel(int s, int cnt, int64_t npairs,
+__global__ void __launch_bounds__(kT, 2) batch_ldlt_update_kernel(int s, int cnt, int64_t npairs,
                                                                const int64_t* __restrict__ pairs,
                                                                const int64_t* __restrict__ row_off,
                                                                const int64_t* __restrict__ dn_off,
@@ -535,7 +537,8 @@ __global__ void __launch_bounds__(kT, 3) batch_ldlt_update_kernel(int s, int cnt
     extern __shared__ __align__(16) double upd_smem[];
     double(*sW)[kUpdP] = reinterpret_cast<double(*)[kUpdP]>(upd_smem);                // L[rb + r, k0 + k]
     double(*sL)[kUpdP] = reinterpret_cast<double(*)[kUpdP]>(upd_smem + kFb * kUpdP);  // L[cb + c, k0 + k]
-    double* sD = upd_smem + 2 * kFb * kUpdP;
+    double(*sC)[kUpdP] = reinterpret_cast<double(*)[kUpdP]>(upd_smem + 2 * kFb * kUpdP);  // A[rb + r, cb + c]
+    double* sD = upd_smem + 3 * kFb * kUpdP;
     const int tid = threadIdx.x;
     const int k0 = s * kFb;
     int lo = 0;  // the instance of the previous pair: pairs arrive in increasing order
@@ -586,6 +589,15 @@ __global__ void __launch_bounds__(kT, 3) batch_ldlt_update_kernel(int s, int cnt
             }
             asm volatile("cp.async.commit_group;\n" ::: "memory");
         }
+        // the output tile (third group): rows or columns past m are zero-filled
+        for (int idx = tid; idx < kFb * 32; idx += kT) {
+            const int rr = idx >> 5, q2 = idx & 31;
+            const int row = rb + rr, col = cb + 2 * q2;
+            const bool ok = row < m && col < m;
+            const double* src = A + (ok ? (int64_t)row * ld + col : (int64_t)rb * ld + k0);
+            cp_async16(sC[rr] + 2 * q2, src, ok);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
         if (tid < kFb) sD[tid] = dD[r0 + k0 + tid];
         // warp w: rows 16 (w >> 1) .. + 16 (two 8-row tiles), columns
         // 32 (w & 1) .. + 32 (four 8-column tiles) of the 64 x 64 output
@@ -600,9 +612,9 @@ __global__ void __launch_bounds__(kT, 3) batch_ldlt_update_kernel(int s, int cnt
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             if (h == 0)
-                asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+                asm volatile("cp.async.wait_group 2;\n" ::: "memory");
             else
-                asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                asm volatile("cp.async.wait_group 1;\n" ::: "memory");
             __syncthreads();
 #pragma unroll
             for (int kq = h * 32; kq < h * 32 + 32; kq += 4) {
@@ -618,6 +630,8 @@ __global__ void __launch_bounds__(kT, 3) batch_ldlt_update_kernel(int s, int cnt
                     for (int j = 0; j < 4; ++j) dmma_m8n8k4(acc[i][j], a[i], b[j]);
             }
         }
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();  // the output tile is in shared memory
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
             const int gr = rb + wr + 8 * i + fr;
@@ -627,7 +641,7 @@ __global__ void __launch_bounds__(kT, 3) batch_ldlt_update_kernel(int s, int cnt
 #pragma unroll
                 for (int t = 0; t < 2; ++t) {
                     const int gc = cb + wc + 8 * j + 2 * fk + t;
-                    if (gc <= gr) A[(int64_t)gr * ld + gc] -= acc[i][j][t];
+                    if (gc <= gr) A[(int64_t)gr * ld + gc] = sC[wr + 8 * i + fr][wc + 8 * j + 2 * fk + t] - acc[i][j][t];
                 }
             }
         }

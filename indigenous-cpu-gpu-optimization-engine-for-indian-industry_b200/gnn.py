@@ -190,8 +190,9 @@ class Batch:
         rp, ci, self.m_off, self.n_off = pack(lps)
         self.m, self.n = int(self.m_off[-1]), int(self.n_off[-1])
         vr, vc = zip(*(normalised_values(lp) for lp in lps))
-        self.Ar = hn.Csr(self.m, self.n, rp, ci, np.concatenate(vr))
-        self.Ac = hn.Csr(self.m, self.n, rp, ci, np.concatenate(vc))
+        # the aggregations use the SpMM kernel, not the SpMV paths: no autotuning
+        self.Ar = hn.Csr(self.m, self.n, rp, ci, np.concatenate(vr), autotune=False)
+        self.Ac = hn.Csr(self.m, self.n, rp, ci, np.concatenate(vc), autotune=False)
         F = [features(lp) for lp in lps]
         dev = "cuda"
         self.Fv = torch.as_tensor(np.concatenate([f[0] for f in F]), device=dev)

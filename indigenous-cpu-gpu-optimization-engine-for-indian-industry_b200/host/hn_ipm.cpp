@@ -771,9 +771,13 @@ InteriorPointResult InteriorPointSolver::solve(const model::LpProblem& problem) 
                 numerical_error = true;
                 break;
             }
-            if (O.verbose)
-                std::fprintf(stderr, "IPM it=%zu mu=%g rp=%g rd=%g ap=%g ad=%g\n", iter, mu, sc[HN_IPM_NRP],
-                             sc[HN_IPM_NRD], sc[HN_IPM_AP], sc[HN_IPM_AD]);
+            if (O.verbose) {
+                double dreg = 0.0;
+                ck(hn_memcpy_d2h(&dreg, dyn.p, 8, st), "D2H dyn_reg");
+                std::fprintf(stderr, "IPM it=%zu mu=%g rp=%g rd=%g ap=%g ad=%g dyn_reg=%g kkt=%g (%g %g %g)\n", iter,
+                             mu, sc[HN_IPM_NRP], sc[HN_IPM_NRD], sc[HN_IPM_AP], sc[HN_IPM_AD], dreg, kv[0], kv[1],
+                             kv[2], kv[3]);
+            }
             result.iterations = iter + 1;
         }
         double last_nrp = 0.0;
