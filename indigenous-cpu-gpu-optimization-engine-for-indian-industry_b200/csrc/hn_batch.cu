@@ -403,7 +403,7 @@ __device__ __forceinline__ void dmma_m8n8k4(double* d, double a, double b) {
                  : "d"(a), "d"(b));
 }
 constexpr int kFbP = kFb + 1;  // padded smem row (conflict-free column walks)
-constexpr size_t kPanelSmem = sizeof(double) * (kFb * kFbP + kFb);
+constexpr size_t kPanelSmem = sizeof(double) * (2 * kFb * kFbP + kFb);
 
 __global__ void __launch_bounds__(kT) batch_ldlt_diag_kernel(int s, const int64_t* __restrict__ row_off,
                                                              const int64_t* __restrict__ dn_off,
@@ -413,7 +413,8 @@ __global__ void __launch_bounds__(kT) batch_ldlt_diag_kernel(int s, const int64_
                                                              double tol) {
     extern __shared__ double smem[];
     double(*sA)[kFbP] = reinterpret_cast<double(*)[kFbP]>(smem);
-    double* sD = smem + kFb * kFbP;
+    double(*sL)[kFbP] = reinterpret_cast<double(*)[kFbP]>(smem + kFb * kFbP);
+    double* sD = smem + 2 * kFb * kFbP;
     const int tid = threadIdx.x;
     const int inst = order[blockIdx.x];
     if (status[inst] != ST_RUN) return;
@@ -429,25 +430,27 @@ __global__ void __launch_bounds__(kT) batch_ldlt_diag_kernel(int s, const int64_
         sA[r][c] = (r < nb && c <= r) ? A[(int64_t)(k0 + r) * ld + k0 + c] : 0.0;
     }
     __syncthreads();
+    // pivot j: every thread forms the clamped pivot itself; warp w takes rows
+    // rr = j + 1 + w, j + 9 + w, ..., lanes the columns j < cc <= rr; each
+    // element takes A_rr,cc -= (l_rr d) l_cc with l = A_.,j / d, the sequence
+    // and roundings of the column-by-column elimination; L goes to sL so
+    // column j stays unscaled for the other warps within the step
+    const int lane = tid & 31, warp = tid >> 5;
     for (int j = 0; j < nb; ++j) {
-        if (tid == 0) {
-            double d = sA[j][j];
-            if (d <= tol) d = tol;  // SparseCholesky pivot clamp
-            sD[j] = d;
-        }
-        __syncthreads();
-        for (int r = j + 1 + tid; r < nb; r += kT) sA[r][j] = sA[r][j] / sD[j];
-        __syncthreads();
-        const int w = nb - j - 1;
-        for (int idx = tid; idx < w * w; idx += kT) {
-            const int rr = j + 1 + idx / w, cc = j + 1 + idx % w;
-            if (cc <= rr) sA[rr][cc] -= (sA[rr][j] * sD[j]) * sA[cc][j];
+        double d = sA[j][j];
+        if (d <= tol) d = tol;  // SparseCholesky pivot clamp
+        if (tid == 0) sD[j] = d;
+        for (int rr = j + 1 + warp; rr < nb; rr += kT / 32) {
+            const double lr = sA[rr][j] / d;
+            const double wr = lr * d;
+            for (int cc = j + 1 + lane; cc <= rr; cc += 32) sA[rr][cc] -= wr * (sA[cc][j] / d);
+            if (lane == 0) sL[rr][j] = lr;
         }
         __syncthreads();
     }
     for (int idx = tid; idx < nb * nb; idx += kT) {
         const int r = idx / nb, c = idx % nb;
-        if (c < r) A[(int64_t)(k0 + r) * ld + k0 + c] = sA[r][c];
+        if (c < r) A[(int64_t)(k0 + r) * ld + k0 + c] = sL[r][c];
     }
     if (tid < nb) dD[r0 + k0 + tid] = sD[tid];
 }
@@ -490,6 +493,9 @@ __global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, int cnt, co
     __syncthreads();
     const int r = k1 + static_cast<int>(local) * kT + tid;
     if (r >= m) return;
+    // lv[c] holds A[r, k0 + c] until column c is final; then L[r, c] goes to
+    // memory and lv[c] keeps L[r, c] D_c, the factor every later column
+    // multiplies (the same single rounding as computing it there each time)
     double lv[kFb];
     double* Ar = A + (int64_t)r * ld + k0;
 #pragma unroll
@@ -499,13 +505,12 @@ __global__ void __launch_bounds__(kT) batch_ldlt_panel_kernel(int s, int cnt, co
         if (c < nb) {
             double v = lv[c];
 #pragma unroll
-            for (int q = 0; q < c; ++q) v -= (lv[q] * sD[q]) * sL[c][q];
-            lv[c] = v / sD[c];
+            for (int q = 0; q < c; ++q) v -= lv[q] * sL[c][q];
+            const double l = v / sD[c];
+            Ar[c] = l;
+            lv[c] = l * sD[c];
         }
     }
-#pragma unroll
-    for (int c = 0; c < kFb; ++c)
-        if (c < nb) Ar[c] = lv[c];
 }
 
 // Trailing update of one 64 x 64 tile pair per CTA iteration. Both 64-column
@@ -1016,6 +1021,9 @@ int hn_batch_create(int64_t K, const int64_t* row_off_host, const int64_t* col_o
             check_cuda(cudaFuncSetAttribute(batch_ldlt_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)kUpdSmem),
                        "update smem attribute");
+            check_cuda(cudaFuncSetAttribute(batch_ldlt_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kPanelSmem),
+                       "diagonal-block smem attribute");
             B->ref_iter = dmalloc<int32_t>(K);
             B->kkt = dmalloc<double>(4 * K);
             B->kkt_ref = dmalloc<double>(4 * K);

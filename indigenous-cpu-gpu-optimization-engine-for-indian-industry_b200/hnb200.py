@@ -633,6 +633,10 @@ def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=
     opt.verbose = int(verbose)
     cb = INTERRUPT_CB(lambda _u: int(bool(interrupt()))) if interrupt is not None else INTERRUPT_CB()
     opt.interrupt_cb = cb
+    # the C API reads n (x, s) and m (y) entries: a point of another size is
+    # not a warm start for this LP and is not passed at all
+    if any(a is not None and np.asarray(a).shape != (k,) for a, k in ((x0, n), (y0, m), (s0, n))):
+        x0 = y0 = s0 = None
     keep = _warm_arrays(opt, x0, y0, s0)  # noqa: F841 (alive through the call)
     if warm_floor is not None:
         opt.warm_start_floor = warm_floor
@@ -693,6 +697,10 @@ def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs
     opt.device = device
     opt.kkt_tol = float(kkt_tol)
     opt.kkt_extra_iterations = int(kkt_extra)
+    for arrs, key in ((x0s, "n"), (y0s, "m"), (s0s, "n")):
+        if arrs is not None and (len(arrs) != K or any(np.asarray(a).shape != (int(lp[key]),)
+                                                       for a, lp in zip(arrs, lps))):
+            raise ValueError(f"warm-start arrays must have one entry per instance of length {key}")
     keep = _warm_arrays(opt, None if x0s is None else np.concatenate(x0s),  # noqa: F841
                         None if y0s is None else np.concatenate(y0s), None if s0s is None else np.concatenate(s0s))
     if warm_floor is not None:
