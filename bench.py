@@ -463,7 +463,7 @@ def bb_batch(K: int, chunk: int, sample: int = 2):
     t0 = time.perf_counter()
     r0 = hn.lp_solve(base)
     base_s = time.perf_counter() - t0
-    status, obj, iters, used = [], [], [], []
+    status, obj, iters, used, kkt = [], [], [], [], []
     t0 = time.perf_counter()
     for c0 in range(0, K, chunk):
         part = nodes[c0:c0 + chunk]
@@ -473,9 +473,10 @@ def bb_batch(K: int, chunk: int, sample: int = 2):
         obj.append(r["objective"])
         iters.append(r["iterations"])
         used.append(r["warm_used"])
+        kkt.append(r["kkt"][:, 0])
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
-    status, obj, iters, used = map(np.concatenate, (status, obj, iters, used))
+    status, obj, iters, used, kkt = map(np.concatenate, (status, obj, iters, used, kkt))
     pt, matched = [], 0
     for i in range(sample):
         t1 = time.perf_counter()
@@ -490,6 +491,7 @@ def bb_batch(K: int, chunk: int, sample: int = 2):
             "batched_s": round(wall, 2), "batched_solves_per_s": round(K / wall, 2),
             "status_counts": {int(k): int(v) for k, v in zip(*np.unique(status, return_counts=True))},
             "warm_used": int(used.sum()), "iterations_mean": round(float(iters.mean()), 2),
+            "kkt_le_1e-8": int(((status == 1) & (kkt <= 1e-8)).sum()), "kkt_median": float(np.nanmedian(kkt)),
             "plain_gpu_s_extrapolated": round(est, 1), "plain_gpu_solves_per_s_extrapolated": round(K / est, 3),
             "speedup_vs_plain_gpu": round(est / wall, 2), "plain_sample": {"instances": sample, "matching": matched}}
 

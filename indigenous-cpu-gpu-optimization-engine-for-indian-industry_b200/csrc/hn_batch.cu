@@ -703,14 +703,20 @@ __global__ void __launch_bounds__(kFb) batch_fwd_diag_kernel(int s, const int64_
         const int r = idx / kFb, c = idx % kFb;
         sL[r][c] = (r < nb && c < r) ? L[(int64_t)(k0 + r) * ld + k0 + c] : 0.0;
     }
-    double v = i < nb ? x[k0 + i] : 0.0;
+    sy[i] = i < nb ? x[k0 + i] : 0.0;
     __syncthreads();
+    // warp 0 runs the substitution, rows lane and lane + 32, broadcasting
+    // each solved entry by a shuffle (no barriers); same operations per
+    // entry in the same order as a row-per-thread substitution
+    if (i >= 32) return;
+    double v0 = sy[i], v1 = sy[i + 32];
     for (int j = 0; j < nb; ++j) {
-        if (i == j) sy[j] = v;
-        __syncthreads();
-        if (i > j && i < nb) v -= sL[i][j] * sy[j];
+        const double yj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
+        if (i > j && i < nb) v0 -= sL[i][j] * yj;
+        if (i + 32 > j && i + 32 < nb) v1 -= sL[i + 32][j] * yj;
     }
-    if (i < nb) x[k0 + i] = v;
+    if (i < nb) x[k0 + i] = v0;
+    if (i + 32 < nb) x[k0 + i + 32] = v1;
 }
 
 __global__ void __launch_bounds__(kT) batch_fwd_gemv_kernel(int s, int cnt, const int64_t* __restrict__ chunks,
@@ -842,14 +848,19 @@ __global__ void __launch_bounds__(kFb) batch_bwd_diag_kernel(int s, const int64_
     double t = 0.0;
     if (q < nb)
         for (int64_t ch = c0; ch < c1; ++ch) t += part[ch * kFb + q];
-    double v = q < nb ? x[k0 + q] - t : 0.0;
+    sxj[q] = q < nb ? x[k0 + q] - t : 0.0;
     __syncthreads();
+    // warp 0 runs the back substitution over rows lane and lane + 32 with
+    // shuffle broadcasts (no barriers), operations as row-per-thread
+    if (q >= 32) return;
+    double v0 = sxj[q], v1 = sxj[q + 32];
     for (int j = nb - 1; j >= 0; --j) {
-        if (q == j) sxj[j] = v;
-        __syncthreads();
-        if (q < j) v -= sL[j][q] * sxj[j];
+        const double xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
+        if (q < j) v0 -= sL[j][q] * xj;
+        if (q + 32 < j) v1 -= sL[j][q + 32] * xj;
     }
-    if (q < nb) x[k0 + q] = v;
+    if (q < nb) x[k0 + q] = v0;
+    if (q + 32 < nb) x[k0 + q + 32] = v1;
 }
 
 // Refinement bookkeeping per instance (refinement.cpp:15-30): with r = rhs - N x,
