@@ -573,6 +573,9 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
     warm_s = time.perf_counter() - t0
     same = (cold["status"] == warm["status"]) & (np.abs(cold["objective"] - warm["objective"]) <=
                                                   1e-8 * (1 + np.abs(cold["objective"])))
+    # the batched factorisation's work is ~ iterations x m^3 per instance
+    m3 = np.array([float(lp["m"]) ** 3 for lp in eval_lps])
+    work_ratio = float((warm["iterations"] * m3).sum() / (cold["iterations"] * m3).sum())
     pt = []
     for i in range(min(plain_sample, n_eval)):
         t1 = time.perf_counter()
@@ -589,6 +592,7 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
             "warm_inference_s": round(infer[0], 2),
             "iterations_mean_cold": round(float(cold["iterations"].mean()), 2),
             "iterations_mean_warm": round(float(warm["iterations"].mean()), 2),
+            "factor_work_warm_over_cold": round(work_ratio, 4),
             "warm_used": int(warm["warm_used"].sum()), "optimal_cold": int((cold["status"] == 1).sum()),
             "optimal_warm": int((warm["status"] == 1).sum()),
             "kkt_le_1e-8_cold": int(((cold["status"] == 1) & (cold["kkt"] <= 1e-8)).sum()),
