@@ -436,6 +436,8 @@ def batched_ipm(K: int, sample_per_stratum: int = 4, rank: int = 0, world: int =
             "iterations_mean": round(float(r["iterations"].mean()), 2),
             "reference_rule_iterations_mean": round(float(r["reference_iterations"].mean()), 2),
             "factor_ms": round(r["stats"]["factor_ms"], 1), "solve_ms": round(r["stats"]["solve_ms"], 1),
+            "forms_ms": round(r["stats"]["forms_ms"], 1), "setup_ms": round(r["stats"]["setup_ms"], 1),
+            "total_ms": round(r["stats"]["total_ms"], 1),
             "factor_fp64_tflops": round(factor_flops / (r["stats"]["factor_ms"] * 1e-3) / 1e12, 2),
             "plain_gpu_s_extrapolated": round(est, 2) if sampled else None,
             "plain_gpu_solves_per_s_extrapolated": round(K / est, 2) if sampled else None,

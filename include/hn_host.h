@@ -102,6 +102,8 @@ typedef struct hn_batch_stats {
     int64_t rows, cols, nnz, nnz_normal;
     int64_t iterations;
     double total_ms, factor_ms, solve_ms;
+    double forms_ms;  /* host: standard forms and start points of every instance */
+    double setup_ms;  /* device matrix, A^T, A D A^T pattern and batch tables */
 } hn_batch_stats;
 int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off, const int64_t* nnz_off,
                       const uint64_t* row_ptr, const uint64_t* col_idx, const double* val, const double* c,

@@ -664,7 +664,7 @@ def lp_solve(lp: dict, sense=None, lb=None, ub=None, maximize=False, obj_offset=
 class BatchStats(C.Structure):
     _fields_ = [("rows", C.c_int64), ("cols", C.c_int64), ("nnz", C.c_int64), ("nnz_normal", C.c_int64),
                 ("iterations", C.c_int64), ("total_ms", C.c_double), ("factor_ms", C.c_double),
-                ("solve_ms", C.c_double)]
+                ("solve_ms", C.c_double), ("forms_ms", C.c_double), ("setup_ms", C.c_double)]
 
 
 def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs=None, x0s=None, y0s=None,

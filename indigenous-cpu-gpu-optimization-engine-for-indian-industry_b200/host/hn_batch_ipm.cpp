@@ -54,6 +54,7 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
     try {
         PackedForm pf;
         build_forms(problems, O.feasibility_tol, pf, warm, O.warm_start_floor);
+        stats_.forms_ms = ms_since(start);
         const std::size_t m = pf.row_off.back(), n = pf.col_off.back();
         stats_.rows = m;
         stats_.cols = n;
@@ -97,6 +98,7 @@ std::vector<InteriorPointResult> BatchInteriorPointSolver::solve(const std::vect
             for (int32_t v : hstatus) running += (v == 0);
             return running;
         };
+        stats_.setup_ms = ms_since(start) - stats_.forms_ms;
         const int max_it = O.max_iterations;
         int iter = 0;
         bool time_up = false;

@@ -293,6 +293,8 @@ int hn_lp_solve_batch(int64_t K, const int64_t* row_off, const int64_t* col_off,
             stats->total_ms = S.total_ms;
             stats->factor_ms = S.factor_ms;
             stats->solve_ms = S.solve_ms;
+            stats->forms_ms = S.forms_ms;
+            stats->setup_ms = S.setup_ms;
         }
         if (!S.error.empty()) throw std::runtime_error(S.error);
     });

@@ -174,6 +174,7 @@ struct BatchStats {
     std::size_t rows = 0, cols = 0, nnz = 0, nnz_normal = 0;
     int iterations = 0;
     double total_ms = 0.0, factor_ms = 0.0, solve_ms = 0.0;
+    double forms_ms = 0.0, setup_ms = 0.0;  // host standard forms and start points; device matrix, pattern, batch
     std::vector<std::size_t> running_per_iter;
     std::string error;
 };
