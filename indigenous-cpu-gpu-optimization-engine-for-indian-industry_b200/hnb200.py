@@ -157,6 +157,15 @@ def u64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.uint64)
 
 
+def _as_u64(a: np.ndarray) -> np.ndarray:
+    """Index array as uint64: int64 input is reinterpreted in place when
+    non-negative, anything else converted."""
+    a = np.ascontiguousarray(a)
+    if a.dtype == np.int64 and (a.size == 0 or a.min() >= 0):
+        return a.view(np.uint64)
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
 def f64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
 
@@ -681,8 +690,10 @@ def lp_solve_batch(lps: list, max_iter=100, device=0, senses=None, lbs=None, ubs
         row_off[i + 1] = row_off[i] + lp["m"]
         col_off[i + 1] = col_off[i] + lp["n"]
         nnz_off[i + 1] = nnz_off[i] + len(lp["ci"])
-    rp = u64(np.concatenate([np.asarray(lp["rp"], np.uint64) for lp in lps]))
-    ci = u64(np.concatenate([np.asarray(lp["ci"], np.uint64) for lp in lps]))
+    # one concatenation, then the non-negative int64 indices reinterpreted
+    # as uint64 (a per-instance conversion costs ten times as much)
+    rp = _as_u64(np.concatenate([np.asarray(lp["rp"]) for lp in lps]))
+    ci = _as_u64(np.concatenate([np.asarray(lp["ci"]) for lp in lps]))
     val = f64(np.concatenate([lp["val"] for lp in lps]))
     c = f64(np.concatenate([lp["c"] for lp in lps]))
     b = f64(np.concatenate([lp["b"] for lp in lps]))

@@ -13,6 +13,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <unordered_set>
 
 #include "hn_lp.hpp"
@@ -85,25 +86,51 @@ void csr_from_triplets(std::size_t rows, std::vector<Trip>& t, std::vector<std::
 }
 
 // remove_duplicate_rows (interior_point.cpp:79-132): a row equal to an
-// earlier one in entries (sorted), sense and rhs bits is dropped.
+// earlier one in entries (sorted by column, then value), sense and rhs bits
+// is dropped. Rows are compared through a 64-bit hash of that key and then
+// exactly (the reference compares decimal string keys of the same fields).
 model::LpProblem remove_duplicate_rows(const model::LpProblem& p) {
     if (p.num_rows == 0) return p;
-    std::unordered_set<std::string> seen;
-    std::vector<std::size_t> keep;
-    for (std::size_t i = 0; i < p.num_rows; ++i) {
-        std::vector<std::pair<std::size_t, double>> ent;
+    using Entry = std::pair<std::size_t, double>;
+    auto bits = [](double v) {
+        std::uint64_t b;
+        std::memcpy(&b, &v, 8);
+        return b;
+    };
+    auto row_entries = [&](std::size_t i) {
+        std::vector<Entry> ent;
+        ent.reserve(p.row_ptr[i + 1] - p.row_ptr[i]);
         for (std::size_t k = p.row_ptr[i]; k < p.row_ptr[i + 1]; ++k) ent.emplace_back(p.col_indices[k], p.values[k]);
         std::sort(ent.begin(), ent.end());
-        std::string key;
-        for (const auto& e : ent) {
-            std::uint64_t bv;
-            std::memcpy(&bv, &e.second, 8);
-            key += std::to_string(e.first) + ':' + std::to_string(bv) + ';';
+        return ent;
+    };
+    auto same = [&](const std::vector<Entry>& a, std::size_t ia, const std::vector<Entry>& b, std::size_t ib) {
+        if (p.sense[ia] != p.sense[ib] || bits(p.rhs[ia]) != bits(p.rhs[ib]) || a.size() != b.size()) return false;
+        for (std::size_t k = 0; k < a.size(); ++k)
+            if (a[k].first != b[k].first || bits(a[k].second) != bits(b[k].second)) return false;
+        return true;
+    };
+    std::unordered_map<std::uint64_t, std::vector<std::size_t>> seen;  // hash -> kept rows
+    std::vector<std::vector<Entry>> kept_ent;
+    std::vector<std::size_t> keep;
+    for (std::size_t i = 0; i < p.num_rows; ++i) {
+        std::vector<Entry> ent = row_entries(i);
+        std::uint64_t h = 0x9e3779b97f4a7c15ull ^ bits(p.rhs[i]) ^ (static_cast<std::uint64_t>(p.sense[i]) << 61);
+        for (const Entry& e : ent) {
+            h ^= e.first + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+            h ^= bits(e.second) + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
         }
-        std::uint64_t br;
-        std::memcpy(&br, &p.rhs[i], 8);
-        key += '|' + std::to_string(static_cast<int>(p.sense[i])) + ':' + std::to_string(br);
-        if (seen.insert(key).second) keep.push_back(i);
+        auto& bucket = seen[h];
+        bool dup = false;
+        for (std::size_t q : bucket)
+            if (same(kept_ent[q], keep[q], ent, i)) {
+                dup = true;
+                break;
+            }
+        if (dup) continue;
+        bucket.push_back(keep.size());
+        keep.push_back(i);
+        kept_ent.push_back(std::move(ent));
     }
     if (keep.size() == p.num_rows) return p;
     model::LpProblem q = p;
@@ -113,11 +140,9 @@ model::LpProblem remove_duplicate_rows(const model::LpProblem& p) {
     q.values.clear();
     q.sense.clear();
     q.rhs.clear();
-    for (std::size_t i : keep) {
-        std::vector<std::pair<std::size_t, double>> ent;
-        for (std::size_t k = p.row_ptr[i]; k < p.row_ptr[i + 1]; ++k) ent.emplace_back(p.col_indices[k], p.values[k]);
-        std::sort(ent.begin(), ent.end());
-        for (const auto& e : ent) {
+    for (std::size_t t = 0; t < keep.size(); ++t) {
+        const std::size_t i = keep[t];
+        for (const Entry& e : kept_ent[t]) {
             q.col_indices.push_back(e.first);
             q.values.push_back(e.second);
         }
@@ -222,11 +247,25 @@ StandardForm build_standard_form(const model::LpProblem& p, double feas_tol) {
     for (std::size_t k = 0; k < f.val.size(); ++k) colmax[f.ci[k]] = std::max(colmax[f.ci[k]], std::abs(f.val[k]));
     for (std::size_t j = 0; j < ncols; ++j)
         if (colmax[j] > 0.0) f.col_scale[j] = 1.0 / colmax[j];
-    std::vector<Trip> scaled;
-    scaled.reserve(f.val.size());
-    for (std::size_t i = 0; i < m_rows; ++i)
-        for (std::size_t k = f.rp[i]; k < f.rp[i + 1]; ++k) scaled.push_back({i, f.ci[k], f.val[k] * f.col_scale[f.ci[k]]});
-    csr_from_triplets(m_rows, scaled, f.rp, f.ci, f.val);
+    // the scaled matrix: the reference rebuilds it from triplets; the
+    // pattern is already sorted and duplicate-free, so that amounts to
+    // scaling in place and dropping entries that became exactly zero
+    {
+        std::size_t w = 0, k = 0;
+        for (std::size_t i = 0; i < m_rows; ++i) {
+            const std::size_t e = f.rp[i + 1];
+            for (; k < e; ++k) {
+                const double v = f.val[k] * f.col_scale[f.ci[k]];
+                if (v == 0.0) continue;
+                f.ci[w] = f.ci[k];
+                f.val[w] = v;
+                ++w;
+            }
+            f.rp[i + 1] = w;
+        }
+        f.ci.resize(w);
+        f.val.resize(w);
+    }
     for (std::size_t j = 0; j < ncols; ++j) f.c[j] *= f.col_scale[j];
     return f;
 }
