@@ -657,7 +657,10 @@ def pricing(A, m, n, steps, warmup, flush):
 def gnn_layer(steps, warmup, rows=1 << 20):
     """One 128 -> 64 GNN layer over `rows` rows (X = [X1 | X2], FP32, 512 MB
     at 2^20 rows): the tcgen05 kernel and the mma.sync kernel, per call time
-    (CUDA events; the input exceeds L2), bytes (X read, Y written) and flops."""
+    (CUDA events; the input exceeds L2), bytes (X read, Y written) and flops;
+    and its backward (hn_gnn_linear_bwd: G = dY relu'(Y), dX = G W^T and
+    dW = X^T G on the tcgen05 kernels) with bytes Y, dY read, G written and
+    read twice, dX written, X read."""
     import torch
 
     import hnb200 as hn
@@ -670,6 +673,13 @@ def gnn_layer(steps, warmup, rows=1 << 20):
     Wt = torch.empty(128 * 64, dtype=torch.bfloat16, device="cuda")
     Wb = torch.empty(128 * 64, dtype=torch.bfloat16, device="cuda")
     Y = torch.empty((rows, 64), device="cuda")
+    dY = torch.randn((rows, 64), generator=g, device="cuda")
+    G = torch.empty((rows, 64), device="cuda")
+    dX = torch.empty((rows, 128), device="cuda")
+    dW = torch.empty(128 * 64, device="cuda")
+    db = torch.empty(64, device="cuda")
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    scratch = torch.empty(sms * (128 * 64 + 64), device="cuda")
     lib = hn.load()
     hn.check(lib.hn_gnn_cast_weights(128, W.data_ptr(), Wt.data_ptr(), Wb.data_ptr(), None))
     calls = {
@@ -677,10 +687,14 @@ def gnn_layer(steps, warmup, rows=1 << 20):
                                                            b.data_ptr(), 1, Y.data_ptr(), None)),
         "mma_sync": lambda: hn.check(lib.hn_gnn_linear(rows, 64, 64, X1.data_ptr(), X2.data_ptr(), Wt.data_ptr(), 64,
                                                        b.data_ptr(), 1, Y.data_ptr(), None)),
+        "backward_tcgen05": lambda: hn.check(lib.hn_gnn_linear_bwd(
+            rows, 64, 64, X1.data_ptr(), X2.data_ptr(), Wb.data_ptr(), Y.data_ptr(), dY.data_ptr(), 1, G.data_ptr(),
+            dX.data_ptr(), dW.data_ptr(), db.data_ptr(), scratch.data_ptr(), scratch.numel(), None)),
     }
-    nbytes = rows * (128 * 4 + 64 * 4)
-    flops = 2 * rows * 128 * 64
-    res = {"workload": f"GNN layer [X1 | X2] ({rows} x 128, FP32) x W (128 x 64, BF16) + b, ReLU"}
+    fwd_bytes, fwd_flops = rows * (128 * 4 + 64 * 4), 2 * rows * 128 * 64
+    work = {"tcgen05": (fwd_bytes, fwd_flops), "mma_sync": (fwd_bytes, fwd_flops),
+            "backward_tcgen05": (rows * 4 * (64 * 3 + 64 * 2 + 128 + 128), 2 * 2 * rows * 128 * 64)}
+    res = {"workload": f"GNN layer [X1 | X2] ({rows} x 128, FP32) x W (128 x 64, BF16) + b, ReLU, and its backward"}
     hn.check(lib.hn_gnn_check(None))
     for name, fn in calls.items():
         for _ in range(warmup):
@@ -696,6 +710,7 @@ def gnn_layer(steps, warmup, rows=1 << 20):
             ts.append(e0.elapsed_time(e1))
         ms = sorted(ts)[steps // 2]
         hn.check(lib.hn_gnn_check(None))
+        nbytes, flops = work[name]
         res[name] = {"us": round(ms * 1e3, 1), "GB/s": round(nbytes / (ms * 1e-3) / 1e9, 1),
                      "TFLOP/s": round(flops / (ms * 1e-3) / 1e12, 2)}
     return res

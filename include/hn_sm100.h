@@ -418,7 +418,8 @@ int hn_gnn_linear_umma(int64_t M, int K1, int K2, const float* X1_dev, const flo
                        const float* bias_dev, int relu, float* Y_dev, void* stream);
 int hn_gnn_check(void* stream);
 /* Test hook of the bounded waits above (no reference counterpart): the
- * tcgen05 layer's pipeline waits (bulk copies in, MMA done) give up after
+ * pipeline waits of the tcgen05 kernels (the layer and both GEMMs of its
+ * backward: bulk copies in, MMA done) give up after
  * `polls` non-blocking mbarrier polls instead of 2^24 blocking ones (0
  * restores the default). A call with a small limit gives up while its own
  * copies are in flight; the CTA then
@@ -428,7 +429,12 @@ int hn_gnn_check(void* stream);
 int hn_gnn_set_wait_limit(uint32_t polls);
 /* Backward of hn_gnn_linear with N = 64: G = dY * relu'(Y); dX (M x K, may be
  * NULL; K = 64 or 128) = G W^T; dW (K x 64) = [X1 | X2]^T G; db (64) = sum of
- * G's rows. scratch: >= ceil(M / 64) * (64 K + 64) floats. Deterministic. */
+ * G's rows. dX and dW run on the tcgen05 tensor cores (BF16 operands, FP32
+ * accumulation in tensor memory; dW as one partial per persistent CTA,
+ * summed in a fixed order). scratch: >= min(ceil(M / 64), SM count) *
+ * (64 K + 64) floats. X1, X2, G, dX, Wb and scratch 16-byte aligned.
+ * Deterministic on a given GPU. A timed-out wait sets the flag that
+ * hn_gnn_check reports. */
 int hn_gnn_linear_bwd(int64_t M, int K1, int K2, const float* X1_dev, const float* X2_dev, const void* Wb_bf16_dev,
                       const float* Y_dev, const float* dY_dev, int relu, float* G_dev, float* dX_dev, float* dW_dev,
                       float* db_dev, float* scratch_dev, int64_t scratch_floats, void* stream);

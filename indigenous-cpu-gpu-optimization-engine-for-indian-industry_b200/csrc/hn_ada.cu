@@ -343,24 +343,35 @@ __global__ void __launch_bounds__(kT, 4) ada_slot_kernel(int64_t nnz, const uint
 // Relative map: one warp per row of N at a time (rows handed out longest
 // first), kRmapU slots per lane per trip, the next trip's map words loaded
 // before this trip's gathers. A single-term slot's word gives its A entry
-// within row i (e = rp_A[i] + high bits) and its A^T entry within row j of A^T
-// (ecs[e] + low bits); (A value x A^T value) x d is the slot kernel's
-// arithmetic, so the layouts give the same bits. The row's A entries are
-// read through L1 (a row of A is a few cache lines, reused by every slot of
-// the row); the A^T values are gathered from L2 without allocating in L1
-// (they would evict the row's entries); the map streams from HBM once.
+// within row i (high bits: e - rp_A[i]) and its A^T entry within row j of
+// A^T (low bits: p - rp_AT[j]). The warp first stages its row's A entries --
+// (A value, d) and the start of the A^T row of their column -- in its own
+// shared-memory slice (rows of A are at most kRmapTerms long in this
+// layout), so a slot costs one 4-byte map word from HBM, two shared loads
+// and one A^T value gathered through L1 (the slots of a row walk each of its
+// A^T rows in order, so neighbouring values share lines). (A value x A^T
+// value) x d is the slot kernel's arithmetic, so the layouts give the same
+// bits. Every index read from the map is clamped into its table, so a
+// corrupt map gives wrong values, never an access outside the buffers.
 constexpr int kRmapU = 8;
-__global__ void __launch_bounds__(kT, 3) ada_rmap_kernel(int m, const int32_t* __restrict__ order,
-                                                         unsigned* __restrict__ row_next,
-                                                         const int32_t* __restrict__ rpA,
-                                                         const double2* __restrict__ vd,
-                                                         const int32_t* __restrict__ ecs,
-                                                         const double* __restrict__ valT,
-                                                         const int64_t* __restrict__ rpN,
-                                                         const int64_t* __restrict__ msrow,
-                                                         const uint32_t* __restrict__ rmap, int qbits,
-                                                         const double* __restrict__ mval, double* __restrict__ nval) {
-    const int lane = threadIdx.x & 31;
+constexpr int kRmapT = 256;      // threads (8 warps, one row each)
+constexpr int kRmapTerms = 256;  // longest row of A this layout takes
+__global__ void __launch_bounds__(kRmapT, 3) ada_rmap_kernel(int m, const int32_t* __restrict__ order,
+                                                             unsigned* __restrict__ row_next,
+                                                             const int32_t* __restrict__ rpA,
+                                                             const double2* __restrict__ vd,
+                                                             const int32_t* __restrict__ ecs,
+                                                             const double* __restrict__ valT, int64_t nnzA,
+                                                             const int64_t* __restrict__ rpN,
+                                                             const int64_t* __restrict__ msrow, int64_t nms,
+                                                             const uint32_t* __restrict__ rmap, int qbits,
+                                                             const double* __restrict__ mval,
+                                                             double* __restrict__ nval) {
+    __shared__ double2 s_q[kRmapT / 32][kRmapTerms];
+    __shared__ int32_t s_cs[kRmapT / 32][kRmapTerms];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double2* sq = s_q[warp];
+    int32_t* scs = s_cs[warp];
     const uint32_t qmask = (1u << qbits) - 1u;
     constexpr int64_t kStep = 32 * kRmapU;
     for (;;) {
@@ -371,7 +382,14 @@ __global__ void __launch_bounds__(kT, 3) ada_rmap_kernel(int m, const int32_t* _
         const int i = __ldg(order + idx);
         const int64_t r0 = __ldg(rpN + i), r1 = __ldg(rpN + i + 1);
         const int e0 = __ldg(rpA + i);
+        const int ne = min(__ldg(rpA + i + 1) - e0, kRmapTerms);
         const int64_t ms0 = __ldg(msrow + i);
+        __syncwarp();  // the previous row's slots are done with the slice
+        for (int t = lane; t < ne; t += 32) {
+            sq[t] = __ldg(vd + e0 + t);
+            scs[t] = __ldg(ecs + e0 + t);
+        }
+        __syncwarp();
         uint32_t g[kRmapU];
 #pragma unroll
         for (int u = 0; u < kRmapU; ++u) {
@@ -386,21 +404,21 @@ __global__ void __launch_bounds__(kT, 3) ada_rmap_kernel(int m, const int32_t* _
                 gn[u] = t < r1 ? __ldcs(rmap + t) : kMulti;
             }
             double2 q[kRmapU];
-            int32_t cs[kRmapU];
-#pragma unroll
-            for (int u = 0; u < kRmapU; ++u) {
-                const int e = (g[u] & kMulti) ? 0 : e0 + static_cast<int>(g[u] >> qbits);
-                q[u] = __ldg(vd + e);
-                cs[u] = __ldg(ecs + e);
-            }
             double b[kRmapU];
 #pragma unroll
             for (int u = 0; u < kRmapU; ++u) {
                 const int64_t t = t0 + u * 32;
-                if (g[u] & kMulti)
-                    b[u] = t < r1 ? __ldcs(mval + ms0 + (g[u] & ~kMulti)) : 0.0;
-                else
-                    b[u] = __ldcg(valT + cs[u] + static_cast<int>(g[u] & qmask));
+                if (g[u] & kMulti) {
+                    const int64_t ms = min(ms0 + (int64_t)(g[u] & ~kMulti), nms - 1);
+                    q[u] = make_double2(0.0, 0.0);
+                    b[u] = t < r1 ? __ldcs(mval + ms) : 0.0;
+                } else {
+                    const int eo = min(static_cast<int>(g[u] >> qbits), kRmapTerms - 1);
+                    q[u] = sq[eo];
+                    int64_t pT = (int64_t)scs[eo] + (int64_t)(g[u] & qmask);
+                    pT = pT < nnzA ? pT : 0;
+                    b[u] = __ldg(valT + pT);
+                }
             }
 #pragma unroll
             for (int u = 0; u < kRmapU; ++u) {
@@ -602,8 +620,8 @@ void launch_numeric(const hn_pattern* P, const double* d, double* nval, cudaStre
     if (P->rmap) {
         check_cuda(cudaMemsetAsync(P->row_next, 0, sizeof(unsigned), s), "memset row counter");
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P->m + 7) / 8, (int64_t)ctx().sm_count * 3));
-        ada_rmap_kernel<<<grid, kT, 0, s>>>((int)P->m, P->order, P->row_next, A->rp, P->vd, P->ecs, A->valT, P->rp,
-                                            P->msrow, P->rmap, P->qbits, P->mval, nval);
+        ada_rmap_kernel<<<grid, kRmapT, 0, s>>>((int)P->m, P->order, P->row_next, A->rp, P->vd, P->ecs, A->valT,
+                                                A->nnz, P->rp, P->msrow, P->nms, P->rmap, P->qbits, P->mval, nval);
         launched("ada_rmap_kernel");
         return;
     }
@@ -728,7 +746,8 @@ int hn_ada_symbolic_ex(const hn_csr* A, unsigned flags, hn_pattern** out) {
                 int64_t maxcol = 1;
                 for (int64_t j = 0; j < A->n; ++j) maxcol = std::max<int64_t>(maxcol, rpT[j + 1] - rpT[j]);
                 while ((int64_t(1) << qbits) < maxcol) ++qbits;
-                const bool fits = qbits < 31 && (int64_t)std::max(maxes[2], 1u) <= (int64_t(1) << (31 - qbits));
+                const bool fits = qbits < 31 && (int64_t)std::max(maxes[2], 1u) <= (int64_t(1) << (31 - qbits)) &&
+                                  maxes[2] <= (unsigned)kRmapTerms;
                 rel = fits && (flags & HN_ADA_RELATIVE);
             }
             P->ci = dmalloc<int32_t>(P->nnz);

@@ -256,7 +256,9 @@ def backward(model: Model, B: Batch, cache: dict):
     hn.check(lib.hn_gnn_head_grad(B.m, cache["oc"].data_ptr(), B.Tc.data_ptr(), 1, 1.0 / B.m, doc.data_ptr(),
                                   lp_c.data_ptr(), nparts, None))
     rows_max = max(B.n, B.m)
-    scratch_len = ((rows_max + 63) // 64) * (H * 2 * H + H)
+    # one dW/db partial per CTA of the weight-gradient kernel (at most one per SM)
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    scratch_len = max(1, min((rows_max + 63) // 64, sms)) * (H * 2 * H + H)
     scratch = torch.empty(scratch_len, dtype=torch.float32, device="cuda")
     G = torch.empty(rows_max * H, dtype=torch.float32, device="cuda")
 
@@ -289,6 +291,7 @@ def backward(model: Model, B: Batch, cache: dict):
         dhv, dhc = ndhv, ndhc
     lin_bwd(B.Fv, None, "ev", hv[0], dhv, 1, B.n, None)
     lin_bwd(B.Fc, None, "ec", hc[0], dhc, 1, B.m, None)
+    hn.check(lib.hn_gnn_check(None))
     return float(lp_v.sum().item()) / B.n + float(lp_c.sum().item()) / B.m
 
 

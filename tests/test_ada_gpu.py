@@ -212,13 +212,16 @@ def test_long_row_of_a_selects_gather_mode(hn, torch_cuda):
     A, P, rp_, ci_, vals_, dyn = assemble(hn, torch_cuda, lp2, D, compact=True)
     assert P.mode()[0] != hn.Pattern.ROW
     check_values(lp2, D, 1e-8, rp_, ci_, vals_, dyn)
+    # the relative map stages a row's entries in a 256-entry slice: not taken either
+    assert hn.Pattern(A, layout=hn.Pattern.RELATIVE).mode()[0] == hn.Pattern.GATHER
 
 
 def test_row_layout_long_rows_bit_identical_to_gather(hn, torch_cuda):
     """Rows of N longer than the row layout's 8,192-slot shared-memory window
     (m 30,000, n 90,000, 60 nonzeros per column: ~9,000 slots per row, rows of
     A 180 entries on average, 236 at most): the row layout assembles each row
-    in several windows and
+    in several windows, the relative map stages rows of A of up to 236
+    entries in its warp's shared slice, and both
     must give the gather layout's bits (the gather layout is pinned to the
     oracle by the tests above)."""
     torch = torch_cuda
@@ -229,7 +232,7 @@ def test_row_layout_long_rows_bit_identical_to_gather(hn, torch_cuda):
     A = hn.Csr(m, n, lp["rp"], lp["ci"], lp["val"])
     Dd = torch.as_tensor(D, device="cuda")
     out = []
-    for layout in (hn.Pattern.ROW, hn.Pattern.GATHER):
+    for layout in (hn.Pattern.ROW, hn.Pattern.GATHER, hn.Pattern.RELATIVE):
         P = hn.Pattern(A, layout=layout)
         assert P.mode()[0] == layout
         if layout == hn.Pattern.ROW:
@@ -240,4 +243,5 @@ def test_row_layout_long_rows_bit_identical_to_gather(hn, torch_cuda):
         torch.cuda.synchronize()
         out.append((nval.cpu().numpy(), dyn.item()))
         del P, nval
-    assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+    for v, d in out[1:]:
+        assert np.array_equal(out[0][0], v) and out[0][1] == d

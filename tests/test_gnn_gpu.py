@@ -177,3 +177,108 @@ def test_tcgen05_wait_timeout_is_reported_and_the_context_recovers(hn, torch_cud
     torch.cuda.synchronize()
     y, r = Y.cpu().numpy().astype(np.float64), ref.cpu().numpy().astype(np.float64)
     assert np.max(np.abs(y - r)) <= 1e-5 * (np.abs(r).max() + 1.0)
+
+
+def _bf16(torch, t):
+    return t.to(torch.bfloat16).to(torch.float64).cpu().numpy()
+
+
+def _linear_bwd(hn, torch, lib, M, K1, K2, relu, X1, X2, Wb, Y, dY, with_dx):
+    K = K1 + K2
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    nb = max(1, min((M + 63) // 64, sms))
+    scratch = torch.empty(nb * (64 * K + 64), device="cuda")
+    G = torch.empty((M, 64), device="cuda")
+    dX = torch.full((M, K), float("nan"), device="cuda") if with_dx else None
+    dW = torch.full((K, 64), float("nan"), device="cuda")
+    db = torch.full((64,), float("nan"), device="cuda")
+    hn.check(lib.hn_gnn_linear_bwd(M, K1, K2, X1.data_ptr(), None if X2 is None else X2.data_ptr(), Wb.data_ptr(),
+                                   Y.data_ptr(), dY.data_ptr(), relu, G.data_ptr(),
+                                   None if dX is None else dX.data_ptr(), dW.data_ptr(), db.data_ptr(),
+                                   scratch.data_ptr(), scratch.numel(), None))
+    return G, dX, dW, db
+
+
+@pytest.mark.parametrize("K1,K2,relu,M", [(16, 0, 1, 1000), (64, 0, 0, 130), (64, 64, 1, 4097), (32, 32, 1, 64),
+                                            (64, 64, 1, 148 * 64 * 3 + 77), (48, 16, 0, 20001), (16, 0, 1, 1),
+                                            (64, 64, 0, 148 * 128 * 2 + 5)])
+def test_tcgen05_backward_matches_float64_of_the_bf16_operands(hn, torch_cuda, K1, K2, relu, M):
+    """hn_gnn_linear_bwd: dX = G W^T (the tcgen05 layer kernel with 64 or 128
+    outputs) and dW = [X1 | X2]^T G (the tcgen05 weight-gradient kernel, one
+    TMEM accumulator per persistent CTA over its 64-row tiles) against a
+    float64 product of the same BF16-rounded operands; db against the FP32
+    G. Every element is within 1e-4 of the sum of its terms' magnitudes
+    (FP32 accumulation; a wrong operand layout or a dropped tile gives errors
+    of order one). The larger cases give each CTA several tiles (all three
+    staging buffers cycle) and end on a partial tile; M = 1 is one row."""
+    torch = torch_cuda
+    g = torch.Generator(device="cuda").manual_seed(K1 * 7 + K2 + M)
+    K = K1 + K2
+    X1 = torch.randn((M, K1), generator=g, device="cuda")
+    X2 = torch.randn((M, K2), generator=g, device="cuda") if K2 else None
+    W = torch.randn(K * 64, generator=g, device="cuda") / K ** 0.5
+    Wt = torch.empty(K * 64, dtype=torch.bfloat16, device="cuda")
+    Wb = torch.empty(K * 64, dtype=torch.bfloat16, device="cuda")
+    Y = torch.randn((M, 64), generator=g, device="cuda")
+    dY = torch.randn((M, 64), generator=g, device="cuda")
+    lib = hn.load()
+    hn.check(lib.hn_gnn_cast_weights(K, W.data_ptr(), Wt.data_ptr(), Wb.data_ptr(), None))
+    with_dx = K in (64, 128)
+    G, dX, dW, db = _linear_bwd(hn, torch, lib, M, K1, K2, relu, X1, X2, Wb, Y, dY, with_dx)
+    hn.check(lib.hn_gnn_check(None))
+    torch.cuda.synchronize()
+    Gf = torch.where(Y > 0, dY, torch.zeros_like(dY)) if relu else dY
+    assert torch.equal(G, Gf)
+    Gb = _bf16(torch, Gf)
+    X = X1 if X2 is None else torch.cat([X1, X2], dim=1)
+    Xb = _bf16(torch, X)
+    Wd = _bf16(torch, W.view(K, 64))
+    dW_ref = Xb.T @ Gb
+    bound = 1e-4 * (np.abs(Xb).T @ np.abs(Gb)) + 1e-30
+    assert np.all(np.abs(dW.cpu().numpy().astype(np.float64) - dW_ref) <= bound)
+    Gd = Gf.to(torch.float64).cpu().numpy()
+    assert np.all(np.abs(db.cpu().numpy() - Gd.sum(0)) <= 1e-4 * np.abs(Gd).sum(0) + 1e-30)
+    if with_dx:
+        dX_ref = Gb @ Wd.T
+        bx = 1e-4 * (np.abs(Gb) @ np.abs(Wd).T) + 1e-30
+        assert np.all(np.abs(dX.cpu().numpy().astype(np.float64) - dX_ref) <= bx)
+    # deterministic: a second call gives the same bits
+    _, dX2, dW2, db2 = _linear_bwd(hn, torch, lib, M, K1, K2, relu, X1, X2, Wb, Y, dY, with_dx)
+    assert torch.equal(dW, dW2) and torch.equal(db, db2)
+    assert (not with_dx) or torch.equal(dX, dX2)
+
+
+@pytest.mark.parametrize("polls", [1, 8])
+def test_tcgen05_backward_wait_timeout_is_reported_and_the_context_recovers(hn, torch_cuda, polls):
+    """The backward's tcgen05 kernels (dX and dW) share the layer's bounded
+    waits and flag: with the test hook's few polls they give up while their
+    own bulk copies are in flight, settle them with the full bound, free
+    TMEM and return; hn_gnn_check reports it. Then the normal limit gives
+    the same result as a fresh run."""
+    torch = torch_cuda
+    M, K1, K2 = 148 * 128 * 2 + 5, 64, 64
+    g = torch.Generator(device="cuda").manual_seed(11)
+    X1 = torch.randn((M, K1), generator=g, device="cuda")
+    X2 = torch.randn((M, K2), generator=g, device="cuda")
+    W = torch.randn(128 * 64, generator=g, device="cuda") / 128 ** 0.5
+    Wt = torch.empty(128 * 64, dtype=torch.bfloat16, device="cuda")
+    Wb = torch.empty(128 * 64, dtype=torch.bfloat16, device="cuda")
+    Y = torch.randn((M, 64), generator=g, device="cuda")
+    dY = torch.randn((M, 64), generator=g, device="cuda")
+    lib = hn.load()
+    hn.check(lib.hn_gnn_cast_weights(128, W.data_ptr(), Wt.data_ptr(), Wb.data_ptr(), None))
+    ref = _linear_bwd(hn, torch, lib, M, K1, K2, 1, X1, X2, Wb, Y, dY, True)
+    hn.check(lib.hn_gnn_check(None))
+    try:
+        hn.check(lib.hn_gnn_set_wait_limit(polls))
+        _linear_bwd(hn, torch, lib, M, K1, K2, 1, X1, X2, Wb, Y, dY, True)
+        st = lib.hn_gnn_check(None)
+        assert st == hn.HN_ERR_CUDA, st
+        assert b"timed out" in lib.hn_last_error()
+    finally:
+        hn.check(lib.hn_gnn_set_wait_limit(0))
+    assert lib.hn_gnn_check(None) == hn.HN_OK
+    out = _linear_bwd(hn, torch, lib, M, K1, K2, 1, X1, X2, Wb, Y, dY, True)
+    hn.check(lib.hn_gnn_check(None))
+    for a, b in zip(ref, out):
+        assert torch.equal(a, b)
