@@ -181,15 +181,18 @@ int hn_nrm2(int64_t n, const double* v_dev, double* result_dev, void* stream);
  * limited by their largest block only), and nnz(N) < 2^31. */
 int hn_ada_symbolic(const hn_csr* A, hn_pattern** out);
 /* The numeric phase has three layouts with bit-identical results.
- *  - Gather mode (the default) keeps an 8-byte source pair (A^T entry, A
- *    entry) per slot of N; one thread per slot, in slot order.
- *  - Relative map, asked for with HN_ADA_RELATIVE and used when the offsets
- *    fit 32 bits (longest row of A x longest row of A^T < 2^31), keeps 4
- *    bytes per slot: the single term's entry within its row of A and within
- *    its row of A^T (or the slot's index among its row's multi-term slots);
- *    one warp per row of N, longest rows first. Half the map memory; on the
- *    large LP it is not faster (both layouts are bound by the random L2
- *    gathers of A^T values). HN_ADA_GATHER8 asks for gather mode.
+ *  - Gather mode keeps an 8-byte source pair (A^T entry, A entry) per slot
+ *    of N; one thread per slot, in slot order. The default unless the
+ *    relative map is.
+ *  - Relative map, used when the offsets fit 32 bits (longest row of A x
+ *    longest row of A^T < 2^31) and every row of A has <= 256 entries, and
+ *    either HN_ADA_RELATIVE asks for it or the rows of N average >= 2,048
+ *    slots (without HN_ADA_COMPACT): 4 bytes per slot, the single term's
+ *    entry within its row of A and within its row of A^T (or the slot's
+ *    index among its row's multi-term slots); one warp per row of N, longest
+ *    rows first, the row's A entries staged in shared memory. Half the map
+ *    memory, 5 % faster than gather mode on the 200k x 500k LP.
+ *    HN_ADA_GATHER8 asks for gather mode.
  *  - Row mode, asked for with HN_ADA_COMPACT and used when every row of N has
  *    <= 65,534 slots and every row of A <= 256 entries, keeps a 2-byte slot
  *    offset per term and assembles each row of N in shared-memory windows. */

@@ -356,6 +356,7 @@ __global__ void __launch_bounds__(kT, 4) ada_slot_kernel(int64_t nnz, const uint
 constexpr int kRmapU = 8;
 constexpr int kRmapT = 256;      // threads (8 warps, one row each)
 constexpr int kRmapTerms = 256;  // longest row of A this layout takes
+constexpr int64_t kRmapMinRow = 2048;  // mean slots per row of N above which it is the default
 __global__ void __launch_bounds__(kRmapT, 3) ada_rmap_kernel(int m, const int32_t* __restrict__ order,
                                                              unsigned* __restrict__ row_next,
                                                              const int32_t* __restrict__ rpA,
@@ -748,7 +749,10 @@ int hn_ada_symbolic_ex(const hn_csr* A, unsigned flags, hn_pattern** out) {
                 while ((int64_t(1) << qbits) < maxcol) ++qbits;
                 const bool fits = qbits < 31 && (int64_t)std::max(maxes[2], 1u) <= (int64_t(1) << (31 - qbits)) &&
                                   maxes[2] <= (unsigned)kRmapTerms;
-                rel = fits && (flags & HN_ADA_RELATIVE);
+                // without a request: the relative map when the rows of N are
+                // long enough for a warp per row to amortise its set-up
+                const bool long_rows = P->nnz >= kRmapMinRow * m;
+                rel = fits && ((flags & HN_ADA_RELATIVE) || (!(flags & HN_ADA_COMPACT) && long_rows));
             }
             P->ci = dmalloc<int32_t>(P->nnz);
             if (P->row_mode) {
