@@ -50,28 +50,62 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+    """SM clock and throttle reasons sampled during the timed region: NVML
+    queries every 10 ms (read-only), or nvidia-smi every 200 ms when the
+    NVML binding is missing."""
+
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
+        self.samples = []  # (sm MHz, max sm MHz, [reason flags in NAMES order])
         self._stop = threading.Event()
         self._t = None
 
+    def _nvml_loop(self, nv):
+        h = nv.nvmlDeviceGetHandleByIndex(self.index)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        while not self._stop.is_set():
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), float(mx),
+                                 [bool(r & b) for b in bits]))
+            self._stop.wait(0.01)
+
+    def _smi_loop(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                f = [x.strip() for x in out.split(",")]
+                if len(f) == 6 and f[0].replace(".", "").isdigit() and f[1].replace(".", "").isdigit():
+                    self.samples.append((float(f[0]), float(f[1]), [x.lower() == "active" for x in f[2:]]))
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
     def start(self):
         def run():
-            q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-            while not self._stop.is_set():
+            try:
+                import pynvml as nv
+
+                nv.nvmlInit()
+            except Exception:
+                self._smi_loop()
+                return
+            try:
+                self._nvml_loop(nv)
+            except Exception:
+                self._smi_loop()
+            finally:
                 try:
-                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.samples.append([s.strip() for s in out.split(",")])
+                    nv.nvmlShutdown()
                 except Exception:
                     pass
-                self._stop.wait(0.2)
 
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
@@ -82,11 +116,9 @@ class ClockSampler:
             self._t.join(timeout=10)
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+        sm = [s[0] for s in self.samples]
+        reasons = sorted({self.NAMES[i] for s in self.samples for i in range(4) if s[2][i]})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(s[1] for s in self.samples),
                 "reasons": reasons, "samples": len(self.samples)}
 
 
@@ -551,6 +583,8 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
     t0 = time.perf_counter()
     lab = batched(train_lps)
     label_s = time.perf_counter() - t0
+    print(json.dumps({"gnn_progress": "labelled", "train": n_train, "label_s": round(label_s, 1)}), file=sys.stderr,
+          flush=True)
     keep = [i for i in range(n_train) if lab["status"][i] == 1]
     batches = []
     for j in range(0, len(keep), 8):
@@ -562,6 +596,8 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     del batches
+    print(json.dumps({"gnn_progress": "trained", "train_s": round(train_s, 1),
+                      "loss_first_last": [losses[0], losses[-1]]}), file=sys.stderr, flush=True)
 
     eval_lps = gen(n_eval, 1_000_000)
     torch.cuda.synchronize()
@@ -569,6 +605,8 @@ def gnn_warm(n_train: int, n_eval: int, mlo: int, mhi: int, epochs: int, chunk: 
     cold = batched(eval_lps)
     torch.cuda.synchronize()
     cold_s = time.perf_counter() - t0
+    print(json.dumps({"gnn_progress": "cold", "cold_s": round(cold_s, 2),
+                      "iterations_mean_cold": float(cold["iterations"].mean())}), file=sys.stderr, flush=True)
     t0 = time.perf_counter()
     warm = batched(eval_lps, warm=model)
     torch.cuda.synchronize()
