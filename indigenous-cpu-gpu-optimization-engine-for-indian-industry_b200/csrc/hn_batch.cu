@@ -403,7 +403,7 @@ __device__ __forceinline__ void dmma_m8n8k4(double* d, double a, double b) {
                  : "d"(a), "d"(b));
 }
 constexpr int kFbP = kFb + 1;  // padded smem row (conflict-free column walks)
-constexpr size_t kPanelSmem = sizeof(double) * (2 * kFb * kFbP + kFb);
+constexpr size_t kPanelSmem = sizeof(double) * (2 * kFb * kFbP + 2 * kFb);
 
 __global__ void __launch_bounds__(kT) batch_ldlt_diag_kernel(int s, const int64_t* __restrict__ row_off,
                                                              const int64_t* __restrict__ dn_off,
@@ -415,6 +415,7 @@ __global__ void __launch_bounds__(kT) batch_ldlt_diag_kernel(int s, const int64_
     double(*sA)[kFbP] = reinterpret_cast<double(*)[kFbP]>(smem);
     double(*sL)[kFbP] = reinterpret_cast<double(*)[kFbP]>(smem + kFb * kFbP);
     double* sD = smem + 2 * kFb * kFbP;
+    double* sLc = sD + kFb;  // column j of L during pivot j
     const int tid = threadIdx.x;
     const int inst = order[blockIdx.x];
     if (status[inst] != ST_RUN) return;
@@ -430,21 +431,25 @@ __global__ void __launch_bounds__(kT) batch_ldlt_diag_kernel(int s, const int64_
         sA[r][c] = (r < nb && c <= r) ? A[(int64_t)(k0 + r) * ld + k0 + c] : 0.0;
     }
     __syncthreads();
-    // pivot j: every thread forms the clamped pivot itself; warp w takes rows
-    // rr = j + 1 + w, j + 9 + w, ..., lanes the columns j < cc <= rr; each
-    // element takes A_rr,cc -= (l_rr d) l_cc with l = A_.,j / d, the sequence
-    // and roundings of the column-by-column elimination; L goes to sL so
-    // column j stays unscaled for the other warps within the step
+    // pivot j: every thread forms the clamped pivot itself; column j of L,
+    // l = A_.,j / d, is divided out once (to sLc and sL; column j of sA stays
+    // unscaled); then warp w takes rows rr = j + 1 + w, j + 9 + w, ..., lanes
+    // the columns j < cc <= rr, and each element takes A_rr,cc -= (l_rr d) l_cc:
+    // the sequence and roundings of the column-by-column elimination
     const int lane = tid & 31, warp = tid >> 5;
     for (int j = 0; j < nb; ++j) {
         double d = sA[j][j];
         if (d <= tol) d = tol;  // SparseCholesky pivot clamp
         if (tid == 0) sD[j] = d;
+        for (int cc = j + 1 + tid; cc < nb; cc += kT) {
+            const double l = sA[cc][j] / d;
+            sLc[cc] = l;
+            sL[cc][j] = l;
+        }
+        __syncthreads();
         for (int rr = j + 1 + warp; rr < nb; rr += kT / 32) {
-            const double lr = sA[rr][j] / d;
-            const double wr = lr * d;
-            for (int cc = j + 1 + lane; cc <= rr; cc += 32) sA[rr][cc] -= wr * (sA[cc][j] / d);
-            if (lane == 0) sL[rr][j] = lr;
+            const double wr = sLc[rr] * d;
+            for (int cc = j + 1 + lane; cc <= rr; cc += 32) sA[rr][cc] -= wr * sLc[cc];
         }
         __syncthreads();
     }
