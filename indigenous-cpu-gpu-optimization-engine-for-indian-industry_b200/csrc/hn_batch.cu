@@ -536,6 +536,16 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool vali
                  : "memory");
 }
 
+struct UpdPair {
+    int m, ld, rb, cb;
+    int64_t r0;
+    double* A;
+};
+
+// Persistent: each CTA walks pairs blockIdx.x, + grid, ... and overlaps the
+// next pair's panel copies with the current pair's epilogue (the panels are
+// free once the multiply is done; the output tile's buffer once the epilogue
+// has read it).
 __global__ void __launch_bounds__(kT, 2) batch_ldlt_update_kernel(int s, int cnt, int64_t npairs,
                                                                const int64_t* __restrict__ pairs,
                                                                const int64_t* __restrict__ row_off,
@@ -551,69 +561,88 @@ __global__ void __launch_bounds__(kT, 2) batch_ldlt_update_kernel(int s, int cnt
     double* sD = upd_smem + 3 * kFb * kUpdP;
     const int tid = threadIdx.x;
     const int k0 = s * kFb;
-    int lo = 0;  // the instance of the previous pair: pairs arrive in increasing order
-    for (int64_t pidx = blockIdx.x; pidx < npairs; pidx += gridDim.x) {
-        // instance of this pair: first b with pairs[b] > pidx (pairs is
-        // inclusive), searched from the previous one by doubling steps
-        if (pairs[lo] <= pidx) {
-            int step = 1, base = lo;
-            while (base + step < cnt - 1 && pairs[base + step] <= pidx) {
-                base += step;
-                step <<= 1;
+    const int k1 = k0 + kFb;  // a trailing part exists only below a full block
+    int lo = 0;               // the instance of the previous pair: pairs arrive in increasing order
+    int64_t pidx = blockIdx.x;
+    // the next pair of a running instance from pidx on (pidx moves past it);
+    // the same answer in every thread
+    auto next_pair = [&](UpdPair& P) -> bool {
+        for (; pidx < npairs; pidx += gridDim.x) {
+            // instance of this pair: first b with pairs[b] > pidx (pairs is
+            // inclusive), searched from the previous one by doubling steps
+            if (pairs[lo] <= pidx) {
+                int step = 1, base = lo;
+                while (base + step < cnt - 1 && pairs[base + step] <= pidx) {
+                    base += step;
+                    step <<= 1;
+                }
+                int a = base + 1, b = min(base + step, cnt - 1);
+                while (a < b) {
+                    const int mid = (a + b) >> 1;
+                    if (pairs[mid] <= pidx)
+                        a = mid + 1;
+                    else
+                        b = mid;
+                }
+                lo = a;
             }
-            int a = base + 1, b = min(base + step, cnt - 1);
-            while (a < b) {
-                const int mid = (a + b) >> 1;
-                if (pairs[mid] <= pidx)
-                    a = mid + 1;
-                else
-                    b = mid;
-            }
-            lo = a;
+            const int inst = order[lo];
+            if (status[inst] != ST_RUN) continue;
+            const int64_t local = pidx - (lo > 0 ? pairs[lo - 1] : 0);
+            int ti = static_cast<int>((sqrt(8.0 * (double)local + 1.0) - 1.0) * 0.5);
+            while ((int64_t)(ti + 1) * (ti + 2) / 2 <= local) ++ti;
+            while ((int64_t)ti * (ti + 1) / 2 > local) --ti;
+            const int tj = static_cast<int>(local - (int64_t)ti * (ti + 1) / 2);
+            P.r0 = row_off[inst];
+            P.m = static_cast<int>(row_off[inst + 1] - P.r0);
+            P.ld = dense_ld(P.m);
+            P.rb = k1 + ti * kFb;
+            P.cb = k1 + tj * kFb;
+            P.A = dense + dn_off[inst];
+            pidx += gridDim.x;
+            return true;
         }
-        const int inst = order[lo];
-        if (status[inst] != ST_RUN) continue;  // uniform across the CTA
-        const int64_t local = pidx - (lo > 0 ? pairs[lo - 1] : 0);
-        const int64_t r0 = row_off[inst];
-        const int m = static_cast<int>(row_off[inst + 1] - r0);
-        const int ld = dense_ld(m);
-        // a trailing part exists only below a full block: nb = kFb here
-        const int k1 = k0 + kFb;
-        int ti = static_cast<int>((sqrt(8.0 * (double)local + 1.0) - 1.0) * 0.5);
-        while ((int64_t)(ti + 1) * (ti + 2) / 2 <= local) ++ti;
-        while ((int64_t)ti * (ti + 1) / 2 > local) --ti;
-        const int tj = static_cast<int>(local - (int64_t)ti * (ti + 1) / 2);
-        const int rb = k1 + ti * kFb, cb = k1 + tj * kFb;
-        double* A = dense + dn_off[inst];
-        __syncthreads();  // the previous pair's fragment loads are done with the buffers
-        // 2 slices x 64 rows x 16 chunks of 16 bytes per half; rows past m are zero-filled
+        return false;
+    };
+    // 2 slices x 64 rows x 16 chunks of 16 bytes per half, one commit group
+    // per half; rows past m are zero-filled
+    auto issue_panels = [&](const UpdPair& P) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             for (int idx = tid; idx < 2 * kFb * 16; idx += kT) {
                 const int side = idx >> 10, rr = (idx >> 4) & (kFb - 1), q2 = idx & 15;
-                const int row = (side ? cb : rb) + rr;
-                const bool ok = row < m;
-                const double* src = A + (int64_t)(ok ? row : rb) * ld + k0 + h * 32 + 2 * q2;
+                const int row = (side ? P.cb : P.rb) + rr;
+                const bool ok = row < P.m;
+                const double* src = P.A + (int64_t)(ok ? row : P.rb) * P.ld + k0 + h * 32 + 2 * q2;
                 double* dst = (side ? sL[rr] : sW[rr]) + h * 32 + 2 * q2;
                 cp_async16(dst, src, ok);
             }
             asm volatile("cp.async.commit_group;\n" ::: "memory");
         }
-        // the output tile (third group): rows or columns past m are zero-filled
+    };
+    // the output tile, one commit group: rows or columns past m are zero-filled
+    auto issue_tile = [&](const UpdPair& P) {
         for (int idx = tid; idx < kFb * 32; idx += kT) {
             const int rr = idx >> 5, q2 = idx & 31;
-            const int row = rb + rr, col = cb + 2 * q2;
-            const bool ok = row < m && col < m;
-            const double* src = A + (ok ? (int64_t)row * ld + col : (int64_t)rb * ld + k0);
+            const int row = P.rb + rr, col = P.cb + 2 * q2;
+            const bool ok = row < P.m && col < P.m;
+            const double* src = P.A + (ok ? (int64_t)row * P.ld + col : (int64_t)P.rb * P.ld + k0);
             cp_async16(sC[rr] + 2 * q2, src, ok);
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
-        if (tid < kFb) sD[tid] = dD[r0 + k0 + tid];
-        // warp w: rows 16 (w >> 1) .. + 16 (two 8-row tiles), columns
-        // 32 (w & 1) .. + 32 (four 8-column tiles) of the 64 x 64 output
-        const int lane = tid & 31, warp = tid >> 5;
-        const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
-        const int fr = lane >> 2, fk = lane & 3;
+    };
+    UpdPair cur;
+    if (!next_pair(cur)) return;
+    issue_panels(cur);
+    issue_tile(cur);
+    if (tid < kFb) sD[tid] = dD[cur.r0 + k0 + tid];
+    // warp w: rows 16 (w >> 1) .. + 16 (two 8-row tiles), columns
+    // 32 (w & 1) .. + 32 (four 8-column tiles) of the 64 x 64 output
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
+    const int fr = lane >> 2, fk = lane & 3;
+    for (;;) {
+        // in flight: this pair's panel halves, then its output tile
         double acc[2][4][2];
 #pragma unroll
         for (int i = 0; i < 2; ++i)
@@ -640,21 +669,35 @@ __global__ void __launch_bounds__(kT, 2) batch_ldlt_update_kernel(int s, int cnt
                     for (int j = 0; j < 4; ++j) dmma_m8n8k4(acc[i][j], a[i], b[j]);
             }
         }
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();  // every warp is done with the panels and D
+        UpdPair nxt;
+        const bool more = next_pair(nxt);
+        if (more) {
+            issue_panels(nxt);
+            if (tid < kFb) sD[tid] = dD[nxt.r0 + k0 + tid];
+            asm volatile("cp.async.wait_group 2;\n" ::: "memory");  // this pair's tile; the next panels stay in flight
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        }
         __syncthreads();  // the output tile is in shared memory
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
-            const int gr = rb + wr + 8 * i + fr;
-            if (gr >= m) continue;
+            const int gr = cur.rb + wr + 8 * i + fr;
+            if (gr >= cur.m) continue;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
 #pragma unroll
                 for (int t = 0; t < 2; ++t) {
-                    const int gc = cb + wc + 8 * j + 2 * fk + t;
-                    if (gc <= gr) A[(int64_t)gr * ld + gc] = sC[wr + 8 * i + fr][wc + 8 * j + 2 * fk + t] - acc[i][j][t];
+                    const int gc = cur.cb + wc + 8 * j + 2 * fk + t;
+                    if (gc <= gr)
+                        cur.A[(int64_t)gr * cur.ld + gc] = sC[wr + 8 * i + fr][wc + 8 * j + 2 * fk + t] - acc[i][j][t];
                 }
             }
         }
+        if (!more) break;
+        __syncthreads();  // every warp is done reading the output tile
+        issue_tile(nxt);
+        cur = nxt;
     }
 }
 
@@ -1200,7 +1243,7 @@ int hn_batch_factor(hn_batch* B, const double* D, double reg, double singular_to
             }
             const int64_t np = B->step_pairs_h[st];
             if (np > 0) {
-                const int grid = (int)std::min<int64_t>(np, (int64_t)ctx().sm_count * 8);
+                const int grid = (int)std::min<int64_t>(np, (int64_t)ctx().sm_count * 2);
                 batch_ldlt_update_kernel<<<grid, kT, kUpdSmem, s>>>((int)st, cnt, np, B->step_pairs + B->pair_off_h[st],
                                                              B->row_off, B->dn_off, B->order, status, B->dense,
                                                              B->dD);
