@@ -51,57 +51,81 @@ def peaks():
 
 class ClockSampler:
     """SM clock and throttle reasons sampled during the timed region: NVML
-    queries every 10 ms (read-only), or nvidia-smi every 200 ms when the
-    NVML binding is missing."""
+    queries every 10 ms (read-only), or nvidia-smi every 200 ms when NVML
+    cannot be queried. The NVML handle and the reasons call are probed in
+    start(), before the timed region, so a failing call falls back to
+    nvidia-smi from the first sample on."""
 
     NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
         self.samples = []  # (sm MHz, max sm MHz, [reason flags in NAMES order])
+        self.source = None
+        self.note = None
         self._stop = threading.Event()
         self._t = None
 
-    def _nvml_loop(self, nv):
-        h = nv.nvmlDeviceGetHandleByIndex(self.index)
-        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
-                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
-        while not self._stop.is_set():
-            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-            self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), float(mx),
-                                 [bool(r & b) for b in bits]))
-            self._stop.wait(0.01)
+    def _nvml_probe(self):
+        import pynvml as nv
 
-    def _smi_loop(self):
+        nv.nvmlInit()
+        h = nv.nvmlDeviceGetHandleByIndex(self.index)
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        reasons = None
+        for name in ("nvmlDeviceGetCurrentClocksEventReasons", "nvmlDeviceGetCurrentClocksThrottleReasons"):
+            fn = getattr(nv, name, None)
+            if fn is None:
+                continue
+            try:
+                fn(h)
+                reasons = fn
+                break
+            except Exception:
+                continue
+        if reasons is None:
+            raise RuntimeError("no NVML clock-reasons call")
+        bits = [getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
+                getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+                getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+                getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4)]
+
+        def sample():
+            r = reasons(h)
+            return (float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), mx, [bool(r & b) for b in bits])
+
+        sample()
+        return nv, sample
+
+    def _smi_sample(self):
         q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                f = [x.strip() for x in out.split(",")]
-                if len(f) == 6 and f[0].replace(".", "").isdigit() and f[1].replace(".", "").isdigit():
-                    self.samples.append((float(f[0]), float(f[1]), [x.lower() == "active" for x in f[2:]]))
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits"],
+                             capture_output=True, text=True, timeout=5).stdout.strip()
+        f = [x.strip() for x in out.split(",")]
+        if len(f) == 6 and f[0].replace(".", "").isdigit() and f[1].replace(".", "").isdigit():
+            return (float(f[0]), float(f[1]), [x.lower() == "active" for x in f[2:]])
+        return None
 
     def start(self):
-        def run():
-            try:
-                import pynvml as nv
+        nv = sample = None
+        try:
+            nv, sample = self._nvml_probe()
+            self.source = "nvml"
+        except Exception as e:  # no NVML binding or call: nvidia-smi
+            self.source = "nvidia-smi"
+            self.note = f"nvml: {type(e).__name__}: {e}"[:160]
 
-                nv.nvmlInit()
-            except Exception:
-                self._smi_loop()
-                return
-            try:
-                self._nvml_loop(nv)
-            except Exception:
-                self._smi_loop()
-            finally:
+        def run():
+            while not self._stop.is_set():
+                try:
+                    v = sample() if sample else self._smi_sample()
+                    if v:
+                        self.samples.append(v)
+                except Exception as e:
+                    self.note = f"{self.source}: {type(e).__name__}: {e}"[:160]
+                self._stop.wait(0.01 if sample else 0.2)
+            if nv is not None:
                 try:
                     nv.nvmlShutdown()
                 except Exception:
@@ -115,11 +139,14 @@ class ClockSampler:
         if self._t:
             self._t.join(timeout=10)
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+            out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "source": self.source}
+            if self.note:
+                out["note"] = self.note
+            return out
         sm = [s[0] for s in self.samples]
         reasons = sorted({self.NAMES[i] for s in self.samples for i in range(4) if s[2][i]})
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(s[1] for s in self.samples),
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(self.samples), "source": self.source}
 
 
 def dist_setup():
